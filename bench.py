@@ -1,0 +1,388 @@
+"""Benchmark of the B200 Jacobi-PCG hot path on the 1108x1108 2D P1-FEM system.
+
+Workload: interior grid 1108 x 1108 (n = 1,227,664, ~7 nnz/row), jittered nodes (0.3h),
+log-normal per-element conductivity sigma = 2.0, random symmetric permutation (seed 1) then
+reverse Cuthill-McKee, SELL-C-sigma C=32 sigma=256, b = A x_true with x_true ~ U(-1,1), x0 = 0,
+tolerance 1e-8 FP64 true relative residual.  Synthetic (generated here; the reference's
+SuiteSparse thermal2 of the same shape class is not available offline).
+
+A step is one full solve to tolerance.  `value` is solves/s over all ranks; the line also
+carries time-to-tolerance, SpMV GB/s (L2-flushed and warm), the roofline of the persistent
+kernel, an end-to-end number through the public host-array API, and the reference's own CPU
+code timed on a bounded sample (cpu_baseline).  With --gpus N > 1 every rank solves its own
+replica (the single-system solve does not shard; no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--grid G]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "time-to-1e-8 rel. residual: learned/mixed vs plain Jacobi-PCG; SpMV HBM GB/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--grid", type=int, default=1108, help="interior grid side (n = grid^2)")
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--cpu-sample-iters", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    if PEAKS_FILE.exists():
+        p = json.loads(PEAKS_FILE.read_text())
+        return float(p["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_config(args, extra=None):
+    c = {"workload": f"2d-p1fem-{args.grid}x{args.grid}-sigma2-perm1-rcm", "n": args.grid * args.grid,
+         "tol_rel_true": args.tol, "format": "sell-c32-sigma256", "precision": "fp32 values+vectors, fp64 x and residual replacement",
+         "l2": "flushed between timed solves (256 MiB write)", "parallelism": f"replicas x{args.gpus}"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{device_index}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if args.impl == "b200" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device=None):
+    if pg is not None:
+        if device is not None:
+            pg.barrier(device_ids=[device.index])
+        else:
+            pg.barrier()
+
+
+# --------------------------------------------------------------------------------------
+# reference arm: the reference's own CPU code (oracle/_ref, built from its sources)
+# --------------------------------------------------------------------------------------
+def cpu_reference_sample(d, iters):
+    """Times `iters` iterations of the reference's run_jacobi_pcg on this host (1 thread: the
+    reference has no threading).  Returns (seconds per iteration, kind, label)."""
+    from oracle import oracle as O
+    use_ref = O.reflib() is not None
+    t0 = time.perf_counter()
+    O.golden(d, 1e-300, iters, use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    # one SpMV + setup are inside; per-iteration cost is the slope: time a second, shorter run
+    t1 = time.perf_counter()
+    O.golden(d, 1e-300, max(1, iters // 4), use_ref=use_ref)
+    dt2 = time.perf_counter() - t1
+    per_it = (dt - dt2) / (iters - max(1, iters // 4))
+    setup = max(0.0, dt - per_it * iters)
+    kind = "reference" if use_ref else "port"
+    return per_it, setup, kind
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_init(args)
+    if rank != 0:
+        return 0
+    from project_xplus_b200 import generators as g
+    d, _ = g.system_2d_large(args.grid)
+    iters_needed = None
+    ref_iters_file = ROOT / "profiles" / "iterations_2d_large.json"
+    if ref_iters_file.exists():
+        iters_needed = json.loads(ref_iters_file.read_text()).get("fp64_golden_iterations")
+    if not iters_needed:
+        iters_needed = 4000
+    samples = []
+    for k in range(args.warmup + args.steps):
+        per_it, setup, kind = cpu_reference_sample(d, args.cpu_sample_iters)
+        if k >= args.warmup:
+            samples.append(per_it * iters_needed + setup)
+    t = statistics.median(samples)
+    value = 1.0 / t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, {"solver": "reference run_jacobi_pcg (FP64 CSR, 1 thread)"}),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": kind,
+                             "sample": f"{args.cpu_sample_iters} iterations of run_jacobi_pcg per step on the full "
+                                       f"system, extrapolated to {iters_needed} iterations"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------------------
+# B200 arm
+# --------------------------------------------------------------------------------------
+def run_b200(args):
+    import ctypes as C
+
+    import torch
+
+    world, rank, local, pg = dist_init(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import project_xplus_b200 as xp
+    from project_xplus_b200 import _lib
+    from project_xplus_b200 import generators as g
+
+    d, xt = g.system_2d_large(args.grid)
+    n = d.n
+    solver = xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=1, device=local)
+    info = solver.info()
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    b_dev = torch.from_numpy(d.b).to(dev)
+    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    hbm, hbm_kind = peaks()
+
+    def one_solve():
+        x_dev.zero_()
+        _lib.check(_lib.lib.xplus_pcg_solve_device(solver.handle, b_dev.data_ptr(), x_dev.data_ptr(),
+                                                   args.tol, _lib.XPLUS_TAU_REL_TRUE, 20000, sp))
+
+    def metrics():
+        m = _lib.XplusMetrics()
+        _lib.check(_lib.lib.xplus_pcg_last_metrics(solver.handle, C.byref(m)))
+        return m
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        one_solve()
+        torch.cuda.synchronize()
+    m0 = metrics()
+    barrier(pg, dev)
+    torch.cuda.synchronize()
+    step_ms, kern_ms, iters, repls, relres = [], [], [], [], []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            one_solve()
+            e1.record(stream)
+            e1.synchronize()
+            m = metrics()
+            step_ms.append(e0.elapsed_time(e1))
+            kern_ms.append(m.kernel_ms)
+            iters.append(m.iterations)
+            repls.append(m.replacements)
+            relres.append(m.true_rel_residual)
+            if m.status != 0:
+                raise SystemExit(f"solve did not converge: status {m.status} res {m.true_rel_residual}")
+    torch.cuda.synchronize()
+    barrier(pg, dev)
+    total_ms = sum(step_ms)
+    total_ms_max = max_over_ranks(pg, total_ms, dev)
+    value = world * args.steps / (total_ms_max / 1e3)
+    ms_per_step = total_ms_max / args.steps
+
+    # roofline of the persistent kernel: algorithmic bytes per launch / launch time
+    nnz = info["nnz"]
+    it_mean = statistics.mean(iters)
+    rp_mean = statistics.mean(repls)
+    bytes_iter = 8 * nnz + 52 * n
+    bytes_repl = 12 * nnz + 24 * n + 4 * n
+    bytes_launch = it_mean * bytes_iter + (rp_mean + 2) * bytes_repl
+    kern_mean = statistics.mean(kern_ms)
+    achieved = bytes_launch / (kern_mean / 1e3) / 1e9
+
+    # SpMV alone: cold (L2 flushed before every launch) and warm (back to back)
+    xs = C.c_void_p()
+    ys = C.c_void_p()
+    _lib.check(_lib.lib.xplus_pcg_scratch_vectors(solver.handle, C.byref(xs), C.byref(ys)))
+    spmv_bytes = info["spmv_bytes"]
+
+    def spmv():
+        _lib.check(_lib.lib.xplus_pcg_spmv_device(solver.handle, xs, ys, sp))
+
+    cold = []
+    for k in range(23):
+        flush.fill_(1.0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        spmv()
+        b.record(stream)
+        b.synchronize()
+        if k >= 3:
+            cold.append(a.elapsed_time(b))
+    for _ in range(5):
+        spmv()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(100):
+        spmv()
+    b.record(stream)
+    b.synchronize()
+    warm_ms = a.elapsed_time(b) / 100
+    cold_ms = statistics.median(cold)
+    spmv_cold_gbs = spmv_bytes / (cold_ms / 1e3) / 1e9
+    spmv_warm_gbs = spmv_bytes / (warm_ms / 1e3) / 1e9
+
+    # end to end through the public host-array API (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        b_host = torch.from_numpy(d.b).pin_memory()
+        x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+        iters_c = C.c_int()
+        mm = _lib.XplusMetrics()
+        e2e_ms = []
+        for k in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _lib.check(_lib.lib.xplus_pcg_solve(solver.handle, b_host.data_ptr(), None, args.tol,
+                                                _lib.XPLUS_TAU_REL_TRUE, 20000, x_host.data_ptr(),
+                                                C.byref(iters_c), None, 0, C.byref(mm)))
+            dt = (time.perf_counter() - t0) * 1e3
+            if k >= args.warmup:
+                e2e_ms.append(dt)
+        e2e_tot = max_over_ranks(pg, sum(e2e_ms), dev)
+        e2e = {"value": world * args.steps / (e2e_tot / 1e3), "unit": "solves/s",
+               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n + 128,
+               "ms_per_step": e2e_tot / args.steps}
+
+    # CPU baseline: the reference's own golden on a bounded sample, rank 0 only, N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        per_it, setup, kind = cpu_reference_sample(d, args.cpu_sample_iters)
+        t_cpu = per_it * it_mean + setup
+        cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": kind,
+               "sample": f"{args.cpu_sample_iters} iterations of the reference run_jacobi_pcg (FP64) on the "
+                         f"full system, extrapolated to the {it_mean:.0f} iterations the GPU solve took; "
+                         f"{per_it * 1e3:.1f} ms/iteration"}
+        (ROOT / "profiles").mkdir(exist_ok=True)
+
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, {"nnz": nnz}),
+            "time_to_tol_ms": ms_per_step,
+            "iterations": it_mean, "replacements": rp_mean, "true_rel_residual": max(relres),
+            "spmv": {"cold_gbs": spmv_cold_gbs, "warm_gbs": spmv_warm_gbs, "cold_ms": cold_ms, "warm_ms": warm_ms,
+                     "bytes": spmv_bytes, "frac_cold": spmv_cold_gbs / hbm, "peak_kind": hbm_kind},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "kernel": "pcg_persistent_kernel<float,float,1,false>",
+                         "peak_kind": hbm_kind,
+                         "bytes_per_launch": bytes_launch, "launch_ms": kern_mean},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

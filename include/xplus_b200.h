@@ -1,0 +1,243 @@
+/*
+ * xplus_b200.h -- C ABI of the B200 Jacobi-PCG solver.
+ *
+ * A drop-in for the PCG path of project-xplus: caller-owned host arrays in, the
+ * library owns device memory, one CUDA stream per handle, no CPU fallback (every
+ * compute entry point fails with XPLUS_ERR_CUDA when no usable sm_100 device is
+ * present).  Not thread-safe per handle.  All entry points return an int status
+ * (XPLUS_OK or an XPLUS_ERR_* code) unless stated otherwise; the text of the last
+ * error on the calling thread is returned by xplus_last_error_string().
+ *
+ * Reference interfaces replaced (paths are within the reference project):
+ *   solver entry   SolverConfig{tau,max_iters}      include/cg_common.hpp:52-55
+ *                  run_defaults::kTau/kMaxIters      host/run_defaults.hpp:12-13
+ *                  CuperPcgResult / GoldenResult     host/cuper_pcg_solver.hpp:62-73,
+ *                                                    src/CgSolverGolden.hpp:24-31
+ *   single launch  cuper_pcg_control_kernel(...)     kernels/cuper_pcg_control_kernel.cpp:972-1001
+ *                  status[0..1], metrics[0..3]       kernels/cuper_pcg_control_kernel.cpp:1229-1234
+ *   multi-kernel   spmv_csr_kernel ... update_p_kernel  archived/include/cg_kernels.hpp:9-54
+ *   loader         CsrDataset::load                  src/CsrDataset.hpp:19-67
+ *   jacobi         extract_jacobi_diag / build_jacobi_inverse
+ *                                                    src/CsrDataset.hpp:92-116, host/pcg_common.hpp:42-54
+ *   packed format  build_cuper_control_matrix        host/cuper_control_matrix.hpp:130-207
+ */
+#ifndef XPLUS_B200_H
+#define XPLUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status of a solve: same codes as kernels/cuper_pcg_control_kernel.cpp:90-94,
+ *      plus XPLUS_TIMEOUT for a grid barrier that gave up waiting ---- */
+#define XPLUS_CONVERGED 0
+#define XPLUS_MAX_ITER 1
+#define XPLUS_BREAKDOWN 2
+#define XPLUS_TIMEOUT 3
+
+/* ---- return codes of API calls ---- */
+#define XPLUS_OK 0
+#define XPLUS_ERR_ARG 10     /* invalid argument (null pointer, n <= 0, tau <= 0, ...) */
+#define XPLUS_ERR_CUDA 11    /* CUDA runtime error or no usable device */
+#define XPLUS_ERR_DATA 12    /* invalid CSR, missing or zero diagonal (the loader's throws) */
+#define XPLUS_ERR_IO 13      /* file could not be opened / parsed */
+#define XPLUS_ERR_NOMEM 14   /* host or device allocation failed */
+
+/* ---- element types ---- */
+#define XPLUS_F32 0
+#define XPLUS_BF16 1
+#define XPLUS_F64 2
+
+/* ---- tolerance semantics ---- */
+#define XPLUS_TAU_ABS_RR 0   /* stop when the recurrence rr = ||r||^2 <= tau (the reference's
+                                test, src/CgSolverGolden.hpp:74-76,112) */
+#define XPLUS_TAU_REL_TRUE 1 /* stop when the FP64 true residual ||b - A x|| / ||b|| <= tau,
+                                using FP64 residual replacement (requires the FP64 matrix copy) */
+
+/* ---- preconditioners ---- */
+#define XPLUS_PREC_JACOBI 0
+#define XPLUS_PREC_GTG 1     /* M^-1 = G^T G, G lower-triangular on A's lower pattern */
+
+typedef struct xplus_opts {
+    int value_type;        /* XPLUS_F32 | XPLUS_BF16 | XPLUS_F64: matrix values in the SpMV */
+    int vector_type;       /* XPLUS_F32 | XPLUS_F64: x, r, p, Ap storage in the inner loop */
+    int slice_height;      /* SELL-C-sigma C; must be 32 */
+    int sigma;             /* SELL sort window (rows); multiple of 32, or 1 for no sorting */
+    int chunk;             /* entries per row per vector load: 1, 2 or 4 */
+    int keep_fp64;         /* keep an FP64 copy of A for true residuals (forced on for TAU_REL_TRUE) */
+    int replace_every;     /* FP64 residual replacement every k iterations (0: only on stagnation
+                              / at convergence) */
+    double replace_drop;   /* also replace when ||r|| fell by this factor since the last
+                              replacement (e.g. 1e-4); 0 disables */
+    int block_threads;     /* threads per CTA of the persistent kernel (0: auto) */
+    int blocks_per_sm;     /* CTAs per SM (0: occupancy-derived) */
+    double barrier_timeout_s; /* a grid barrier gives up after this long: status XPLUS_TIMEOUT */
+    int device;            /* CUDA device ordinal */
+    int row_sum_diag;      /* BF16 values: rebuild the FP32 diagonal so Ã keeps A's row sums */
+} xplus_opts;
+
+typedef struct xplus_metrics {
+    int status;            /* XPLUS_CONVERGED .. XPLUS_TIMEOUT */
+    int iterations;        /* inner PCG iterations (status[1] of the control kernel) */
+    int replacements;      /* FP64 residual replacements performed */
+    int reserved0;
+    double rz, rr, pap, alpha;  /* metrics[0..3] of the control kernel */
+    double true_rel_residual;   /* FP64 ||b - A x|| / ||b|| at exit (when the FP64 copy exists) */
+    double kernel_ms;           /* device time of the solve launch(es) */
+    double setup_ms;            /* host+device time of xplus_pcg_create */
+    double reserved[4];
+} xplus_metrics;
+
+typedef struct xplus_pcg xplus_pcg;      /* one SPD system resident on one GPU */
+
+void xplus_opts_default(xplus_opts* opts);
+const char* xplus_last_error_string(void);
+const char* xplus_version(void);
+/* Number of sm_100 devices visible (0 when none); never fails. */
+int xplus_device_count(void);
+
+/* ------------------------------------------------------------------------------------
+ * Single-system solver: replaces the XRT launch of cuper_pcg_control_kernel
+ * (host/cuper_control_xrt_host.cpp:205-272) and the host loops of
+ * run_local_multi_kernel_solver / run_cuper_pcg_solver.
+ * ------------------------------------------------------------------------------------ */
+
+/* Build SELL-C-sigma, Jacobi inverse and upload.  CSR as CsrDataset holds it
+ * (row_ptr[n+1], col_idx[nnz], values[nnz], FP64).  Errors: XPLUS_ERR_DATA for the
+ * loader/diagonal conditions of src/CsrDataset.hpp:25-64,92-116. */
+int xplus_pcg_create(const int* row_ptr, const int* col_idx, const double* values, int n,
+                     const xplus_opts* opts, xplus_pcg** out);
+int xplus_pcg_destroy(xplus_pcg* h);
+
+/* Blocking solve with host arrays.  x0 may be NULL (zeros).  max_iters <= 0 means
+ * max(4n, 1000) as src/CgSolverGolden.hpp:47.  resid_hist (nullable, length hist_len)
+ * receives sqrt(rr) after each iteration, the per-iteration residual of the golden
+ * trace (src/CgSolverGolden.hpp:101-108).  metrics may be NULL. */
+int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau, int tau_mode,
+                    int max_iters, double* x_out, int* iters_out, double* resid_hist,
+                    int hist_len, xplus_metrics* metrics);
+
+/* Asynchronous solve on device-resident FP64 b and x (original row order), enqueued on
+ * `stream` (a cudaStream_t, NULL = the handle's stream).  d_x holds x0 on entry and x on
+ * exit.  Fetch the outcome with xplus_pcg_last_metrics() after synchronising. */
+int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double tau,
+                           int tau_mode, int max_iters, void* stream);
+int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);
+/* Per-iteration trace of the last xplus_pcg_solve that asked for a history: rows x 5
+ * doubles {alpha, beta, rz, rr, sqrt(rr)}, the fields of GoldenIterationTrace
+ * (src/CgSolverGolden.hpp:15-22).  rows <= the hist_len of that solve. */
+int xplus_pcg_last_trace(xplus_pcg* h, double* trace, int rows);
+
+/* Test-only fault injection: in the next solves, CTA `block` withholds its arrival at
+ * the first grid barrier, so every wait runs into its barrier_timeout_s bound and the
+ * solve ends with status XPLUS_TIMEOUT (the context stays usable).  -1 switches it off. */
+int xplus_pcg_debug_skip_arrival(xplus_pcg* h, int block);
+
+/* y = A x through the handle's SELL matrix, FP64 host vectors in original row order. */
+int xplus_pcg_spmv(xplus_pcg* h, const double* x, double* y);
+/* y = A x on device vectors in SELL (permuted) order, of the handle's vector type, n_pad long,
+ * enqueued on `stream`.  For bandwidth measurement. */
+int xplus_pcg_spmv_device(xplus_pcg* h, const void* d_x, void* d_y, void* stream);
+/* Sizes of the resident system: n, n_pad (SELL rows), nnz, stored slots (incl. padding),
+ * and the algorithmic bytes of one SpMV (nnz*(s_val+4) + n*s_x + n*s_y). */
+int xplus_pcg_info(xplus_pcg* h, int64_t* n, int64_t* n_pad, int64_t* nnz, int64_t* slots,
+                   int64_t* spmv_bytes);
+/* Device buffers of the SELL vectors (n_pad elements of the vector type), for tests and
+ * benchmarks that drive xplus_pcg_spmv_device. */
+int xplus_pcg_scratch_vectors(xplus_pcg* h, void** d_x, void** d_y);
+/* Control-kernel ABI (kernels/cuper_pcg_control_kernel.cpp:972-1001) on device pointers:
+ * b and x are FP64 device vectors of length n in original order (x holds x0 on entry);
+ * metrics[4] = {rz, rr, pAp, alpha} and status[2] = {code, iterations} are device
+ * arrays.  The matrix, its Jacobi inverse and the work vectors are the handle's: m_inv,
+ * r, z, p and ap are accepted for signature compatibility and are not touched (the
+ * reference uses them only as workspace).  Tolerance semantics are the reference's
+ * (rr <= tau).  Invalid parameters give status {2, 0} and zeroed metrics, as the
+ * reference does (:1078-1087). */
+int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double* x, double* r,
+                      double* z, double* p, double* ap, double* metrics, int* status,
+                      double tau, int max_iters, int n, void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * Multi-kernel ABI: the five "kernel functions" of archived/include/cg_kernels.hpp:9-54
+ * with the same names and arguments, run on the GPU.  Pointers may be device pointers
+ * (zero copy) or plain host pointers (staged through device buffers), so the reference's
+ * run_local_multi_kernel_solver (archived/host/multi_kernel_solver.hpp:100) can link
+ * against this library unchanged.  There is no n <= 1024 cap; n < 0 returns silently
+ * as valid_n() does (archived/kernels/cg_kernels.cpp:9-12).  Each call is blocking.
+ * ------------------------------------------------------------------------------------ */
+void spmv_csr_kernel(const int* row_ptr, const int* col_idx, const double* values,
+                     const double* x, double* y, int n);
+void spmv_blocked_kernel(const int* row_ptr, const int* col_idx, const double* values,
+                         const double* x, double* y, int n);
+void init_pcg_kernel(const double* b, const double* ax, const double* m_inv, double* r,
+                     double* z, double* p, double* metrics, int n);
+void dot_kernel(const double* a, const double* b, double* out, int n);
+void update_xrz_kernel(double* x, const double* p, double* r, const double* ap,
+                       const double* m_inv, double* z, double* metrics, double alpha, int n);
+void update_p_kernel(const double* z, double* p, double beta, int n);
+
+/* ------------------------------------------------------------------------------------
+ * Host-side data path (no GPU needed).
+ * ------------------------------------------------------------------------------------ */
+
+/* CsrDataset::load: reads row_ptr.txt col_idx.txt values.txt b.txt x0.txt from dir with
+ * the same validation and messages.  Two-phase: call with NULL arrays to get n, nnz. */
+int xplus_dataset_load_text(const char* dir, int* n, int* nnz, int* row_ptr, int* col_idx,
+                            double* values, double* b, double* x0);
+/* Binary cache of the same five arrays (one file).  Same two-phase protocol. */
+int xplus_dataset_save_binary(const char* path, int n, int nnz, const int* row_ptr,
+                              const int* col_idx, const double* values, const double* b,
+                              const double* x0);
+int xplus_dataset_load_binary(const char* path, int* n, int* nnz, int* row_ptr, int* col_idx,
+                              double* values, double* b, double* x0);
+
+/* extract_jacobi_diag: XPLUS_ERR_DATA with the reference's message on a missing/zero entry. */
+int xplus_jacobi_diag(int n, const int* row_ptr, const int* col_idx, const double* values,
+                      double* diag);
+
+/* Synthetic SPD systems.  Two-phase: out arrays NULL -> *n, *nnz.  The matrix is the
+ * P1 finite-element stiffness matrix of -div(k grad u) on the unit square (cube) with
+ * interior nodes g x g (x g), jittered nodes, log-normal per-element conductivity and
+ * eliminated Dirichlet boundary.  perm_seed >= 0 applies a seeded random symmetric
+ * permutation; rcm != 0 then applies reverse Cuthill-McKee.  x_true ~ U(-1,1) from
+ * x_seed, b = A x_true (FP64), x0 = 0. */
+int xplus_gen_fem2d(int g, double sigma, double jitter, uint64_t seed, int64_t perm_seed,
+                    int rcm, uint64_t x_seed, int* n, int* nnz, int* row_ptr, int* col_idx,
+                    double* values, double* b, double* x_true);
+int xplus_gen_fem3d(int g, double sigma, double jitter, uint64_t seed, int64_t perm_seed,
+                    int rcm, uint64_t x_seed, int* n, int* nnz, int* row_ptr, int* col_idx,
+                    double* values, double* b, double* x_true);
+
+/* Reverse Cuthill-McKee ordering of a structurally symmetric CSR: perm[new] = old. */
+int xplus_rcm(int n, const int* row_ptr, const int* col_idx, int* perm);
+/* B = P A P^T for perm[new] = old (columns sorted ascending in each output row). */
+int xplus_permute_symmetric(int n, const int* row_ptr, const int* col_idx, const double* values,
+                            const int* perm, int* out_row_ptr, int* out_col_idx,
+                            double* out_values);
+
+/* SELL-C-sigma layout (host builder; the device copies come from the same function).
+ * Two-phase: pass NULL outputs to get n_slices, slots.  perm[new] = old row,
+ * slice_ptr[n_slices+1] (in slots), slice_width[n_slices], col[slots] in new numbering,
+ * val[slots] (FP64).  diag_split != 0 leaves the diagonal out (returned in diag[n],
+ * new order).  Padding slots hold col = own row, val = 0. */
+int xplus_sell_build(int n, const int* row_ptr, const int* col_idx, const double* values,
+                     int C, int sigma, int chunk, int diag_split, int* n_slices, int64_t* slots,
+                     int* perm, int64_t* slice_ptr, int* slice_width, int* col, double* val,
+                     double* diag);
+
+/* Cuper packed-format import (host/cuper_control_matrix.hpp:73-83,130-207): decode the
+ * 16 channel streams (channel_words words each) into COO triplets in the order they are
+ * stored, skipping padding.  Returns the count in *nnz_out; rows/cols/vals may be NULL
+ * for a size query. */
+int xplus_cuper_unpack(int n, int batch_count, const int* sp_element_list_ptr,
+                       const uint64_t* words, int64_t channel_words, int64_t* nnz_out,
+                       int* rows, int* cols, float* vals);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XPLUS_B200_H */

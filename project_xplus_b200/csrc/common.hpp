@@ -1,0 +1,70 @@
+// common.hpp -- error reporting and small helpers shared by the host and CUDA sources.
+#pragma once
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/xplus_b200.h"
+
+namespace xplus {
+
+// Last error text on the calling thread (xplus_last_error_string).
+void set_error(const std::string& msg);
+const char* last_error();
+
+// An error that maps to an XPLUS_ERR_* code at the C boundary.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Runs f(); converts exceptions to codes and records the message.
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return XPLUS_OK;
+    } catch (const Error& e) {
+        set_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return XPLUS_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return XPLUS_ERR_ARG;
+    }
+}
+
+inline void require(bool cond, int code, const std::string& msg) {
+    if (!cond) throw Error(code, msg);
+}
+
+// CSR structure checks of src/CsrDataset.hpp:29-52, same messages.
+void validate_csr(int n, const int* row_ptr, const int* col_idx, int64_t nnz_expected);
+
+// Jacobi diagonal of src/CsrDataset.hpp:92-116 (throws Error(XPLUS_ERR_DATA, ...)).
+void jacobi_diag(int n, const int* row_ptr, const int* col_idx, const double* values,
+                 double* diag);
+
+struct SellHost {
+    int n = 0, n_pad = 0, C = 32, sigma = 1, chunk = 1, diag_split = 0;
+    int n_slices = 0;
+    int64_t slots = 0;
+    std::vector<int> perm;        // perm[new] = old
+    std::vector<int> iperm;       // iperm[old] = new
+    std::vector<int64_t> slice_ptr;
+    std::vector<int> slice_width;
+    std::vector<int> col;
+    std::vector<double> val;
+    std::vector<double> diag;     // only with diag_split (new order)
+};
+
+// SELL-C-sigma builder (the single implementation behind xplus_sell_build).
+void sell_build(int n, const int* row_ptr, const int* col_idx, const double* values, int C,
+                int sigma, int chunk, int diag_split, SellHost& out);
+
+}  // namespace xplus

@@ -1,0 +1,193 @@
+// device_common.cuh -- element loads, warp/block reductions and the bounded grid barrier
+// shared by the sm_100a kernels.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace xplus {
+namespace dev {
+
+// ---------------------------------------------------------------------------------------
+// Matrix chunk loads: CHUNK consecutive slots of one row, as one vector load through the
+// read-only path (the matrix never changes inside a kernel).
+// ---------------------------------------------------------------------------------------
+template <typename VT, int CHUNK>
+struct ChunkLoad;
+
+template <>
+struct ChunkLoad<float, 1> {
+    static __device__ __forceinline__ void run(const float* p, float* o) { o[0] = __ldg(p); }
+};
+template <>
+struct ChunkLoad<float, 2> {
+    static __device__ __forceinline__ void run(const float* p, float* o) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+        o[0] = v.x; o[1] = v.y;
+    }
+};
+template <>
+struct ChunkLoad<float, 4> {
+    static __device__ __forceinline__ void run(const float* p, float* o) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+template <>
+struct ChunkLoad<double, 1> {
+    static __device__ __forceinline__ void run(const double* p, double* o) { o[0] = __ldg(p); }
+};
+template <>
+struct ChunkLoad<double, 2> {
+    static __device__ __forceinline__ void run(const double* p, double* o) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+        o[0] = v.x; o[1] = v.y;
+    }
+};
+template <>
+struct ChunkLoad<double, 4> {
+    static __device__ __forceinline__ void run(const double* p, double* o) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+};
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+template <>
+struct ChunkLoad<__nv_bfloat16, 1> {
+    static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
+        const unsigned short v = __ldg(reinterpret_cast<const unsigned short*>(p));
+        o[0] = __uint_as_float(static_cast<uint32_t>(v) << 16);
+    }
+};
+template <>
+struct ChunkLoad<__nv_bfloat16, 2> {
+    static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
+        const uint32_t v = __ldg(reinterpret_cast<const unsigned int*>(p));
+        o[0] = bf16_lo(v); o[1] = bf16_hi(v);
+    }
+};
+template <>
+struct ChunkLoad<__nv_bfloat16, 4> {
+    static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+        o[0] = bf16_lo(v.x); o[1] = bf16_hi(v.x); o[2] = bf16_lo(v.y); o[3] = bf16_hi(v.y);
+    }
+};
+
+template <int CHUNK>
+struct ColLoad;
+template <>
+struct ColLoad<1> {
+    static __device__ __forceinline__ void run(const int* p, int* o) { o[0] = __ldg(p); }
+};
+template <>
+struct ColLoad<2> {
+    static __device__ __forceinline__ void run(const int* p, int* o) {
+        const int2 v = __ldg(reinterpret_cast<const int2*>(p));
+        o[0] = v.x; o[1] = v.y;
+    }
+};
+template <>
+struct ColLoad<4> {
+    static __device__ __forceinline__ void run(const int* p, int* o) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(p));
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+
+// The arithmetic type of a matrix value: bf16 values are widened to float.
+template <typename VT> struct ValArith { using type = VT; };
+template <> struct ValArith<__nv_bfloat16> { using type = float; };
+
+// ---------------------------------------------------------------------------------------
+// Reductions in FP64 with a fixed combination order (results identical in every block).
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums NV values per thread over the block; result valid in every thread.
+// scratch: at least 32 * NV doubles of shared memory.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) scratch[q * 32 + warp] = v[q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double t = lane < nwarps ? scratch[q * 32 + lane] : 0.0;
+        v[q] = warp_sum(t);
+    }
+}
+
+__device__ __forceinline__ long long globaltimer_ns() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_volatile_int(const int* p) {
+    return *reinterpret_cast<const volatile int*>(p);
+}
+
+// ---------------------------------------------------------------------------------------
+// Grid barrier for a cooperative (co-resident) launch.  The counter only grows: barrier k
+// completes when it reaches k * gridDim.x.  Every wait is bounded: after timeout_ns the
+// waiting block raises *err (1) and returns false; blocks that see *err set leave too, so
+// no block spins forever.  The fences on both sides give the acquire/release ordering that
+// makes plain global stores before the barrier visible to plain loads after it.
+// ---------------------------------------------------------------------------------------
+struct GridBarrier {
+    unsigned* counter;
+    int* err;
+    long long timeout_ns;
+    unsigned epoch;
+    int skip_block;  // test-only: this block withholds its arrival at the first barrier (-1: none)
+
+    __device__ __forceinline__ bool sync(int* s_flag) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            ++epoch;
+            const unsigned target = epoch * gridDim.x;
+            __threadfence();
+            if (!(static_cast<int>(blockIdx.x) == skip_block && epoch == 1u)) atomicAdd(counter, 1u);
+            int ok = 1;
+            if (ld_acquire_gpu(counter) < target) {
+                const long long t0 = globaltimer_ns();
+                unsigned spins = 0;
+                while (ld_acquire_gpu(counter) < target) {
+                    if ((++spins & 63u) == 0) {
+                        if (ld_volatile_int(err) != 0) { ok = 0; break; }
+                        if (globaltimer_ns() - t0 > timeout_ns) {
+                            atomicExch(err, 1);
+                            ok = 0;
+                            break;
+                        }
+                    }
+                }
+            }
+            __threadfence();
+            *s_flag = ok;
+        }
+        __syncthreads();
+        return *s_flag != 0;
+    }
+};
+
+}  // namespace dev
+}  // namespace xplus

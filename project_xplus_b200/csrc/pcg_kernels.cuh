@@ -1,0 +1,82 @@
+// pcg_kernels.cuh -- launch interface of the persistent Jacobi-PCG kernel and the SELL SpMV.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace xplus {
+
+// Device-side outcome of one persistent solve (written by block 0 at exit).
+struct PcgOut {
+    int status;        // XPLUS_CONVERGED .. XPLUS_BREAKDOWN (XPLUS_TIMEOUT is set by the host)
+    int iterations;
+    int replacements;
+    int stagnated;
+    double rz, rr, pap, alpha;
+    double true_rr;    // ||b - A x||^2 in FP64 at exit
+    double reserved;
+    long long t_start_ns, t_end_ns;
+};
+
+// Matrix + vectors + control of one persistent solve.  All vectors are in SELL order and
+// n_pad long; padding rows hold zeros and stay zero.
+struct PcgArgs {
+    int n, n_pad, n_slices;
+    const long long* slice_ptr;
+    const int* col;
+    const void* val;        // VT, slots
+    const double* val64;    // FP64 copy in the same layout (nullable)
+    const void* diag;       // XT, n_pad: diagonal when it is stored apart (DIAG=true)
+    const double* diag64;   // FP64 diagonal when apart (with val64)
+    const void* minv;       // XT, n_pad
+    const double* b64;
+    double* x64;            // FP64 solution accumulator (x0 on entry)
+    void* r;                // XT
+    void* p;                // XT
+    void* ap;               // XT
+    // optional M^-1 = G^T G (G and its transpose in SELL form over the same ordering)
+    const long long* g_slice_ptr; const int* g_col; const void* g_val;
+    const long long* gt_slice_ptr; const int* gt_col; const void* gt_val;
+    void* t;                // XT, n_pad: G r temporary
+    void* z;                // XT, n_pad: preconditioned residual (GTG mode only)
+    double* partial;        // 2 banks x 4 slots x gridDim.x
+    unsigned* bar;
+    int* err;
+    PcgOut* out;
+    double* trace;          // [trace_cap][5] alpha, beta, rz, rr, sqrt(rr) (nullable)
+    int trace_cap;
+    double tau_rr;          // stop when recurrence rr <= tau_rr (abs mode)
+    double tau_true_rr;     // >= 0: FP64 true-residual mode, stop when ||b-Ax||^2 <= this
+    int max_iters;
+    int replace_every;
+    double replace_drop;    // rr ratio that triggers a replacement (0: off)
+    long long timeout_ns;
+    int debug_skip_block;   // test-only fault injection: block that skips its first arrival
+};
+
+struct SpmvArgs {
+    int n_pad, n_slices;
+    const long long* slice_ptr;
+    const int* col;
+    const void* val;
+    const void* diag;       // DIAG only
+};
+
+// vt: XPLUS_F32/BF16/F64 ; xt: XPLUS_F32/F64 ; chunk 1/2/4 ; diag split ; gtg preconditioner
+struct KernelKey {
+    int vt, xt, chunk, diag, gtg;
+};
+
+// Occupancy-derived cooperative grid for the persistent kernel (blocks, threads).
+cudaError_t pcg_grid(const KernelKey& k, int device, int n_slices, int want_tpb, int want_bps,
+                     int* grid, int* tpb);
+cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s);
+cudaError_t spmv_launch(const KernelKey& k, const SpmvArgs& a, const void* x, void* y,
+                        cudaStream_t s);
+// dst[i] = (T) src[perm[i]] for i < n, 0 for n <= i < n_pad   (T per xt; f64 when xt==F64)
+cudaError_t gather_to_sell(int xt, const double* src, void* dst, const int* perm, int n, int n_pad,
+                           cudaStream_t s);
+// dst[perm[i]] = src[i]
+cudaError_t scatter_from_sell(const double* src, double* dst, const int* perm, int n,
+                              cudaStream_t s);
+
+}  // namespace xplus

@@ -1,0 +1,558 @@
+// solver.cu -- the single-system handle behind the C ABI: builds the SELL-C-sigma matrix,
+// keeps it and the solve vectors resident on one GPU, launches the persistent PCG kernel.
+//
+// Replaces the XRT host of the reference's single-launch solver
+// (host/cuper_control_xrt_host.cpp:163-337): there the host packs the 16-channel stream,
+// allocates 26 buffers and launches cuper_pcg_control_kernel once; here the host builds
+// SELL-C-sigma, uploads it once per handle and launches one cooperative kernel per solve.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "common.hpp"
+#include "pcg_kernels.cuh"
+
+struct xplus_pcg {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    xplus_opts opts{};
+    xplus::KernelKey key{};
+    int n = 0, n_pad = 0, n_slices = 0;
+    int64_t nnz = 0, slots = 0;
+    // device matrix
+    long long* d_slice_ptr = nullptr;
+    int* d_col = nullptr;
+    void* d_val = nullptr;
+    double* d_val64 = nullptr;
+    void* d_diag = nullptr;
+    double* d_diag64 = nullptr;
+    int* d_perm = nullptr;
+    // device vectors (SELL order, n_pad)
+    void* d_minv = nullptr;
+    double* d_b64 = nullptr;
+    double* d_x64 = nullptr;
+    void* d_r = nullptr;
+    void* d_p = nullptr;
+    void* d_ap = nullptr;
+    void* d_sx = nullptr;   // scratch SpMV in/out (vector type)
+    void* d_sy = nullptr;
+    // original-order FP64 staging
+    double* d_bio = nullptr;
+    double* d_xio = nullptr;
+    // control
+    double* d_partial = nullptr;
+    unsigned* d_bar = nullptr;
+    int* d_err = nullptr;
+    xplus::PcgOut* d_out = nullptr;
+    double* d_trace = nullptr;
+    int trace_cap = 0;
+    int grid = 0, tpb = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    xplus_metrics last{};
+    double last_bnorm2 = 0.0;
+    bool pending = false;
+    int debug_skip_block = -1;
+    std::vector<void*> allocations;
+};
+
+namespace xplus {
+namespace {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+template <typename T>
+T* dalloc(xplus_pcg* h, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    h->allocations.push_back(p);
+    return static_cast<T*>(p);
+}
+
+size_t elem_size(int t) { return t == XPLUS_F64 ? 8 : (t == XPLUS_BF16 ? 2 : 4); }
+
+void require_device(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, "no CUDA device available (the solver has no CPU path)");
+    }
+    require(device >= 0 && device < count, XPLUS_ERR_ARG, "device ordinal out of range");
+    cudaDeviceProp prop;
+    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    require(prop.major == 10, XPLUS_ERR_CUDA, "this build targets sm_100 (B200) devices only");
+    int coop = 0;
+    cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device), "attr");
+    require(coop != 0, XPLUS_ERR_CUDA, "device does not support cooperative launch");
+}
+
+// Converts FP64 values to the storage type into a host byte buffer.
+std::vector<unsigned char> convert(const std::vector<double>& v, int type) {
+    std::vector<unsigned char> out(v.size() * elem_size(type));
+    if (type == XPLUS_F64) {
+        std::memcpy(out.data(), v.data(), out.size());
+    } else if (type == XPLUS_F32) {
+        float* o = reinterpret_cast<float*>(out.data());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = static_cast<float>(v[i]);
+    } else {
+        __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(out.data());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = __double2bfloat16(v[i]);
+    }
+    return out;
+}
+
+double bf16_round(double v) { return static_cast<double>(__bfloat162float(__double2bfloat16(v))); }
+
+void destroy(xplus_pcg* h) {
+    if (!h) return;
+    if (h->device >= 0) cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocations) cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaGetLastError();
+    delete h;
+}
+
+void create(const int* row_ptr, const int* col_idx, const double* values, int n,
+            const xplus_opts* opts_in, xplus_pcg** out) {
+    require(row_ptr && col_idx && values && out, XPLUS_ERR_ARG, "null argument");
+    require(n > 0, XPLUS_ERR_ARG, "n must be positive");
+    const auto t0 = std::chrono::steady_clock::now();
+    xplus_opts o;
+    xplus_opts_default(&o);
+    if (opts_in) o = *opts_in;
+    require(o.value_type == XPLUS_F32 || o.value_type == XPLUS_BF16 || o.value_type == XPLUS_F64,
+            XPLUS_ERR_ARG, "bad value_type");
+    require(o.vector_type == XPLUS_F32 || o.vector_type == XPLUS_F64, XPLUS_ERR_ARG, "bad vector_type");
+    require(o.slice_height == 32, XPLUS_ERR_ARG, "slice_height must be 32");
+    require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
+    require(o.sigma >= 1, XPLUS_ERR_ARG, "sigma must be >= 1");
+    validate_csr(n, row_ptr, col_idx, row_ptr[n]);
+    std::vector<double> diag(static_cast<size_t>(n));
+    jacobi_diag(n, row_ptr, col_idx, values, diag.data());
+    for (int i = 0; i < n; ++i)
+        require(std::fabs(diag[static_cast<size_t>(i)]) > 1.0e-30, XPLUS_ERR_DATA,
+                "zero diagonal entry while building Jacobi inverse");
+    require_device(o.device);
+    cuda_check(cudaSetDevice(o.device), "cudaSetDevice");
+
+    const bool split = (o.value_type == XPLUS_BF16);  // bf16 keeps an exact diagonal apart
+    SellHost S;
+    sell_build(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+
+    auto* h = new xplus_pcg();
+    h->device = o.device;
+    try {
+        h->opts = o;
+        h->key = KernelKey{o.value_type, o.vector_type, o.chunk, split ? 1 : 0, 0};
+        h->n = n;
+        h->n_pad = S.n_pad;
+        h->n_slices = S.n_slices;
+        h->nnz = row_ptr[n];
+        h->slots = S.slots;
+        cuda_check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreate(&h->ev0), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&h->ev1), "cudaEventCreate");
+        const size_t np = static_cast<size_t>(S.n_pad);
+        const size_t xs = elem_size(o.vector_type);
+        h->d_slice_ptr = dalloc<long long>(h, S.slice_ptr.size());
+        h->d_col = dalloc<int>(h, static_cast<size_t>(S.slots));
+        h->d_val = dalloc<unsigned char>(h, static_cast<size_t>(S.slots) * elem_size(o.value_type));
+        h->d_perm = dalloc<int>(h, static_cast<size_t>(n));
+        h->d_minv = dalloc<unsigned char>(h, np * xs);
+        h->d_b64 = dalloc<double>(h, np);
+        h->d_x64 = dalloc<double>(h, np);
+        h->d_r = dalloc<unsigned char>(h, np * xs);
+        h->d_p = dalloc<unsigned char>(h, np * xs);
+        h->d_ap = dalloc<unsigned char>(h, np * xs);
+        h->d_sx = dalloc<unsigned char>(h, np * xs);
+        h->d_sy = dalloc<unsigned char>(h, np * xs);
+        h->d_bio = dalloc<double>(h, static_cast<size_t>(n));
+        h->d_xio = dalloc<double>(h, static_cast<size_t>(n));
+        h->d_bar = dalloc<unsigned>(h, 1);
+        h->d_err = dalloc<int>(h, 1);
+        h->d_out = dalloc<PcgOut>(h, 1);
+        cudaStream_t st = h->stream;
+        std::vector<long long> sp(S.slice_ptr.begin(), S.slice_ptr.end());
+        cuda_check(cudaMemcpyAsync(h->d_slice_ptr, sp.data(), sp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
+        cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+        cuda_check(cudaMemcpyAsync(h->d_perm, S.perm.data(), S.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+        std::vector<unsigned char> vbytes = convert(S.val, o.value_type);
+        cuda_check(cudaMemcpyAsync(h->d_val, vbytes.data(), vbytes.size(), cudaMemcpyHostToDevice, st), "H2D");
+        const bool keep64 = o.keep_fp64 != 0 && o.value_type != XPLUS_F64;
+        if (keep64) {
+            h->d_val64 = dalloc<double>(h, static_cast<size_t>(S.slots));
+            cuda_check(cudaMemcpyAsync(h->d_val64, S.val.data(), S.val.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+        } else if (o.value_type == XPLUS_F64) {
+            h->d_val64 = static_cast<double*>(h->d_val);
+        }
+        // Jacobi inverse in SELL order (host/pcg_common.hpp:42-54: m_inv = 1 / diag).
+        std::vector<double> dsell(np, 0.0), minv(np, 0.0);
+        for (int i = 0; i < n; ++i) dsell[static_cast<size_t>(i)] = diag[static_cast<size_t>(S.perm[static_cast<size_t>(i)])];
+        if (split) {
+            // The stored operator keeps an exact diagonal.  With row_sum_diag the diagonal
+            // also absorbs the rounding of its row's off-diagonals (a_ii + sum_j (a_ij -
+            // bf16(a_ij))), so A~ has A's row sums and A - A~ is a Laplacian of the
+            // per-edge rounding errors: spectrally |A - A~| <= 2^-8 |A| for M-matrices.
+            std::vector<double> dstore(dsell);
+            if (o.row_sum_diag) {
+                for (int s = 0; s < S.n_slices; ++s)
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int row = s * 32 + lane;
+                        if (row >= n) continue;
+                        const int64_t base = S.slice_ptr[static_cast<size_t>(s)];
+                        const int w = S.slice_width[static_cast<size_t>(s)];
+                        double corr = 0.0;
+                        for (int j = 0; j < w; ++j) {
+                            const int64_t pos = base + static_cast<int64_t>(j / o.chunk) * 32 * o.chunk + lane * o.chunk + (j % o.chunk);
+                            const double v = S.val[static_cast<size_t>(pos)];
+                            corr += v - bf16_round(v);
+                        }
+                        dstore[static_cast<size_t>(row)] += corr;
+                    }
+            }
+            std::vector<unsigned char> db = convert(dstore, o.vector_type);
+            h->d_diag = dalloc<unsigned char>(h, np * xs);
+            cuda_check(cudaMemcpyAsync(h->d_diag, db.data(), db.size(), cudaMemcpyHostToDevice, st), "H2D");
+            h->d_diag64 = dalloc<double>(h, np);
+            cuda_check(cudaMemcpyAsync(h->d_diag64, dsell.data(), np * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+            for (int i = 0; i < n; ++i) minv[static_cast<size_t>(i)] = 1.0 / dstore[static_cast<size_t>(i)];
+        } else {
+            for (int i = 0; i < n; ++i) minv[static_cast<size_t>(i)] = 1.0 / dsell[static_cast<size_t>(i)];
+        }
+        std::vector<unsigned char> mb = convert(minv, o.vector_type);
+        cuda_check(cudaMemcpyAsync(h->d_minv, mb.data(), mb.size(), cudaMemcpyHostToDevice, st), "H2D");
+        const int want_tpb = o.block_threads > 0 ? o.block_threads : 512;
+        cuda_check(pcg_grid(h->key, o.device, S.n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
+        h->d_partial = dalloc<double>(h, static_cast<size_t>(8) * h->grid);
+        cuda_check(cudaMemsetAsync(h->d_x64, 0, np * sizeof(double), st), "memset");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        h->last.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        *out = h;
+    } catch (...) {
+        destroy(h);
+        throw;
+    }
+}
+
+void ensure_trace(xplus_pcg* h, int cap) {
+    if (cap <= h->trace_cap) return;
+    if (h->d_trace) {
+        cudaFree(h->d_trace);
+        h->allocations.erase(std::remove(h->allocations.begin(), h->allocations.end(), static_cast<void*>(h->d_trace)), h->allocations.end());
+        h->d_trace = nullptr;
+    }
+    h->d_trace = dalloc<double>(h, static_cast<size_t>(cap) * 5);
+    h->trace_cap = cap;
+}
+
+// Enqueue one solve on stream st: b64/x64 already in SELL order on the device.
+void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, double bnorm2,
+                   int trace_rows, cudaStream_t st) {
+    require(tau > 0.0 && tau == tau, XPLUS_ERR_ARG, "tau must be positive");
+    require(tau_mode == XPLUS_TAU_ABS_RR || tau_mode == XPLUS_TAU_REL_TRUE, XPLUS_ERR_ARG, "bad tau_mode");
+    const int max_iters = max_iters_in > 0 ? max_iters_in : std::max(4 * h->n, 1000);
+    PcgArgs a{};
+    a.n = h->n;
+    a.n_pad = h->n_pad;
+    a.n_slices = h->n_slices;
+    a.slice_ptr = h->d_slice_ptr;
+    a.col = h->d_col;
+    a.val = h->d_val;
+    a.val64 = h->d_val64;
+    a.diag = h->d_diag;
+    a.diag64 = h->d_diag64;
+    a.minv = h->d_minv;
+    a.b64 = h->d_b64;
+    a.x64 = h->d_x64;
+    a.r = h->d_r;
+    a.p = h->d_p;
+    a.ap = h->d_ap;
+    a.partial = h->d_partial;
+    a.bar = h->d_bar;
+    a.err = h->d_err;
+    a.out = h->d_out;
+    a.trace = trace_rows > 0 ? h->d_trace : nullptr;
+    a.trace_cap = trace_rows;
+    a.max_iters = max_iters;
+    a.debug_skip_block = h->debug_skip_block;
+    a.timeout_ns = static_cast<long long>((h->opts.barrier_timeout_s > 0 ? h->opts.barrier_timeout_s : 2.0) * 1e9);
+    if (tau_mode == XPLUS_TAU_ABS_RR) {
+        a.tau_rr = tau;
+        a.tau_true_rr = -1.0;
+    } else {
+        require(h->d_val64 != nullptr, XPLUS_ERR_ARG, "TAU_REL_TRUE needs keep_fp64 (the FP64 matrix copy)");
+        a.tau_true_rr = tau * tau * bnorm2;
+        a.tau_rr = a.tau_true_rr;
+        a.replace_every = h->opts.replace_every;
+        a.replace_drop = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
+    }
+    cuda_check(cudaMemsetAsync(h->d_bar, 0, sizeof(unsigned), st), "memset");
+    cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
+    cuda_check(cudaMemsetAsync(h->d_out, 0, sizeof(PcgOut), st), "memset");
+    cuda_check(cudaEventRecord(h->ev0, st), "event");
+    cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st), "persistent PCG launch");
+    cuda_check(cudaEventRecord(h->ev1, st), "event");
+    h->last_bnorm2 = bnorm2;
+    h->pending = true;
+}
+
+void collect(xplus_pcg* h, xplus_metrics* m) {
+    if (h->pending) {
+        cuda_check(cudaEventSynchronize(h->ev1), "sync");
+        PcgOut o{};
+        int err = 0;
+        cuda_check(cudaMemcpy(&o, h->d_out, sizeof(PcgOut), cudaMemcpyDeviceToHost), "D2H");
+        cuda_check(cudaMemcpy(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        float ms = 0.0f;
+        cuda_check(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
+        xplus_metrics& L = h->last;
+        L.status = err ? XPLUS_TIMEOUT : o.status;
+        L.iterations = o.iterations;
+        L.replacements = o.replacements;
+        L.rz = o.rz;
+        L.rr = o.rr;
+        L.pap = o.pap;
+        L.alpha = o.alpha;
+        L.true_rel_residual = h->last_bnorm2 > 0 ? std::sqrt(o.true_rr / h->last_bnorm2) : std::sqrt(o.true_rr);
+        L.kernel_ms = ms;
+        L.reserved[0] = o.stagnated;
+        L.reserved[1] = static_cast<double>(o.t_end_ns - o.t_start_ns) * 1e-6;
+        h->pending = false;
+    }
+    if (m) *m = h->last;
+}
+
+}  // namespace
+}  // namespace xplus
+
+using namespace xplus;
+
+extern "C" {
+
+const char* xplus_version(void) { return "xplus-b200 0.1 (sm_100a)"; }
+
+void xplus_opts_default(xplus_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->value_type = XPLUS_F32;
+    o->vector_type = XPLUS_F32;
+    o->slice_height = 32;
+    o->sigma = 256;
+    o->chunk = 1;
+    o->keep_fp64 = 1;
+    o->replace_every = 0;
+    o->replace_drop = 0.0;
+    o->block_threads = 0;
+    o->blocks_per_sm = 0;
+    o->barrier_timeout_s = 2.0;
+    o->device = 0;
+    o->row_sum_diag = 1;
+}
+
+int xplus_device_count(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int good = 0;
+    for (int d = 0; d < count; ++d) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10) ++good;
+    }
+    cudaGetLastError();
+    return good;
+}
+
+int xplus_pcg_create(const int* row_ptr, const int* col_idx, const double* values, int n,
+                     const xplus_opts* opts, xplus_pcg** out) {
+    return guarded([&] { create(row_ptr, col_idx, values, n, opts, out); });
+}
+
+int xplus_pcg_destroy(xplus_pcg* h) {
+    return guarded([&] { destroy(h); });
+}
+
+int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau, int tau_mode,
+                    int max_iters, double* x_out, int* iters_out, double* resid_hist, int hist_len,
+                    xplus_metrics* metrics) {
+    return guarded([&] {
+        require(h && b && x_out, XPLUS_ERR_ARG, "null argument");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = h->stream;
+        const size_t nb = sizeof(double) * static_cast<size_t>(h->n);
+        double bnorm2 = 0.0;
+        for (int i = 0; i < h->n; ++i) bnorm2 += b[i] * b[i];
+        cuda_check(cudaMemcpyAsync(h->d_bio, b, nb, cudaMemcpyHostToDevice, st), "H2D");
+        if (x0) cuda_check(cudaMemcpyAsync(h->d_xio, x0, nb, cudaMemcpyHostToDevice, st), "H2D");
+        else cuda_check(cudaMemsetAsync(h->d_xio, 0, nb, st), "memset");
+        cuda_check(gather_to_sell(XPLUS_F64, h->d_bio, h->d_b64, h->d_perm, h->n, h->n_pad, st), "gather");
+        cuda_check(gather_to_sell(XPLUS_F64, h->d_xio, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");
+        const int rows = resid_hist && hist_len > 0 ? hist_len : 0;
+        if (rows > 0) ensure_trace(h, rows);
+        enqueue_solve(h, tau, tau_mode, max_iters, bnorm2, rows, st);
+        cuda_check(scatter_from_sell(h->d_x64, h->d_xio, h->d_perm, h->n, st), "scatter");
+        cuda_check(cudaMemcpyAsync(x_out, h->d_xio, nb, cudaMemcpyDeviceToHost, st), "D2H");
+        std::vector<double> tr;
+        if (rows > 0) {
+            tr.resize(static_cast<size_t>(rows) * 5);
+            cuda_check(cudaMemcpyAsync(tr.data(), h->d_trace, tr.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        }
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        xplus_metrics m;
+        collect(h, &m);
+        if (iters_out) *iters_out = m.iterations;
+        if (rows > 0)
+            for (int k = 0; k < rows; ++k) resid_hist[k] = k < m.iterations ? tr[static_cast<size_t>(k) * 5 + 4] : 0.0;
+        if (metrics) *metrics = m;
+    });
+}
+
+int xplus_pcg_last_trace(xplus_pcg* h, double* trace, int rows) {
+    return guarded([&] {
+        require(h && trace && rows > 0 && rows <= h->trace_cap, XPLUS_ERR_ARG, "bad trace request");
+        cuda_check(cudaMemcpy(trace, h->d_trace, static_cast<size_t>(rows) * 5 * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+    });
+}
+
+int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double tau, int tau_mode,
+                           int max_iters, void* stream) {
+    return guarded([&] {
+        require(h && d_b && d_x, XPLUS_ERR_ARG, "null argument");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+        cuda_check(gather_to_sell(XPLUS_F64, d_b, h->d_b64, h->d_perm, h->n, h->n_pad, st), "gather");
+        cuda_check(gather_to_sell(XPLUS_F64, d_x, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");
+        // ||b||^2 is needed for the relative test; it is taken by the kernel's exit
+        // residual only in absolute form, so the host supplies it from the last device b.
+        double bnorm2 = 0.0;
+        if (tau_mode == XPLUS_TAU_REL_TRUE) {
+            std::vector<double> hb(static_cast<size_t>(h->n));
+            cuda_check(cudaMemcpyAsync(hb.data(), d_b, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+            cuda_check(cudaStreamSynchronize(st), "sync");
+            for (double v : hb) bnorm2 += v * v;
+        }
+        enqueue_solve(h, tau, tau_mode, max_iters, bnorm2, 0, st);
+        cuda_check(scatter_from_sell(h->d_x64, d_x, h->d_perm, h->n, st), "scatter");
+    });
+}
+
+int xplus_pcg_debug_skip_arrival(xplus_pcg* h, int block) {
+    return guarded([&] {
+        require(h && block >= -1, XPLUS_ERR_ARG, "bad argument");
+        h->debug_skip_block = block;
+    });
+}
+
+int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics) {
+    return guarded([&] {
+        require(h && metrics, XPLUS_ERR_ARG, "null argument");
+        collect(h, metrics);
+    });
+}
+
+int xplus_pcg_spmv(xplus_pcg* h, const double* x, double* y) {
+    return guarded([&] {
+        require(h && x && y, XPLUS_ERR_ARG, "null argument");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = h->stream;
+        const size_t nb = sizeof(double) * static_cast<size_t>(h->n);
+        cuda_check(cudaMemcpyAsync(h->d_xio, x, nb, cudaMemcpyHostToDevice, st), "H2D");
+        cuda_check(gather_to_sell(h->opts.vector_type, h->d_xio, h->d_sx, h->d_perm, h->n, h->n_pad, st), "gather");
+        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_diag};
+        cuda_check(spmv_launch(h->key, a, h->d_sx, h->d_sy, st), "spmv");
+        // widen the SELL-order result to FP64 and scatter to original order
+        std::vector<unsigned char> ys(static_cast<size_t>(h->n_pad) * elem_size(h->opts.vector_type));
+        cuda_check(cudaMemcpyAsync(ys.data(), h->d_sy, ys.size(), cudaMemcpyDeviceToHost, st), "D2H");
+        std::vector<int> perm(static_cast<size_t>(h->n));
+        cuda_check(cudaMemcpyAsync(perm.data(), h->d_perm, perm.size() * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        for (int i = 0; i < h->n; ++i) {
+            const double v = h->opts.vector_type == XPLUS_F64 ? reinterpret_cast<double*>(ys.data())[i]
+                                                              : static_cast<double>(reinterpret_cast<float*>(ys.data())[i]);
+            y[perm[static_cast<size_t>(i)]] = v;
+        }
+    });
+}
+
+int xplus_pcg_spmv_device(xplus_pcg* h, const void* d_x, void* d_y, void* stream) {
+    return guarded([&] {
+        require(h && d_x && d_y, XPLUS_ERR_ARG, "null argument");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_diag};
+        cuda_check(spmv_launch(h->key, a, d_x, d_y, st), "spmv");
+    });
+}
+
+int xplus_pcg_info(xplus_pcg* h, int64_t* n, int64_t* n_pad, int64_t* nnz, int64_t* slots,
+                   int64_t* spmv_bytes) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        if (n) *n = h->n;
+        if (n_pad) *n_pad = h->n_pad;
+        if (nnz) *nnz = h->nnz;
+        if (slots) *slots = h->slots;
+        if (spmv_bytes)
+            *spmv_bytes = h->nnz * static_cast<int64_t>(elem_size(h->opts.value_type) + 4) +
+                          static_cast<int64_t>(h->n) * 2 * static_cast<int64_t>(elem_size(h->opts.vector_type));
+    });
+}
+
+int xplus_pcg_scratch_vectors(xplus_pcg* h, void** d_x, void** d_y) {
+    return guarded([&] {
+        require(h && d_x && d_y, XPLUS_ERR_ARG, "null argument");
+        *d_x = h->d_sx;
+        *d_y = h->d_sy;
+    });
+}
+
+int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double* x, double* r,
+                      double* z, double* p, double* ap, double* metrics, int* status, double tau,
+                      int max_iters, int n, void* stream) {
+    return guarded([&] {
+        require(h && b && x && metrics && status, XPLUS_ERR_ARG, "null argument");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+        (void)m_inv; (void)r; (void)z; (void)p; (void)ap;
+        // Parameter check of kernels/cuper_pcg_control_kernel.cpp:1078-1087.
+        if (n != h->n || n <= 0 || max_iters < 0 || !(tau > 0.0)) {
+            const int st_bad[2] = {XPLUS_BREAKDOWN, 0};
+            const double zero[4] = {0, 0, 0, 0};
+            cuda_check(cudaMemcpyAsync(status, st_bad, sizeof(st_bad), cudaMemcpyHostToDevice, st), "H2D");
+            cuda_check(cudaMemcpyAsync(metrics, zero, sizeof(zero), cudaMemcpyHostToDevice, st), "H2D");
+            cuda_check(cudaStreamSynchronize(st), "sync");
+            return;
+        }
+        cuda_check(gather_to_sell(XPLUS_F64, b, h->d_b64, h->d_perm, h->n, h->n_pad, st), "gather");
+        cuda_check(gather_to_sell(XPLUS_F64, x, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");
+        enqueue_solve(h, tau, XPLUS_TAU_ABS_RR, max_iters > 0 ? max_iters : std::max(4 * n, 1000), 0.0, 0, st);
+        cuda_check(scatter_from_sell(h->d_x64, x, h->d_perm, h->n, st), "scatter");
+        xplus_metrics m;
+        collect(h, &m);
+        const int st_out[2] = {m.status, m.iterations};
+        const double met[4] = {m.rz, m.rr, m.pap, m.alpha};
+        cuda_check(cudaMemcpyAsync(status, st_out, sizeof(st_out), cudaMemcpyHostToDevice, st), "H2D");
+        cuda_check(cudaMemcpyAsync(metrics, met, sizeof(met), cudaMemcpyHostToDevice, st), "H2D");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+    });
+}
+
+}  // extern "C"

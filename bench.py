@@ -222,7 +222,9 @@ def run_b200(args):
     n = d.n
     solver = xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=1, device=local)
     info = solver.info()
-    stream = torch.cuda.current_stream(dev)
+    # a real (non-default) stream: the library enqueues on exactly the stream the events see
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sp = C.c_void_p(stream.cuda_stream)
     b_dev = torch.from_numpy(d.b).to(dev)
     x_dev = torch.zeros(n, dtype=torch.float64, device=dev)

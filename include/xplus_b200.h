@@ -66,17 +66,28 @@ typedef struct xplus_opts {
     int vector_type;       /* XPLUS_F32 | XPLUS_F64: x, r, p, Ap storage in the inner loop */
     int slice_height;      /* SELL-C-sigma C; must be 32 */
     int sigma;             /* SELL sort window (rows); multiple of 32, or 1 for no sorting */
-    int chunk;             /* entries per row per vector load: 1, 2 or 4 */
+    int chunk;             /* entries per row per vector load: 1, 2 or 4 (default 4) */
     int keep_fp64;         /* keep an FP64 copy of A for true residuals (forced on for TAU_REL_TRUE) */
     int replace_every;     /* FP64 residual replacement every k iterations (0: only on stagnation
                               / at convergence) */
     double replace_drop;   /* also replace when ||r|| fell by this factor since the last
-                              replacement (e.g. 1e-4); 0 disables */
+                              replacement (default 1e-2); 0 disables.  With FP32 vectors the
+                              recurrence residual stalls near 1e-7 of its start, so TAU_REL_TRUE
+                              solves need a replacement before that point */
     int block_threads;     /* threads per CTA of the persistent kernel (0: auto) */
     int blocks_per_sm;     /* CTAs per SM (0: occupancy-derived) */
     double barrier_timeout_s; /* a grid barrier gives up after this long: status XPLUS_TIMEOUT */
     int device;            /* CUDA device ordinal */
-    int row_sum_diag;      /* BF16 values: rebuild the FP32 diagonal so Ã keeps A's row sums */
+    int row_sum_form;      /* FP32/BF16 values: store off-diagonal weights w_ij and row sums
+                              s_i = sum_j a_ij, and compute y_i = s_i x_i + sum_j w_ij (x_j - x_i)
+                              (default 1).  Rounding then perturbs each weight and each row sum
+                              relatively, so the stored operator stays spectrally close to A;
+                              rounding a_ii instead shifts the near-null space of a stiffness
+                              matrix and multiplies the iteration count */
+    int index16;           /* store columns as int16 offsets from the row when every |col - row|
+                              < 32768 after ordering (lossless; default 1) */
+    int l2_persist;        /* mark the matrix stream as persisting in L2 for the solve launch
+                              (default 1; sets this process's persisting-L2 limit) */
 } xplus_opts;
 
 typedef struct xplus_metrics {
@@ -126,6 +137,9 @@ int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau,
 int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double tau,
                            int tau_mode, int max_iters, void* stream);
 int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);
+/* Phase clock of the last solve, read from block 0's %globaltimer (ms, summed over the
+ * iterations): {phase A work, grid-barrier wait after A, phase B work, wait after B}. */
+int xplus_pcg_last_phase_times(xplus_pcg* h, double* ms4);
 /* Per-iteration trace of the last xplus_pcg_solve that asked for a history: rows x 5
  * doubles {alpha, beta, rz, rr, sqrt(rr)}, the fields of GoldenIterationTrace
  * (src/CgSolverGolden.hpp:15-22).  rows <= the hist_len of that solve. */
@@ -142,7 +156,8 @@ int xplus_pcg_spmv(xplus_pcg* h, const double* x, double* y);
  * enqueued on `stream`.  For bandwidth measurement. */
 int xplus_pcg_spmv_device(xplus_pcg* h, const void* d_x, void* d_y, void* stream);
 /* Sizes of the resident system: n, n_pad (SELL rows), nnz, stored slots (incl. padding),
- * and the algorithmic bytes of one SpMV (nnz*(s_val+4) + n*s_x + n*s_y). */
+ * and the bytes one SpMV must move in the stored format, padding excluded: stored entries x
+ * (value + index bytes) + n x (x read + y write [+ row sum in the row-sum form]). */
 int xplus_pcg_info(xplus_pcg* h, int64_t* n, int64_t* n_pad, int64_t* nnz, int64_t* slots,
                    int64_t* spmv_bytes);
 /* Device buffers of the SELL vectors (n_pad elements of the vector type), for tests and

@@ -76,24 +76,46 @@ struct ChunkLoad<__nv_bfloat16, 4> {
     }
 };
 
-template <int CHUNK>
+// Column loads: absolute int32 columns, or int16 offsets from the row (lossless when the
+// bandwidth of the ordered matrix is below 32768) returned as absolute columns.
+template <int CHUNK, typename IT>
 struct ColLoad;
 template <>
-struct ColLoad<1> {
-    static __device__ __forceinline__ void run(const int* p, int* o) { o[0] = __ldg(p); }
+struct ColLoad<1, int> {
+    static __device__ __forceinline__ void run(const int* p, int, int* o) { o[0] = __ldg(p); }
 };
 template <>
-struct ColLoad<2> {
-    static __device__ __forceinline__ void run(const int* p, int* o) {
+struct ColLoad<2, int> {
+    static __device__ __forceinline__ void run(const int* p, int, int* o) {
         const int2 v = __ldg(reinterpret_cast<const int2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
 template <>
-struct ColLoad<4> {
-    static __device__ __forceinline__ void run(const int* p, int* o) {
+struct ColLoad<4, int> {
+    static __device__ __forceinline__ void run(const int* p, int, int* o) {
         const int4 v = __ldg(reinterpret_cast<const int4*>(p));
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+__device__ __forceinline__ int lo16(uint32_t w) { return static_cast<int>(static_cast<short>(w & 0xFFFFu)); }
+__device__ __forceinline__ int hi16(uint32_t w) { return static_cast<int>(static_cast<short>(w >> 16)); }
+template <>
+struct ColLoad<1, short> {
+    static __device__ __forceinline__ void run(const short* p, int row, int* o) { o[0] = row + __ldg(p); }
+};
+template <>
+struct ColLoad<2, short> {
+    static __device__ __forceinline__ void run(const short* p, int row, int* o) {
+        const uint32_t v = __ldg(reinterpret_cast<const unsigned int*>(p));
+        o[0] = row + lo16(v); o[1] = row + hi16(v);
+    }
+};
+template <>
+struct ColLoad<4, short> {
+    static __device__ __forceinline__ void run(const short* p, int row, int* o) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+        o[0] = row + lo16(v.x); o[1] = row + hi16(v.x); o[2] = row + lo16(v.y); o[3] = row + hi16(v.y);
     }
 };
 
@@ -165,9 +187,12 @@ struct GridBarrier {
             ++epoch;
             const unsigned target = epoch * gridDim.x;
             __threadfence();
-            if (!(static_cast<int>(blockIdx.x) == skip_block && epoch == 1u)) atomicAdd(counter, 1u);
+            unsigned seen = target;  // a withheld arrival never completes the barrier
+            if (!(static_cast<int>(blockIdx.x) == skip_block && epoch == 1u)) seen = atomicAdd(counter, 1u) + 1u;
+            else seen = 0u;
             int ok = 1;
-            if (ld_acquire_gpu(counter) < target) {
+            // the last block to arrive sees the full count in its own atomic: no polling
+            if (seen < target && ld_acquire_gpu(counter) < target) {
                 const long long t0 = globaltimer_ns();
                 unsigned spins = 0;
                 while (ld_acquire_gpu(counter) < target) {

@@ -3,12 +3,12 @@
 //
 // One cooperative launch runs the whole solve.  Work is owned per SELL slice: warp w of
 // the grid owns slices w, w + W, w + 2W, ... and lane l of that warp owns row 32*s + l in
-// every phase, so the SpMV result Ap never leaves the thread that uses it and every vector
-// access is a coalesced 32-row segment.  Per iteration:
-//   phase A  Ap = A p (SELL, chunked vector loads), p.Ap partial   -> grid barrier
-//   phase B  x += alpha p (FP64), r -= alpha Ap, z = M^-1 r, r.z and r.r partials
-//                                                                    -> grid barrier
-//   phase C  p = z + beta p                                          -> grid barrier
+// every phase, so Ap is consumed by the thread that produced it and every vector access is
+// a coalesced 32-row segment.  Per iteration (two grid barriers):
+//   phase A  p' = z + beta p and Ap' (neighbours' p' recomputed from their {z, p} records,
+//            so p' needs no exchange of its own), p'.Ap' partial        -> grid barrier
+//   phase B  x += alpha p' (FP64), r -= alpha Ap', z = M^-1 r, r.z and r.r partials,
+//            record {z, p'}                                             -> grid barrier
 // Dot products are reduced in FP64 with a fixed order (warp tree, block tree, then the
 // per-block partials summed identically by every block), so every block takes the same
 // control decisions.  FP64 true residuals r = b - A x (FP64 matrix copy) replace the
@@ -36,15 +36,21 @@ template <> struct TypeOf<float> { static constexpr int id = XPLUS_F32; };
 template <> struct TypeOf<double> { static constexpr int id = XPLUS_F64; };
 template <> struct TypeOf<__nv_bfloat16> { static constexpr int id = XPLUS_BF16; };
 
-// Row `32*s + lane` of the SELL matrix times x, accumulated in AT.
-template <typename VT, int CHUNK, typename XV, typename AT>
+// Row `32*s + lane` of the SELL matrix times x, accumulated in AT.  With DIFF the slots hold
+// the off-diagonal weights w_ij only and the row computes sum_j w_ij (x_j - x_i); the caller
+// adds s_i x_i with the row sum s_i = sum_j a_ij.  That form is exact algebra, and it keeps
+// the operator a weighted graph Laplacian plus a diagonal when w and s are rounded to low
+// precision: every stored number carries only its own relative rounding error, whereas
+// rounding a_ii itself shifts the near-null space of a stiffness matrix.
+template <typename VT, int CHUNK, bool DIFF, typename IT, typename XV, typename AT>
 __device__ __forceinline__ AT sell_row(const long long* __restrict__ slice_ptr,
-                                       const int* __restrict__ col, const VT* __restrict__ val,
-                                       int s, int lane, const XV* x) {
+                                       const IT* __restrict__ col, const VT* __restrict__ val,
+                                       int s, int lane, const XV* x, AT xi) {
     const long long base = slice_ptr[s];
     const int w = static_cast<int>((slice_ptr[s + 1] - base) >> 5);
+    const int row = s * 32 + lane;
     const VT* vp = val + base + lane * CHUNK;
-    const int* cp = col + base + lane * CHUNK;
+    const IT* cp = col + base + lane * CHUNK;
     AT acc = AT(0);
     int c = 0;
     // two chunks in flight per step
@@ -52,14 +58,21 @@ __device__ __forceinline__ AT sell_row(const long long* __restrict__ slice_ptr,
         typename ValArith<VT>::type v0[CHUNK], v1[CHUNK];
         int c0[CHUNK], c1[CHUNK];
         ChunkLoad<VT, CHUNK>::run(vp, v0);
-        ColLoad<CHUNK>::run(cp, c0);
+        ColLoad<CHUNK, IT>::run(cp, row, c0);
         ChunkLoad<VT, CHUNK>::run(vp + 32 * CHUNK, v1);
-        ColLoad<CHUNK>::run(cp + 32 * CHUNK, c1);
+        ColLoad<CHUNK, IT>::run(cp + 32 * CHUNK, row, c1);
         AT xv0[CHUNK], xv1[CHUNK];
 #pragma unroll
         for (int q = 0; q < CHUNK; ++q) xv0[q] = static_cast<AT>(x[c0[q]]);
 #pragma unroll
         for (int q = 0; q < CHUNK; ++q) xv1[q] = static_cast<AT>(x[c1[q]]);
+        if (DIFF) {
+#pragma unroll
+            for (int q = 0; q < CHUNK; ++q) {
+                xv0[q] -= xi;
+                xv1[q] -= xi;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < CHUNK; ++q) acc += static_cast<AT>(v0[q]) * xv0[q];
 #pragma unroll
@@ -71,24 +84,31 @@ __device__ __forceinline__ AT sell_row(const long long* __restrict__ slice_ptr,
         typename ValArith<VT>::type v0[CHUNK];
         int c0[CHUNK];
         ChunkLoad<VT, CHUNK>::run(vp, v0);
-        ColLoad<CHUNK>::run(cp, c0);
+        ColLoad<CHUNK, IT>::run(cp, row, c0);
 #pragma unroll
-        for (int q = 0; q < CHUNK; ++q) acc += static_cast<AT>(v0[q]) * static_cast<AT>(x[c0[q]]);
+        for (int q = 0; q < CHUNK; ++q) {
+            AT xv = static_cast<AT>(x[c0[q]]);
+            if (DIFF) xv -= xi;
+            acc += static_cast<AT>(v0[q]) * xv;
+        }
     }
     return acc;
 }
 
-// FP64 row of A (FP64 copy when present, else the stored values widened) times x64.
-template <typename VT, typename XT, int CHUNK, bool DIAG>
+// FP64 row of A times x64: the FP64 copy when present (off-diagonals + exact diagonal in
+// the split layout), else the stored values widened.
+template <typename VT, typename XT, int CHUNK, bool DIFF, typename IT>
 __device__ __forceinline__ double row_fp64(const PcgArgs& a, int s, int lane, int row) {
+    const double xi = a.x64[row];
+    const IT* col = static_cast<const IT*>(a.col);
     double y;
     if (a.val64) {
-        y = sell_row<double, CHUNK, double, double>(a.slice_ptr, a.col, a.val64, s, lane, a.x64);
-        if (DIAG) y += a.diag64[row] * a.x64[row];
+        y = sell_row<double, CHUNK, false, IT, double, double>(a.slice_ptr, col, a.val64, s, lane, a.x64, 0.0);
+        if (DIFF) y += a.diag64[row] * xi;
     } else {
-        y = sell_row<VT, CHUNK, double, double>(a.slice_ptr, a.col, static_cast<const VT*>(a.val),
-                                                s, lane, a.x64);
-        if (DIAG) y += static_cast<double>(static_cast<const XT*>(a.diag)[row]) * a.x64[row];
+        y = sell_row<VT, CHUNK, DIFF, IT, double, double>(a.slice_ptr, col, static_cast<const VT*>(a.val),
+                                                          s, lane, a.x64, xi);
+        if (DIFF) y += static_cast<double>(static_cast<const XT*>(a.rowsum)[row]) * xi;
     }
     return y;
 }
@@ -118,23 +138,142 @@ __device__ __forceinline__ void publish(double (&v)[NV], double* s_red, double* 
 
 inline __device__ bool bad(double v) { return v != v; }
 
-template <typename VT, typename XT, int CHUNK, bool DIAG>
-__global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
+// What the SpMV needs from a neighbour j: z_j = M^-1 r_j and the previous search direction
+// p_j, packed so one 8-byte (FP32) or 16-byte (FP64) load fetches both.  The new direction
+// p'_j = z_j + beta p_j is recomputed by every reader with the same node_pnew(), so all copies
+// are bit-identical to the owner's; the owner stores {z_new, p'} only in phase B, after the
+// barrier that ends every read of the old pair, so one buffer suffices.
+template <typename XT>
+struct alignas(2 * sizeof(XT)) NodeRec {
+    XT z, p;
+};
+
+__device__ __forceinline__ float node_pnew(float z, float beta, float p) { return __fmaf_rn(beta, p, z); }
+__device__ __forceinline__ double node_pnew(double z, double beta, double p) { return __fma_rn(beta, p, z); }
+
+__device__ __forceinline__ NodeRec<float> load_rec(const NodeRec<float>* q) {
+    const float2 v = *reinterpret_cast<const float2*>(q);
+    return NodeRec<float>{v.x, v.y};
+}
+__device__ __forceinline__ NodeRec<double> load_rec(const NodeRec<double>* q) {
+    const double2 v = *reinterpret_cast<const double2*>(q);
+    return NodeRec<double>{v.x, v.y};
+}
+__device__ __forceinline__ void store_rec(NodeRec<float>* q, float z, float p) {
+    *reinterpret_cast<float2*>(q) = make_float2(z, p);
+}
+__device__ __forceinline__ void store_rec(NodeRec<double>* q, double z, double p) {
+    *reinterpret_cast<double2*>(q) = make_double2(z, p);
+}
+
+// NS slices of one warp at a time (lane = row within each): for every pair of chunks, the
+// value/column loads of all NS rows are issued, then all their neighbour-record gathers,
+// then the arithmetic -- so NS * 2 * CHUNK gathers per thread are in flight together.
+// Returns y_k = (A p')_row_k without the row-sum term; pi[k] = p'_row_k.
+template <typename VT, int CHUNK, bool DIFF, typename IT, typename XT, int NS>
+__device__ __forceinline__ void sell_rows_pnew(const int2 (&sl)[NS], const int (&row)[NS], int lane,
+                                               const IT* __restrict__ col, const VT* __restrict__ val,
+                                               const NodeRec<XT>* rec, XT beta, const XT (&pi)[NS],
+                                               XT (&y)[NS]) {
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        y[k] = XT(0);
+        wmax = max(wmax, sl[k].y);
+    }
+    for (int c = 0; c < wmax; c += 2 * CHUNK) {
+        typename ValArith<VT>::type v[NS][2][CHUNK];
+        int cc[NS][2][CHUNK];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (c + h * CHUNK < sl[k].y) {
+                    const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
+                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
+                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < CHUNK; ++q) {
+                        v[k][h][q] = 0;
+                        cc[k][h][q] = -1;
+                    }
+                }
+            }
+        NodeRec<XT> nb[NS][2][CHUNK];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q)
+                    nb[k][h][q] = cc[k][h][q] >= 0 ? load_rec(rec + cc[k][h][q]) : NodeRec<XT>{XT(0), XT(0)};
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q) {
+                    XT pj = node_pnew(nb[k][h][q].z, beta, nb[k][h][q].p);
+                    if (DIFF) pj -= pi[k];
+                    y[k] += static_cast<XT>(v[k][h][q]) * pj;
+                }
+    }
+}
+
+constexpr int kMaxSlicesPerBlock = 1024;  // shared slice table capacity (host checks the fit)
+constexpr int kSlicesInFlight = 2;
+
+// One iteration needs two grid barriers: the update p' = z + beta p is folded into the next
+// SpMV (each row recomputes its neighbours' p' from their records), so the search direction
+// is never exchanged through a barrier of its own.
+//   phase A  p'_i, Ap'_i (neighbours' p' recomputed), p'.Ap'   -> grid barrier
+//   phase B  x += alpha p' (FP64), r -= alpha Ap', z = M^-1 r, r.z, r.r, record {z, p'}
+//                                                               -> grid barrier
+// Block b owns the contiguous slice range [b*S, (b+1)*S): with a bandwidth-reducing order the
+// rows a block gathers from are mostly its own band, which stays in its L1.
+template <typename VT, typename XT, int CHUNK, bool DIFF, typename IT>
+__global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
+    constexpr int NS = kSlicesInFlight;
     __shared__ double s_red[32 * 3];
     __shared__ double s_tot[4];
     __shared__ int s_flag;
+    __shared__ int2 s_slice[kMaxSlicesPerBlock];  // {first slot, width} of the block's slices
+    __shared__ long long s_clk[6];
     GridBarrier bar{a.bar, a.err, a.timeout_ns, 0u, a.debug_skip_block};
     const int lane = threadIdx.x & 31;
-    const int gwarp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int nwarps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int per_block = (a.n_slices + gridDim.x - 1) / gridDim.x;
+    const int sb = blockIdx.x * per_block;
+    const int se = min(a.n_slices, sb + per_block);
     const VT* __restrict__ val = static_cast<const VT*>(a.val);
     const XT* __restrict__ minv = static_cast<const XT*>(a.minv);
-    const XT* __restrict__ diag = static_cast<const XT*>(a.diag);
+    const XT* __restrict__ rowsum = static_cast<const XT*>(a.rowsum);
+    NodeRec<XT>* rec = static_cast<NodeRec<XT>*>(a.rec);
     XT* r = static_cast<XT*>(a.r);
-    XT* p = static_cast<XT*>(a.p);
     XT* ap = static_cast<XT*>(a.ap);
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     const bool true_mode = a.tau_true_rr >= 0.0;
+    for (int k = threadIdx.x; k < se - sb; k += blockDim.x) {
+        const long long b0 = a.slice_ptr[sb + k];
+        s_slice[k] = make_int2(static_cast<int>(b0), static_cast<int>((a.slice_ptr[sb + k + 1] - b0) >> 5));
+    }
+    // phase clock of block 0 (globaltimer, in shared memory): work of phase A / B incl. the
+    // block reduction, and the grid-barrier waits after each.  Slot 5 is the last mark.
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 5; ++k) s_clk[k] = 0;
+        s_clk[5] = globaltimer_ns();
+        if (lead) a.out->t_start_ns = s_clk[5];
+    }
+    __syncthreads();
+    auto clock = [&](int slot) {
+        if (lead) {
+            const long long t = globaltimer_ns();
+            s_clk[slot] += t - s_clk[5];
+            s_clk[5] = t;
+        }
+    };
     // Two banks of 4 partial slots: consecutive publishes alternate banks, so a block that
     // runs ahead can never overwrite partials another block has not read yet (a barrier
     // separates any two publishes, and a bank is reused only two publishes later).
@@ -144,37 +283,38 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
         bank ^= 1;
         return b;
     };
-    double* cur = nullptr;
-    if (lead) a.out->t_start_ns = globaltimer_ns();
+    double* cur_bank = nullptr;
 
-    // ---- residual phase: r = b - A x (FP64), z = M^-1 r, optionally p = z ----
-    // partial slots: 0 = r.z, 1 = r.r (of the stored r), 2 = true r.r (FP64)
-    auto residual_phase = [&](bool set_p) {
+    // ---- residual phase: r = b - A x in FP64, stored rounded, z = M^-1 r into the record
+    //      (init also clears p); partials r.z, r.r, true r.r ----
+    auto residual_phase = [&](bool init) {
         double acc[3] = {0.0, 0.0, 0.0};
-        for (int s = gwarp; s < a.n_slices; s += nwarps) {
+        for (int s = sb + warp; s < se; s += wpb) {
             const int row = s * 32 + lane;
-            const double y = row_fp64<VT, XT, CHUNK, DIAG>(a, s, lane, row);
+            const double y = row_fp64<VT, XT, CHUNK, DIFF, IT>(a, s, lane, row);
             const double rt = a.b64[row] - y;
             const XT rv = static_cast<XT>(rt);
             const XT zv = minv[row] * rv;
             r[row] = rv;
-            if (set_p) p[row] = zv;
+            if (init) store_rec(rec + row, zv, XT(0));
+            else rec[row].z = zv;
             acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
             acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
             acc[2] += rt * rt;
         }
-        cur = next_bank();
-        publish<3>(acc, s_red, cur);
+        cur_bank = next_bank();
+        publish<3>(acc, s_red, cur_bank);
     };
 
     residual_phase(true);
     if (!bar.sync(&s_flag)) return;
-    grid_totals(cur, 3, s_tot);
+    grid_totals(cur_bank, 3, s_tot);
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     double rr_at_replace = rr, best_true = true_rr;
-    double pap = 0.0, alpha = 0.0;
+    double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
-    bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    clock(4);
 
     if (converged_now) {
         status = XPLUS_CONVERGED;
@@ -184,22 +324,43 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            // ---- phase A: Ap = A p, p.Ap ----
+            const XT be = static_cast<XT>(beta);
+            // ---- phase A: p' = z + beta p (own row), Ap' with recomputed neighbours, p'.Ap' ----
             {
                 double acc[1] = {0.0};
-                for (int s = gwarp; s < a.n_slices; s += nwarps) {
-                    const int row = s * 32 + lane;
-                    XT y = sell_row<VT, CHUNK, XT, XT>(a.slice_ptr, a.col, val, s, lane, p);
-                    const XT pv = p[row];
-                    if (DIAG) y += diag[row] * pv;
-                    ap[row] = y;
-                    acc[0] += static_cast<double>(pv) * static_cast<double>(y);
+                for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
+                    int2 sl[NS];
+                    int row[NS];
+                    XT pi[NS], y[NS];
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        const int s = s0 + k * wpb;
+                        const bool on = s < se;
+                        sl[k] = on ? s_slice[s - sb] : make_int2(0, 0);
+                        row[k] = on ? s * 32 + lane : -1;
+                    }
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        const NodeRec<XT> me = row[k] >= 0 ? load_rec(rec + row[k]) : NodeRec<XT>{XT(0), XT(0)};
+                        pi[k] = node_pnew(me.z, be, me.p);
+                    }
+                    sell_rows_pnew<VT, CHUNK, DIFF, IT, XT, NS>(sl, row, lane, static_cast<const IT*>(a.col), val,
+                                                                rec, be, pi, y);
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        if (row[k] < 0) continue;
+                        if (DIFF) y[k] += rowsum[row[k]] * pi[k];
+                        ap[row[k]] = y[k];
+                        acc[0] += static_cast<double>(pi[k]) * static_cast<double>(y[k]);
+                    }
                 }
-                cur = next_bank();
-                publish<1>(acc, s_red, cur);
+                cur_bank = next_bank();
+                publish<1>(acc, s_red, cur_bank);
             }
+            clock(0);
             if (!bar.sync(&s_flag)) return;
-            grid_totals(cur, 1, s_tot);
+            grid_totals(cur_bank, 1, s_tot);
+            clock(1);
             pap = s_tot[0];
             if (bad(pap) || fabs(pap) <= kBreakdownEps) {
                 status = XPLUS_BREAKDOWN;
@@ -211,25 +372,47 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            // ---- phase B: x, r, z and the two dots ----
+            // ---- phase B: x, r, z and the two dots; the record becomes {z_new, p'}; two
+            //      slices per step so the loads of both are in flight together ----
             {
                 double acc[2] = {0.0, 0.0};
                 const XT al = static_cast<XT>(alpha);
-                for (int s = gwarp; s < a.n_slices; s += nwarps) {
-                    const int row = s * 32 + lane;
-                    const XT pv = p[row];
-                    a.x64[row] += alpha * static_cast<double>(pv);
-                    const XT rv = r[row] - al * ap[row];
-                    const XT zv = minv[row] * rv;
-                    r[row] = rv;
-                    acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
-                    acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
+                for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
+                    int row[NS];
+                    NodeRec<XT> me[NS];
+                    XT apv[NS], rv0[NS], mv[NS];
+                    double xv[NS];
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        const int s = s0 + k * wpb;
+                        row[k] = s < se ? s * 32 + lane : -1;
+                        const int rr_ = row[k] >= 0 ? row[k] : s0 * 32 + lane;
+                        me[k] = load_rec(rec + rr_);
+                        apv[k] = ap[rr_];
+                        rv0[k] = r[rr_];
+                        mv[k] = minv[rr_];
+                        xv[k] = a.x64[rr_];
+                    }
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        if (row[k] < 0) continue;
+                        const XT pv = node_pnew(me[k].z, be, me[k].p);
+                        a.x64[row[k]] = xv[k] + alpha * static_cast<double>(pv);
+                        const XT rv = rv0[k] - al * apv[k];
+                        const XT zv = mv[k] * rv;
+                        r[row[k]] = rv;
+                        store_rec(rec + row[k], zv, pv);
+                        acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
+                        acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
+                    }
                 }
-                cur = next_bank();
-                publish<2>(acc, s_red, cur);
+                cur_bank = next_bank();
+                publish<2>(acc, s_red, cur_bank);
             }
+            clock(2);
             if (!bar.sync(&s_flag)) return;
-            grid_totals(cur, 2, s_tot);
+            grid_totals(cur_bank, 2, s_tot);
+            clock(3);
             double rz_new = s_tot[0], rr_new = s_tot[1];
             iterations = it + 1;
             if (bad(rz_new) || bad(rr_new)) {
@@ -247,7 +430,8 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
             if (do_replace) {
                 residual_phase(false);
                 if (!bar.sync(&s_flag)) return;
-                grid_totals(cur, 3, s_tot);
+                grid_totals(cur_bank, 3, s_tot);
+                clock(4);
                 rz_new = s_tot[0];
                 rr_new = s_tot[1];
                 true_rr = s_tot[2];
@@ -279,20 +463,11 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            const double beta = rz / rz_old;
+            beta = rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            // ---- phase C: p = z + beta p ----
-            {
-                const XT be = static_cast<XT>(beta);
-                for (int s = gwarp; s < a.n_slices; s += nwarps) {
-                    const int row = s * 32 + lane;
-                    p[row] = minv[row] * r[row] + be * p[row];
-                }
-            }
-            if (!bar.sync(&s_flag)) return;
         }
     }
     if (status == XPLUS_MAX_ITER && !true_mode && rr <= a.tau_rr) status = XPLUS_CONVERGED;
@@ -300,18 +475,18 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
     // ---- exit: FP64 true residual of the final x ----
     {
         double acc[1] = {0.0};
-        for (int s = gwarp; s < a.n_slices; s += nwarps) {
+        for (int s = sb + warp; s < se; s += wpb) {
             const int row = s * 32 + lane;
-            const double y = row_fp64<VT, XT, CHUNK, DIAG>(a, s, lane, row);
+            const double y = row_fp64<VT, XT, CHUNK, DIFF, IT>(a, s, lane, row);
             const double rt = a.b64[row] - y;
             acc[0] += rt * rt;
         }
-        cur = next_bank();
-        publish<1>(acc, s_red, cur);
+        cur_bank = next_bank();
+        publish<1>(acc, s_red, cur_bank);
     }
     if (!bar.sync(&s_flag)) return;
     if (blockIdx.x == 0) {
-        grid_totals(cur, 1, s_tot);
+        grid_totals(cur_bank, 1, s_tot);
         if (threadIdx.x == 0) {
             PcgOut* o = a.out;
             o->status = status;
@@ -324,19 +499,22 @@ __global__ void __launch_bounds__(512) pcg_persistent_kernel(PcgArgs a) {
             o->alpha = alpha;
             o->true_rr = s_tot[0];
             o->t_end_ns = globaltimer_ns();
+            for (int k = 0; k < 4; ++k) o->t_phase[k] = s_clk[k];
         }
     }
 }
 
-template <typename VT, typename XT, int CHUNK, bool DIAG>
+template <typename VT, typename XT, int CHUNK, bool DIFF, typename IT>
 __global__ void __launch_bounds__(256) sell_spmv_kernel(SpmvArgs a, const XT* __restrict__ x,
                                                         XT* __restrict__ y) {
     const int s = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (s >= a.n_slices) return;
     const int row = s * 32 + lane;
-    XT acc = sell_row<VT, CHUNK, XT, XT>(a.slice_ptr, a.col, static_cast<const VT*>(a.val), s, lane, x);
-    if (DIAG) acc += static_cast<const XT*>(a.diag)[row] * x[row];
+    const XT xi = x[row];
+    XT acc = sell_row<VT, CHUNK, DIFF, IT, XT, XT>(a.slice_ptr, static_cast<const IT*>(a.col),
+                                                   static_cast<const VT*>(a.val), s, lane, x, xi);
+    if (DIFF) acc += static_cast<const XT*>(a.rowsum)[row] * xi;
     y[row] = acc;
 }
 
@@ -353,19 +531,31 @@ __global__ void scatter_kernel(const double* __restrict__ src, double* __restric
     if (i < n) dst[perm[i]] = src[i];
 }
 
-// ---- dispatch over (value type, vector type, chunk, diag) ----
-template <typename XT, int CHUNK, bool DIAG, typename F>
+// ---- dispatch over (value type, vector type, chunk, row-sum form, index width) ----
+// Instantiated combinations: FP32 values in either form, BF16 values in the row-sum form only,
+// FP64 values in the plain form only.
+template <typename XT, int CHUNK, bool DIFF, typename IT, typename F>
 bool with_vt(int vt, F&& f) {
+    using C = std::integral_constant<int, CHUNK>;
+    using D = std::integral_constant<bool, DIFF>;
     switch (vt) {
-        case XPLUS_F32: f(static_cast<float*>(nullptr), static_cast<XT*>(nullptr), std::integral_constant<int, CHUNK>(), std::integral_constant<bool, DIAG>()); return true;
-        case XPLUS_BF16: f(static_cast<__nv_bfloat16*>(nullptr), static_cast<XT*>(nullptr), std::integral_constant<int, CHUNK>(), std::integral_constant<bool, DIAG>()); return true;
-        case XPLUS_F64: f(static_cast<double*>(nullptr), static_cast<XT*>(nullptr), std::integral_constant<int, CHUNK>(), std::integral_constant<bool, DIAG>()); return true;
+        case XPLUS_F32: f(static_cast<float*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true;
+        case XPLUS_BF16:
+            if constexpr (DIFF) { f(static_cast<__nv_bfloat16*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true; }
+            return false;
+        case XPLUS_F64:
+            if constexpr (!DIFF) { f(static_cast<double*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true; }
+            return false;
     }
     return false;
 }
+template <typename XT, int CHUNK, bool DIFF, typename F>
+bool with_idx(const KernelKey& k, F&& f) {
+    return k.idx16 ? with_vt<XT, CHUNK, DIFF, short>(k.vt, f) : with_vt<XT, CHUNK, DIFF, int>(k.vt, f);
+}
 template <typename XT, int CHUNK, typename F>
 bool with_diag(const KernelKey& k, F&& f) {
-    return k.diag ? with_vt<XT, CHUNK, true>(k.vt, f) : with_vt<XT, CHUNK, false>(k.vt, f);
+    return k.diag ? with_idx<XT, CHUNK, true>(k, f) : with_idx<XT, CHUNK, false>(k, f);
 }
 template <typename XT, typename F>
 bool with_chunk(const KernelKey& k, F&& f) {
@@ -393,11 +583,12 @@ cudaError_t pcg_grid(const KernelKey& k, int device, int n_slices, int want_tpb,
     if (e != cudaSuccess) return e;
     const int threads = want_tpb > 0 ? want_tpb : 512;
     int per_sm = 0;
-    const bool ok = dispatch(k, [&](auto* vt, auto* xt, auto chunk, auto diag) {
+    const bool ok = dispatch(k, [&](auto* vt, auto* xt, auto chunk, auto diag, auto* it) {
         using VT = std::remove_pointer_t<decltype(vt)>;
         using XT = std::remove_pointer_t<decltype(xt)>;
+        using IT = std::remove_pointer_t<decltype(it)>;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, pcg_persistent_kernel<VT, XT, decltype(chunk)::value, decltype(diag)::value>,
+            &per_sm, pcg_persistent_kernel<VT, XT, decltype(chunk)::value, decltype(diag)::value, IT>,
             threads, 0);
     });
     if (!ok) return cudaErrorInvalidValue;
@@ -408,21 +599,37 @@ cudaError_t pcg_grid(const KernelKey& k, int device, int n_slices, int want_tpb,
     const int warps_per_block = threads / 32;
     const int need = (n_slices + warps_per_block - 1) / warps_per_block;
     if (blocks > need) blocks = need > 0 ? need : 1;
+    // every block's contiguous slice range must fit its shared slice table
+    if ((n_slices + blocks - 1) / blocks > kMaxSlicesPerBlock) return cudaErrorInvalidConfiguration;
     *grid = blocks;
     *tpb = threads;
     return cudaSuccess;
 }
 
-cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s) {
+cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s,
+                       const cudaAccessPolicyWindow& window) {
     cudaError_t e = cudaErrorInvalidValue;
-    dispatch(k, [&](auto* vt, auto* xt, auto chunk, auto diag) {
+    dispatch(k, [&](auto* vt, auto* xt, auto chunk, auto diag, auto* it) {
         using VT = std::remove_pointer_t<decltype(vt)>;
         using XT = std::remove_pointer_t<decltype(xt)>;
-        void* args[] = {const_cast<PcgArgs*>(&a)};
-        e = cudaLaunchCooperativeKernel(
-            reinterpret_cast<const void*>(
-                pcg_persistent_kernel<VT, XT, decltype(chunk)::value, decltype(diag)::value>),
-            dim3(grid), dim3(tpb), args, 0, s);
+        using IT = std::remove_pointer_t<decltype(it)>;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(tpb);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[2];
+        int na = 0;
+        attr[na].id = cudaLaunchAttributeCooperative;
+        attr[na].val.cooperative = 1;
+        ++na;
+        if (window.num_bytes > 0) {
+            attr[na].id = cudaLaunchAttributeAccessPolicyWindow;
+            attr[na].val.accessPolicyWindow = window;
+            ++na;
+        }
+        cfg.attrs = attr;
+        cfg.numAttrs = na;
+        e = cudaLaunchKernelEx(&cfg, pcg_persistent_kernel<VT, XT, decltype(chunk)::value, decltype(diag)::value, IT>, a);
     });
     return e;
 }
@@ -430,12 +637,13 @@ cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, 
 cudaError_t spmv_launch(const KernelKey& k, const SpmvArgs& a, const void* x, void* y,
                         cudaStream_t s) {
     cudaError_t e = cudaErrorInvalidValue;
-    dispatch(k, [&](auto* vt, auto* xt, auto chunk, auto diag) {
+    dispatch(k, [&](auto* vt, auto* xt, auto chunk, auto diag, auto* it) {
         using VT = std::remove_pointer_t<decltype(vt)>;
         using XT = std::remove_pointer_t<decltype(xt)>;
+        using IT = std::remove_pointer_t<decltype(it)>;
         const int threads = 256;
         const int blocks = (a.n_slices * 32 + threads - 1) / threads;
-        sell_spmv_kernel<VT, XT, decltype(chunk)::value, decltype(diag)::value>
+        sell_spmv_kernel<VT, XT, decltype(chunk)::value, decltype(diag)::value, IT>
             <<<blocks, threads, 0, s>>>(a, static_cast<const XT*>(x), static_cast<XT*>(y));
         e = cudaGetLastError();
     });

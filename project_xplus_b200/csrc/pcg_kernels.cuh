@@ -15,6 +15,7 @@ struct PcgOut {
     double true_rr;    // ||b - A x||^2 in FP64 at exit
     double reserved;
     long long t_start_ns, t_end_ns;
+    long long t_phase[4];  // block 0: phase A work, barrier wait, phase B work, barrier wait (ns)
 };
 
 // Matrix + vectors + control of one persistent solve.  All vectors are in SELL order and
@@ -22,16 +23,16 @@ struct PcgOut {
 struct PcgArgs {
     int n, n_pad, n_slices;
     const long long* slice_ptr;
-    const int* col;
+    const void* col;        // int32 columns or int16 row offsets (KernelKey::idx16)
     const void* val;        // VT, slots
     const double* val64;    // FP64 copy in the same layout (nullable)
-    const void* diag;       // XT, n_pad: diagonal when it is stored apart (DIAG=true)
-    const double* diag64;   // FP64 diagonal when apart (with val64)
+    const void* rowsum;     // XT, n_pad: row sums s_i = sum_j a_ij (row-sum form only)
+    const double* diag64;   // FP64 diagonal when the slots hold off-diagonals only
     const void* minv;       // XT, n_pad
     const double* b64;
     double* x64;            // FP64 solution accumulator (x0 on entry)
+    void* rec;              // n_pad node records {z, p} of the vector type
     void* r;                // XT
-    void* p;                // XT
     void* ap;               // XT
     // optional M^-1 = G^T G (G and its transpose in SELL form over the same ordering)
     const long long* g_slice_ptr; const int* g_col; const void* g_val;
@@ -56,20 +57,23 @@ struct PcgArgs {
 struct SpmvArgs {
     int n_pad, n_slices;
     const long long* slice_ptr;
-    const int* col;
+    const void* col;
     const void* val;
-    const void* diag;       // DIAG only
+    const void* rowsum;     // row-sum form only
 };
 
-// vt: XPLUS_F32/BF16/F64 ; xt: XPLUS_F32/F64 ; chunk 1/2/4 ; diag split ; gtg preconditioner
+// vt: XPLUS_F32/BF16/F64 ; xt: XPLUS_F32/F64 ; chunk 1/2/4 ; diag = row-sum form ; gtg
+// preconditioner ; idx16 = int16 column offsets
 struct KernelKey {
-    int vt, xt, chunk, diag, gtg;
+    int vt, xt, chunk, diag, gtg, idx16;
 };
 
 // Occupancy-derived cooperative grid for the persistent kernel (blocks, threads).
 cudaError_t pcg_grid(const KernelKey& k, int device, int n_slices, int want_tpb, int want_bps,
                      int* grid, int* tpb);
-cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s);
+// window: L2 access-policy window for the matrix stream (num_bytes 0 = none)
+cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s,
+                       const cudaAccessPolicyWindow& window);
 cudaError_t spmv_launch(const KernelKey& k, const SpmvArgs& a, const void* x, void* y,
                         cudaStream_t s);
 // dst[i] = (T) src[perm[i]] for i < n, 0 for n <= i < n_pad   (T per xt; f64 when xt==F64)

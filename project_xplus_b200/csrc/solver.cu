@@ -27,18 +27,19 @@ struct xplus_pcg {
     int64_t nnz = 0, slots = 0;
     // device matrix
     long long* d_slice_ptr = nullptr;
-    int* d_col = nullptr;
+    void* d_col = nullptr;     // int32 columns or int16 row offsets, followed by the values
+    cudaAccessPolicyWindow window{};
     void* d_val = nullptr;
     double* d_val64 = nullptr;
-    void* d_diag = nullptr;
+    void* d_rowsum = nullptr;
     double* d_diag64 = nullptr;
     int* d_perm = nullptr;
     // device vectors (SELL order, n_pad)
     void* d_minv = nullptr;
     double* d_b64 = nullptr;
     double* d_x64 = nullptr;
+    void* d_rec = nullptr;  // node records {z, p}
     void* d_r = nullptr;
-    void* d_p = nullptr;
     void* d_ap = nullptr;
     void* d_sx = nullptr;   // scratch SpMV in/out (vector type)
     void* d_sy = nullptr;
@@ -58,6 +59,7 @@ struct xplus_pcg {
     double last_bnorm2 = 0.0;
     bool pending = false;
     int debug_skip_block = -1;
+    long long phase_ns[4] = {0, 0, 0, 0};
     std::vector<void*> allocations;
 };
 
@@ -116,8 +118,6 @@ std::vector<unsigned char> convert(const std::vector<double>& v, int type) {
     return out;
 }
 
-double bf16_round(double v) { return static_cast<double>(__bfloat162float(__double2bfloat16(v))); }
-
 void destroy(xplus_pcg* h) {
     if (!h) return;
     if (h->device >= 0) cudaSetDevice(h->device);
@@ -153,7 +153,11 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     require_device(o.device);
     cuda_check(cudaSetDevice(o.device), "cudaSetDevice");
 
-    const bool split = (o.value_type == XPLUS_BF16);  // bf16 keeps an exact diagonal apart
+    // Row-sum form for FP32/BF16 values: slots hold the off-diagonal weights, the row sums
+    // s_i = sum_j a_ij (FP64 sum) are kept apart in the vector type, and the FP64 diagonal
+    // stays apart for the true residual.
+    const bool split = (o.value_type != XPLUS_F64) && o.row_sum_form;
+    require(o.value_type != XPLUS_BF16 || split, XPLUS_ERR_ARG, "BF16 values need row_sum_form");
     SellHost S;
     sell_build(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
 
@@ -161,7 +165,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     h->device = o.device;
     try {
         h->opts = o;
-        h->key = KernelKey{o.value_type, o.vector_type, o.chunk, split ? 1 : 0, 0};
+        h->key = KernelKey{o.value_type, o.vector_type, o.chunk, split ? 1 : 0, 0, 0};
         h->n = n;
         h->n_pad = S.n_pad;
         h->n_slices = S.n_slices;
@@ -173,14 +177,56 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         const size_t np = static_cast<size_t>(S.n_pad);
         const size_t xs = elem_size(o.vector_type);
         h->d_slice_ptr = dalloc<long long>(h, S.slice_ptr.size());
-        h->d_col = dalloc<int>(h, static_cast<size_t>(S.slots));
-        h->d_val = dalloc<unsigned char>(h, static_cast<size_t>(S.slots) * elem_size(o.value_type));
+        // int16 offsets from the row when the ordered bandwidth allows (lossless)
+        bool idx16 = o.index16 != 0;
+        std::vector<short> col16;
+        if (idx16) {
+            col16.resize(static_cast<size_t>(S.slots));
+            for (int sl = 0; sl < S.n_slices && idx16; ++sl) {
+                const int64_t base = S.slice_ptr[static_cast<size_t>(sl)], end = S.slice_ptr[static_cast<size_t>(sl) + 1];
+                for (int64_t pos = base; pos < end; ++pos) {
+                    const int lane = static_cast<int>(((pos - base) % (32 * o.chunk)) / o.chunk);
+                    const int d = S.col[static_cast<size_t>(pos)] - (sl * 32 + lane);
+                    if (d < -32768 || d > 32767) {
+                        idx16 = false;
+                        break;
+                    }
+                    col16[static_cast<size_t>(pos)] = static_cast<short>(d);
+                }
+            }
+        }
+        h->key.idx16 = idx16 ? 1 : 0;
+        // columns and values in one allocation, so one L2 access-policy window covers both
+        const size_t col_bytes = (static_cast<size_t>(S.slots) * (idx16 ? 2 : 4) + 255) / 256 * 256;
+        const size_t val_bytes = static_cast<size_t>(S.slots) * elem_size(o.value_type);
+        unsigned char* mat = dalloc<unsigned char>(h, col_bytes + val_bytes);
+        h->d_col = mat;
+        h->d_val = mat + col_bytes;
+        if (o.l2_persist) {
+            int max_window = 0;
+            cudaDeviceProp prop;
+            cuda_check(cudaGetDeviceProperties(&prop, o.device), "props");
+            cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, o.device), "attr");
+            const size_t bytes = std::min(col_bytes + val_bytes, static_cast<size_t>(max_window));
+            size_t limit = 0;
+            cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+            const size_t want = std::min(bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
+            if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
+            cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+            if (bytes > 0 && limit > 0) {
+                h->window.base_ptr = mat;
+                h->window.num_bytes = bytes;
+                h->window.hitRatio = std::min(1.0f, static_cast<float>(limit) / static_cast<float>(bytes));
+                h->window.hitProp = cudaAccessPropertyPersisting;
+                h->window.missProp = cudaAccessPropertyStreaming;
+            }
+        }
         h->d_perm = dalloc<int>(h, static_cast<size_t>(n));
         h->d_minv = dalloc<unsigned char>(h, np * xs);
         h->d_b64 = dalloc<double>(h, np);
         h->d_x64 = dalloc<double>(h, np);
+        h->d_rec = dalloc<unsigned char>(h, np * xs * 2);
         h->d_r = dalloc<unsigned char>(h, np * xs);
-        h->d_p = dalloc<unsigned char>(h, np * xs);
         h->d_ap = dalloc<unsigned char>(h, np * xs);
         h->d_sx = dalloc<unsigned char>(h, np * xs);
         h->d_sy = dalloc<unsigned char>(h, np * xs);
@@ -192,7 +238,10 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         cudaStream_t st = h->stream;
         std::vector<long long> sp(S.slice_ptr.begin(), S.slice_ptr.end());
         cuda_check(cudaMemcpyAsync(h->d_slice_ptr, sp.data(), sp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
-        cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+        if (h->key.idx16)
+            cuda_check(cudaMemcpyAsync(h->d_col, col16.data(), col16.size() * sizeof(short), cudaMemcpyHostToDevice, st), "H2D");
+        else
+            cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(cudaMemcpyAsync(h->d_perm, S.perm.data(), S.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
         std::vector<unsigned char> vbytes = convert(S.val, o.value_type);
         cuda_check(cudaMemcpyAsync(h->d_val, vbytes.data(), vbytes.size(), cudaMemcpyHostToDevice, st), "H2D");
@@ -203,39 +252,26 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         } else if (o.value_type == XPLUS_F64) {
             h->d_val64 = static_cast<double*>(h->d_val);
         }
-        // Jacobi inverse in SELL order (host/pcg_common.hpp:42-54: m_inv = 1 / diag).
+        // Jacobi inverse in SELL order (host/pcg_common.hpp:42-54: m_inv = 1 / diag), from
+        // the exact FP64 diagonal.
         std::vector<double> dsell(np, 0.0), minv(np, 0.0);
-        for (int i = 0; i < n; ++i) dsell[static_cast<size_t>(i)] = diag[static_cast<size_t>(S.perm[static_cast<size_t>(i)])];
+        for (int i = 0; i < n; ++i) {
+            dsell[static_cast<size_t>(i)] = diag[static_cast<size_t>(S.perm[static_cast<size_t>(i)])];
+            minv[static_cast<size_t>(i)] = 1.0 / dsell[static_cast<size_t>(i)];
+        }
         if (split) {
-            // The stored operator keeps an exact diagonal.  With row_sum_diag the diagonal
-            // also absorbs the rounding of its row's off-diagonals (a_ii + sum_j (a_ij -
-            // bf16(a_ij))), so A~ has A's row sums and A - A~ is a Laplacian of the
-            // per-edge rounding errors: spectrally |A - A~| <= 2^-8 |A| for M-matrices.
-            std::vector<double> dstore(dsell);
-            if (o.row_sum_diag) {
-                for (int s = 0; s < S.n_slices; ++s)
-                    for (int lane = 0; lane < 32; ++lane) {
-                        const int row = s * 32 + lane;
-                        if (row >= n) continue;
-                        const int64_t base = S.slice_ptr[static_cast<size_t>(s)];
-                        const int w = S.slice_width[static_cast<size_t>(s)];
-                        double corr = 0.0;
-                        for (int j = 0; j < w; ++j) {
-                            const int64_t pos = base + static_cast<int64_t>(j / o.chunk) * 32 * o.chunk + lane * o.chunk + (j % o.chunk);
-                            const double v = S.val[static_cast<size_t>(pos)];
-                            corr += v - bf16_round(v);
-                        }
-                        dstore[static_cast<size_t>(row)] += corr;
-                    }
+            std::vector<double> rs(np, 0.0);
+            for (int i = 0; i < n; ++i) {
+                const int old = S.perm[static_cast<size_t>(i)];
+                double acc = 0.0;
+                for (int k = row_ptr[old]; k < row_ptr[old + 1]; ++k) acc += values[k];
+                rs[static_cast<size_t>(i)] = acc;
             }
-            std::vector<unsigned char> db = convert(dstore, o.vector_type);
-            h->d_diag = dalloc<unsigned char>(h, np * xs);
-            cuda_check(cudaMemcpyAsync(h->d_diag, db.data(), db.size(), cudaMemcpyHostToDevice, st), "H2D");
+            std::vector<unsigned char> rb = convert(rs, o.vector_type);
+            h->d_rowsum = dalloc<unsigned char>(h, np * xs);
+            cuda_check(cudaMemcpyAsync(h->d_rowsum, rb.data(), rb.size(), cudaMemcpyHostToDevice, st), "H2D");
             h->d_diag64 = dalloc<double>(h, np);
             cuda_check(cudaMemcpyAsync(h->d_diag64, dsell.data(), np * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
-            for (int i = 0; i < n; ++i) minv[static_cast<size_t>(i)] = 1.0 / dstore[static_cast<size_t>(i)];
-        } else {
-            for (int i = 0; i < n; ++i) minv[static_cast<size_t>(i)] = 1.0 / dsell[static_cast<size_t>(i)];
         }
         std::vector<unsigned char> mb = convert(minv, o.vector_type);
         cuda_check(cudaMemcpyAsync(h->d_minv, mb.data(), mb.size(), cudaMemcpyHostToDevice, st), "H2D");
@@ -277,13 +313,13 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     a.col = h->d_col;
     a.val = h->d_val;
     a.val64 = h->d_val64;
-    a.diag = h->d_diag;
+    a.rowsum = h->d_rowsum;
     a.diag64 = h->d_diag64;
     a.minv = h->d_minv;
     a.b64 = h->d_b64;
     a.x64 = h->d_x64;
+    a.rec = h->d_rec;
     a.r = h->d_r;
-    a.p = h->d_p;
     a.ap = h->d_ap;
     a.partial = h->d_partial;
     a.bar = h->d_bar;
@@ -308,7 +344,7 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_out, 0, sizeof(PcgOut), st), "memset");
     cuda_check(cudaEventRecord(h->ev0, st), "event");
-    cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st), "persistent PCG launch");
+    cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st, h->window), "persistent PCG launch");
     cuda_check(cudaEventRecord(h->ev1, st), "event");
     h->last_bnorm2 = bnorm2;
     h->pending = true;
@@ -335,6 +371,10 @@ void collect(xplus_pcg* h, xplus_metrics* m) {
         L.kernel_ms = ms;
         L.reserved[0] = o.stagnated;
         L.reserved[1] = static_cast<double>(o.t_end_ns - o.t_start_ns) * 1e-6;
+        h->phase_ns[0] = o.t_phase[0];
+        h->phase_ns[1] = o.t_phase[1];
+        h->phase_ns[2] = o.t_phase[2];
+        h->phase_ns[3] = o.t_phase[3];
         h->pending = false;
     }
     if (m) *m = h->last;
@@ -356,15 +396,17 @@ void xplus_opts_default(xplus_opts* o) {
     o->vector_type = XPLUS_F32;
     o->slice_height = 32;
     o->sigma = 256;
-    o->chunk = 1;
+    o->chunk = 4;
     o->keep_fp64 = 1;
     o->replace_every = 0;
-    o->replace_drop = 0.0;
+    o->replace_drop = 1.0e-2;
     o->block_threads = 0;
     o->blocks_per_sm = 0;
     o->barrier_timeout_s = 2.0;
     o->device = 0;
-    o->row_sum_diag = 1;
+    o->row_sum_form = 1;
+    o->index16 = 1;
+    o->l2_persist = 1;
 }
 
 int xplus_device_count(void) {
@@ -462,6 +504,14 @@ int xplus_pcg_debug_skip_arrival(xplus_pcg* h, int block) {
     });
 }
 
+int xplus_pcg_last_phase_times(xplus_pcg* h, double* ms4) {
+    return guarded([&] {
+        require(h && ms4, XPLUS_ERR_ARG, "null argument");
+        collect(h, nullptr);
+        for (int k = 0; k < 4; ++k) ms4[k] = static_cast<double>(h->phase_ns[k]) * 1e-6;
+    });
+}
+
 int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics) {
     return guarded([&] {
         require(h && metrics, XPLUS_ERR_ARG, "null argument");
@@ -477,7 +527,7 @@ int xplus_pcg_spmv(xplus_pcg* h, const double* x, double* y) {
         const size_t nb = sizeof(double) * static_cast<size_t>(h->n);
         cuda_check(cudaMemcpyAsync(h->d_xio, x, nb, cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(gather_to_sell(h->opts.vector_type, h->d_xio, h->d_sx, h->d_perm, h->n, h->n_pad, st), "gather");
-        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_diag};
+        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_rowsum};
         cuda_check(spmv_launch(h->key, a, h->d_sx, h->d_sy, st), "spmv");
         // widen the SELL-order result to FP64 and scatter to original order
         std::vector<unsigned char> ys(static_cast<size_t>(h->n_pad) * elem_size(h->opts.vector_type));
@@ -497,7 +547,7 @@ int xplus_pcg_spmv_device(xplus_pcg* h, const void* d_x, void* d_y, void* stream
     return guarded([&] {
         require(h && d_x && d_y, XPLUS_ERR_ARG, "null argument");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
-        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_diag};
+        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_rowsum};
         cuda_check(spmv_launch(h->key, a, d_x, d_y, st), "spmv");
     });
 }
@@ -510,9 +560,16 @@ int xplus_pcg_info(xplus_pcg* h, int64_t* n, int64_t* n_pad, int64_t* nnz, int64
         if (n_pad) *n_pad = h->n_pad;
         if (nnz) *nnz = h->nnz;
         if (slots) *slots = h->slots;
-        if (spmv_bytes)
-            *spmv_bytes = h->nnz * static_cast<int64_t>(elem_size(h->opts.value_type) + 4) +
-                          static_cast<int64_t>(h->n) * 2 * static_cast<int64_t>(elem_size(h->opts.vector_type));
+        if (spmv_bytes) {
+            // bytes of one SpMV in the stored format, padding excluded: every stored entry
+            // (value + column index), the row sums when kept apart, x read once, y written once
+            const bool split = h->key.diag != 0;
+            const int64_t entries = split ? h->nnz - h->n : h->nnz;
+            const int64_t sv = static_cast<int64_t>(elem_size(h->opts.value_type));
+            const int64_t si = h->key.idx16 ? 2 : 4;
+            const int64_t sx = static_cast<int64_t>(elem_size(h->opts.vector_type));
+            *spmv_bytes = entries * (sv + si) + static_cast<int64_t>(h->n) * (2 * sx + (split ? sx : 0));
+        }
     });
 }
 

@@ -161,9 +161,9 @@ class PcgSolver:
     """One SPD system resident on the GPU (xplus_pcg handle)."""
 
     def __init__(self, row_ptr, col_idx, values, *, values_dtype="f32", vector_dtype="f32",
-                 sigma=256, chunk=1, keep_fp64=True, replace_every=0, replace_drop=0.0,
+                 sigma=256, chunk=4, keep_fp64=True, replace_every=0, replace_drop=1e-2,
                  block_threads=0, blocks_per_sm=0, barrier_timeout_s=2.0, device=0,
-                 row_sum_diag=True):
+                 row_sum_form=True, index16=True, l2_persist=True):
         self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
         self.col_idx = np.ascontiguousarray(col_idx, np.int32)
         self.values = np.ascontiguousarray(values, np.float64)
@@ -172,7 +172,8 @@ class PcgSolver:
             value_type=_type(values_dtype), vector_type=_type(vector_dtype), sigma=sigma, chunk=chunk,
             keep_fp64=int(keep_fp64), replace_every=replace_every, replace_drop=replace_drop,
             block_threads=block_threads, blocks_per_sm=blocks_per_sm,
-            barrier_timeout_s=barrier_timeout_s, device=device, row_sum_diag=int(row_sum_diag))
+            barrier_timeout_s=barrier_timeout_s, device=device, row_sum_form=int(row_sum_form), index16=int(index16),
+            l2_persist=int(l2_persist))
         h = C.c_void_p()
         check(lib.xplus_pcg_create(ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), self.n,
                                    C.byref(self.opts), C.byref(h)))

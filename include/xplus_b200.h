@@ -194,6 +194,28 @@ void update_xrz_kernel(double* x, const double* p, double* r, const double* ap,
                        const double* m_inv, double* z, double* metrics, double alpha, int n);
 void update_p_kernel(const double* z, double* p, double beta, int n);
 
+/* No-allocation variant of update_xrz_kernel.  It has no counterpart in the reference.
+ *
+ * Some callers cannot call cudaMalloc: code that runs inside another framework's fixed
+ * device-memory budget, or a latency-critical loop where an allocation (which can
+ * synchronize the device, or fail under memory pressure) is not allowed.  This entry point
+ * allocates nothing.  Its only scratch, one FP64 pair per reduction block, is a 16 KiB array
+ * compiled into the library, which every GPU that loads the library holds until the process
+ * exits.  The caller still passes every input and output, as device pointers: x, r, z are
+ * updated as update_xrz_kernel updates them, and metrics[0..1] = {r.z, r.r} is written on
+ * the device.  The call is asynchronous on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream).
+ *   - The first call on each device looks the scratch array's device address up with
+ *     cudaGetSymbolAddress; make that first call before any stream capture.
+ *   - All calls share the one scratch array, which keeps the last call's contents: calls
+ *     that overlap on the GPU (other streams, other host threads) race; serialize them.
+ *   - n may be at most XPLUS_NOALLOC_MAX_N (1024 reduction blocks x 256 threads x 16
+ *     elements); a larger n returns XPLUS_ERR_ARG with a message and launches nothing. */
+#define XPLUS_NOALLOC_MAX_N 4194304
+int xplus_update_xrz_noalloc(double* x, const double* p, double* r, const double* ap,
+                             const double* m_inv, double* z, double* metrics, double alpha, int n,
+                             void* stream);
+
 /* ------------------------------------------------------------------------------------
  * Host-side data path (no GPU needed).
  * ------------------------------------------------------------------------------------ */

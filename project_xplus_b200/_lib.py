@@ -15,6 +15,7 @@ XPLUS_CONVERGED, XPLUS_MAX_ITER, XPLUS_BREAKDOWN, XPLUS_TIMEOUT = 0, 1, 2, 3
 XPLUS_OK, XPLUS_ERR_ARG, XPLUS_ERR_CUDA, XPLUS_ERR_DATA, XPLUS_ERR_IO, XPLUS_ERR_NOMEM = 0, 10, 11, 12, 13, 14
 XPLUS_F32, XPLUS_BF16, XPLUS_F64 = 0, 1, 2
 XPLUS_TAU_ABS_RR, XPLUS_TAU_REL_TRUE = 0, 1
+XPLUS_NOALLOC_MAX_N = 4194304
 
 STATUS_NAMES = {0: "converged", 1: "max_iter", 2: "breakdown", 3: "timeout"}
 
@@ -91,6 +92,7 @@ _SIGS = {
     "dot_kernel": (None, [_p, _p, _p, _i]),
     "update_xrz_kernel": (None, [_p, _p, _p, _p, _p, _p, _p, _d, _i]),
     "update_p_kernel": (None, [_p, _p, _d, _i]),
+    "xplus_update_xrz_noalloc": (_i, [_p, _p, _p, _p, _p, _p, _p, _d, _i, _p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.hpp"
@@ -231,6 +232,30 @@ void run_spmv(const int* row_ptr, const int* col_idx, const double* values, cons
     check(cudaStreamSynchronize(c.stream), "sync");
 }
 
+// ---- scratch of the no-allocation update_xrz variant ----
+// One FP64 pair (r.z, r.r) per block of the reduction, compiled into the library: every
+// device that loads the library holds these 16 KiB until the process exits.
+constexpr int kNoallocBlocks = 1024;
+static __device__ __align__(256) double g_noalloc_partial[2 * kNoallocBlocks];
+static_assert(kNoallocBlocks >= kMaxBlocks, "blocks_for() may use up to kMaxBlocks blocks");
+
+// Device address of g_noalloc_partial on the current device, looked up once per device.
+// In host code the symbol is only a host-side stand-in, so the kernels get this address.
+double* noalloc_scratch() {
+    static std::mutex mu;
+    static double* addr[64] = {};
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) throw Error(XPLUS_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> g(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        check(cudaGetSymbolAddress(&p, g_noalloc_partial), "cudaGetSymbolAddress");
+        addr[dev] = static_cast<double*>(p);
+    }
+    return addr[dev];
+}
+
 template <typename F>
 void abi_call(F&& f) {
     const int rc = guarded(f);
@@ -323,6 +348,24 @@ void update_xrz_kernel(double* x, const double* p, double* r, const double* ap,
         check(cudaGetLastError(), "update_xrz launch");
         unbind(c, ax); unbind(c, ar); unbind(c, az); unbind(c, amet);
         check(cudaStreamSynchronize(c.stream), "sync");
+    });
+}
+
+int xplus_update_xrz_noalloc(double* x, const double* p, double* r, const double* ap,
+                             const double* m_inv, double* z, double* metrics, double alpha, int n,
+                             void* stream) {
+    return guarded([&] {
+        require(n >= 0 && n <= XPLUS_NOALLOC_MAX_N, XPLUS_ERR_ARG,
+                "n exceeds the no-allocation limit of " + std::to_string(XPLUS_NOALLOC_MAX_N) + " rows");
+        require(metrics != nullptr && (n == 0 || (x && p && r && ap && m_inv && z)), XPLUS_ERR_ARG,
+                "null argument");
+        double* scratch = noalloc_scratch();
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        // at most kNoallocBlocks blocks, so the partials fit the fixed scratch
+        const int blocks = blocks_for(n);
+        vec_kernel<<<blocks, kThreads, 0, st>>>(2, n, alpha, x, p, r, ap, m_inv, z, nullptr, nullptr, scratch);
+        finish_kernel<<<1, kThreads, 0, st>>>(scratch, blocks, metrics, 2);
+        check(cudaGetLastError(), "update_xrz_noalloc launch");
     });
 }
 

@@ -23,7 +23,7 @@ def main() -> None:
     ap.add_argument("--spmv", type=int, default=5)
     ap.add_argument("--values", default="f32")
     ap.add_argument("--vectors", default="f32")
-    ap.add_argument("--chunk", type=int, default=1)
+    ap.add_argument("--chunk", type=int, default=4)
     a = ap.parse_args()
     d, _ = g.system_2d_large(a.grid)
     s = PcgSolver.from_dataset(d, values_dtype=a.values, vector_dtype=a.vectors, chunk=a.chunk)

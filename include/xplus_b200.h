@@ -88,6 +88,9 @@ typedef struct xplus_opts {
                               < 32768 after ordering (lossless; default 1) */
     int l2_persist;        /* mark the matrix stream as persisting in L2 for the solve launch
                               (default 1; sets this process's persisting-L2 limit) */
+    int resident;          /* FP32 vectors, row-sum form: use the SM-resident kernel (state and
+                              the search direction's band + halo in shared memory) when one CTA
+                              per SM holds it (default 1) */
 } xplus_opts;
 
 typedef struct xplus_metrics {

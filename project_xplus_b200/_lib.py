@@ -27,6 +27,7 @@ class XplusOpts(C.Structure):
         ("replace_every", C.c_int), ("replace_drop", C.c_double), ("block_threads", C.c_int),
         ("blocks_per_sm", C.c_int), ("barrier_timeout_s", C.c_double), ("device", C.c_int),
         ("row_sum_form", C.c_int), ("index16", C.c_int), ("l2_persist", C.c_int),
+        ("resident", C.c_int),
     ]
 
 

@@ -1,0 +1,203 @@
+// pcg_device.cuh -- device helpers shared by the persistent PCG kernels: SELL row products,
+// the FP64 residual row, deterministic grid reductions and the {z, p} node records.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/xplus_b200.h"
+#include "device_common.cuh"
+#include "pcg_kernels.cuh"
+
+namespace xplus {
+namespace dev {
+
+constexpr double kBreakdownEps = 1.0e-30;  // include/cg_common.hpp:13
+
+// Row `32*s + lane` of the SELL matrix times x, accumulated in AT.  With DIFF the slots hold
+// the off-diagonal weights w_ij only and the row computes sum_j w_ij (x_j - x_i); the caller
+// adds s_i x_i with the row sum s_i = sum_j a_ij.  That form is exact algebra, and it keeps
+// the operator a weighted graph Laplacian plus a diagonal when w and s are rounded to low
+// precision: every stored number carries only its own relative rounding error, whereas
+// rounding a_ii itself shifts the near-null space of a stiffness matrix.
+template <typename VT, int CHUNK, bool DIFF, typename IT, typename XV, typename AT>
+__device__ __forceinline__ AT sell_row(const long long* __restrict__ slice_ptr,
+                                       const IT* __restrict__ col, const VT* __restrict__ val,
+                                       int s, int lane, const XV* x, AT xi) {
+    const long long base = slice_ptr[s];
+    const int w = static_cast<int>((slice_ptr[s + 1] - base) >> 5);
+    const int row = s * 32 + lane;
+    const VT* vp = val + base + lane * CHUNK;
+    const IT* cp = col + base + lane * CHUNK;
+    AT acc = AT(0);
+    int c = 0;
+    // two chunks in flight per step
+    for (; c + 2 * CHUNK <= w; c += 2 * CHUNK) {
+        typename ValArith<VT>::type v0[CHUNK], v1[CHUNK];
+        int c0[CHUNK], c1[CHUNK];
+        ChunkLoad<VT, CHUNK>::run(vp, v0);
+        ColLoad<CHUNK, IT>::run(cp, row, c0);
+        ChunkLoad<VT, CHUNK>::run(vp + 32 * CHUNK, v1);
+        ColLoad<CHUNK, IT>::run(cp + 32 * CHUNK, row, c1);
+        AT xv0[CHUNK], xv1[CHUNK];
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) xv0[q] = static_cast<AT>(x[c0[q]]);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) xv1[q] = static_cast<AT>(x[c1[q]]);
+        if (DIFF) {
+#pragma unroll
+            for (int q = 0; q < CHUNK; ++q) {
+                xv0[q] -= xi;
+                xv1[q] -= xi;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) acc += static_cast<AT>(v0[q]) * xv0[q];
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) acc += static_cast<AT>(v1[q]) * xv1[q];
+        vp += 64 * CHUNK;
+        cp += 64 * CHUNK;
+    }
+    if (c < w) {
+        typename ValArith<VT>::type v0[CHUNK];
+        int c0[CHUNK];
+        ChunkLoad<VT, CHUNK>::run(vp, v0);
+        ColLoad<CHUNK, IT>::run(cp, row, c0);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) {
+            AT xv = static_cast<AT>(x[c0[q]]);
+            if (DIFF) xv -= xi;
+            acc += static_cast<AT>(v0[q]) * xv;
+        }
+    }
+    return acc;
+}
+
+// FP64 row of A times x64: the FP64 copy when present (off-diagonals + exact diagonal in
+// the split layout), else the stored values widened.
+template <typename VT, typename XT, int CHUNK, bool DIFF, typename IT>
+__device__ __forceinline__ double row_fp64(const PcgArgs& a, int s, int lane, int row) {
+    const double xi = a.x64[row];
+    const IT* col = static_cast<const IT*>(a.col);
+    double y;
+    if (a.val64) {
+        y = sell_row<double, CHUNK, false, IT, double, double>(a.slice_ptr, col, a.val64, s, lane, a.x64, 0.0);
+        if (DIFF) y += a.diag64[row] * xi;
+    } else {
+        y = sell_row<VT, CHUNK, DIFF, IT, double, double>(a.slice_ptr, col, static_cast<const VT*>(a.val),
+                                                          s, lane, a.x64, xi);
+        if (DIFF) y += static_cast<double>(static_cast<const XT*>(a.rowsum)[row]) * xi;
+    }
+    return y;
+}
+
+// Sum of the per-block partials of slot q (fixed order, same in every block).
+__device__ __forceinline__ void grid_totals(const double* partial, int nq, double* s_tot) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        for (int q = 0; q < nq; ++q) {
+            double v = 0.0;
+            for (int b = lane; b < static_cast<int>(gridDim.x); b += 32)
+                v += __ldcg(partial + static_cast<size_t>(q) * gridDim.x + b);
+            v = warp_sum(v);
+            if (lane == 0) s_tot[q] = v;
+        }
+    }
+    __syncthreads();
+}
+
+template <int NV>
+__device__ __forceinline__ void publish(double (&v)[NV], double* s_red, double* partial) {
+    block_sum<NV>(v, s_red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) partial[static_cast<size_t>(q) * gridDim.x + blockIdx.x] = v[q];
+}
+
+inline __device__ bool bad(double v) { return v != v; }
+
+// What the SpMV needs from a neighbour j: z_j = M^-1 r_j and the previous search direction
+// p_j, packed so one 8-byte (FP32) or 16-byte (FP64) load fetches both.  The new direction
+// p'_j = z_j + beta p_j is recomputed by every reader with the same node_pnew(), so all copies
+// are bit-identical to the owner's; the owner stores {z_new, p'} only in phase B, after the
+// barrier that ends every read of the old pair, so one buffer suffices.
+template <typename XT>
+struct alignas(2 * sizeof(XT)) NodeRec {
+    XT z, p;
+};
+
+__device__ __forceinline__ float node_pnew(float z, float beta, float p) { return __fmaf_rn(beta, p, z); }
+__device__ __forceinline__ double node_pnew(double z, double beta, double p) { return __fma_rn(beta, p, z); }
+
+__device__ __forceinline__ NodeRec<float> load_rec(const NodeRec<float>* q) {
+    const float2 v = *reinterpret_cast<const float2*>(q);
+    return NodeRec<float>{v.x, v.y};
+}
+__device__ __forceinline__ NodeRec<double> load_rec(const NodeRec<double>* q) {
+    const double2 v = *reinterpret_cast<const double2*>(q);
+    return NodeRec<double>{v.x, v.y};
+}
+__device__ __forceinline__ void store_rec(NodeRec<float>* q, float z, float p) {
+    *reinterpret_cast<float2*>(q) = make_float2(z, p);
+}
+__device__ __forceinline__ void store_rec(NodeRec<double>* q, double z, double p) {
+    *reinterpret_cast<double2*>(q) = make_double2(z, p);
+}
+
+// NS slices of one warp at a time (lane = row within each): for every pair of chunks, the
+// value/column loads of all NS rows are issued, then all their neighbour-record gathers,
+// then the arithmetic -- so NS * 2 * CHUNK gathers per thread are in flight together.
+// Returns y_k = (A p')_row_k without the row-sum term; pi[k] = p'_row_k.
+template <typename VT, int CHUNK, bool DIFF, typename IT, typename XT, int NS>
+__device__ __forceinline__ void sell_rows_pnew(const int2 (&sl)[NS], const int (&row)[NS], int lane,
+                                               const IT* __restrict__ col, const VT* __restrict__ val,
+                                               const NodeRec<XT>* rec, XT beta, const XT (&pi)[NS],
+                                               XT (&y)[NS]) {
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        y[k] = XT(0);
+        wmax = max(wmax, sl[k].y);
+    }
+    for (int c = 0; c < wmax; c += 2 * CHUNK) {
+        typename ValArith<VT>::type v[NS][2][CHUNK];
+        int cc[NS][2][CHUNK];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (c + h * CHUNK < sl[k].y) {
+                    const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
+                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
+                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < CHUNK; ++q) {
+                        v[k][h][q] = 0;
+                        cc[k][h][q] = -1;
+                    }
+                }
+            }
+        NodeRec<XT> nb[NS][2][CHUNK];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q)
+                    nb[k][h][q] = cc[k][h][q] >= 0 ? load_rec(rec + cc[k][h][q]) : NodeRec<XT>{XT(0), XT(0)};
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q) {
+                    XT pj = node_pnew(nb[k][h][q].z, beta, nb[k][h][q].p);
+                    if (DIFF) pj -= pi[k];
+                    y[k] += static_cast<XT>(v[k][h][q]) * pj;
+                }
+    }
+}
+
+
+}  // namespace dev
+}  // namespace xplus

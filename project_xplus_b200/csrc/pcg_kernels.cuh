@@ -52,6 +52,10 @@ struct PcgArgs {
     double replace_drop;    // rr ratio that triggers a replacement (0: off)
     long long timeout_ns;
     int debug_skip_block;   // test-only fault injection: block that skips its first arrival
+    // SM-resident kernel only: per-CTA shared window {first row, rows} of the search direction,
+    // and how often the FP32 solution increments are folded into x64
+    const int2* win;
+    int flush_every;
 };
 
 struct SpmvArgs {
@@ -74,6 +78,13 @@ cudaError_t pcg_grid(const KernelKey& k, int device, int n_slices, int want_tpb,
 // window: L2 access-policy window for the matrix stream (num_bytes 0 = none)
 cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s,
                        const cudaAccessPolicyWindow& window);
+// SM-resident variant (pcg_resident.cu): FP32 vectors in the row-sum form only.
+bool resident_supported(const KernelKey& k);
+int resident_max_slices();
+// Sets the dynamic shared-memory opt-in and reports whether one CTA per SM fits.
+cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, int tpb, bool* fits);
+cudaError_t resident_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, size_t smem_bytes,
+                            cudaStream_t s, const cudaAccessPolicyWindow& window);
 cudaError_t spmv_launch(const KernelKey& k, const SpmvArgs& a, const void* x, void* y,
                         cudaStream_t s);
 // dst[i] = (T) src[perm[i]] for i < n, 0 for n <= i < n_pad   (T per xt; f64 when xt==F64)

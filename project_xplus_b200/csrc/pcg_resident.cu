@@ -1,0 +1,447 @@
+// pcg_resident.cu -- the SM-resident persistent Jacobi-PCG kernel (FP32 vectors, row-sum form).
+//
+// One CTA per SM owns a contiguous band of rows [R0, R0 + nb).  Every iteration it copies the
+// records {z, p} of its band plus the bandwidth halo [W0, W0 + wn) into shared memory as the
+// new search direction p' = z + beta p, so the SpMV gathers p' from shared memory and the only
+// global stream of phase A is the matrix itself.  The per-row state that no other CTA reads --
+// r, Ap, the FP32 solution increment dx, M^-1 and the row sums -- lives in shared memory for
+// the whole solve; dx is folded into the FP64 solution x every `flush_every` iterations and
+// before every FP64 residual (which needs x of neighbouring rows).  Two grid barriers per
+// iteration, as in the global-memory kernel (pcg_kernels.cu), with the same control flow,
+// breakdown tests and status codes (kernels/cuper_pcg_control_kernel.cpp:1069-1235).
+//
+// Shared memory (floats): pw[wn] | r[nb] | ap[nb] | dx[nb] | minv[nb] | rowsum[nb].
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "../../include/xplus_b200.h"
+#include "device_common.cuh"
+#include "pcg_device.cuh"
+#include "pcg_kernels.cuh"
+
+namespace xplus {
+namespace {
+
+using namespace dev;
+
+constexpr int kResSlices = 1024;  // slice table capacity per CTA
+constexpr int kResNS = 4;         // slices of one warp in flight together in phase A
+
+// NS slices of one warp: all value/column loads of the group first (the only global traffic),
+// then the products with p' gathered from the shared-memory window.  y_k excludes s_i p'_i.
+template <typename VT, int CHUNK, typename IT, int NS>
+__device__ __forceinline__ void sell_rows_smem(const int2 (&sl)[NS], const int (&row)[NS], int lane,
+                                               const IT* __restrict__ col, const VT* __restrict__ val,
+                                               const float* pw, int w0, const float (&pi)[NS],
+                                               float (&y)[NS]) {
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        y[k] = 0.0f;
+        wmax = max(wmax, sl[k].y);
+    }
+    for (int c = 0; c < wmax; c += 2 * CHUNK) {
+        float v[NS][2][CHUNK];
+        int cc[NS][2][CHUNK];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (c + h * CHUNK < sl[k].y) {
+                    const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
+                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
+                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < CHUNK; ++q) {
+                        v[k][h][q] = 0.0f;
+                        cc[k][h][q] = row[k] >= 0 ? row[k] : w0;
+                    }
+                }
+            }
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q) y[k] += v[k][h][q] * (pw[cc[k][h][q] - w0] - pi[k]);
+    }
+}
+
+template <typename VT, int CHUNK, typename IT>
+__global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
+    constexpr int NS = kResNS;
+    extern __shared__ float smem[];
+    __shared__ double s_red[32 * 3];
+    __shared__ double s_tot[4];
+    __shared__ int s_flag;
+    __shared__ int2 s_slice[kResSlices];
+    __shared__ long long s_clk[6];
+    GridBarrier bar{a.bar, a.err, a.timeout_ns, 0u, a.debug_skip_block};
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int per_block = (a.n_slices + gridDim.x - 1) / gridDim.x;
+    const int sb = blockIdx.x * per_block;
+    const int se = min(a.n_slices, sb + per_block);
+    const int r0 = sb * 32;
+    const int nb = max(0, se - sb) * 32;
+    const int2 win = a.win[blockIdx.x];
+    const int w0 = win.x, wn = win.y;
+    float* pw = smem;
+    float* rv = pw + wn;
+    float* apv = rv + nb;
+    float* dxv = apv + nb;
+    float* mi = dxv + nb;
+    float* rsv = mi + nb;
+    const VT* __restrict__ val = static_cast<const VT*>(a.val);
+    const IT* __restrict__ col = static_cast<const IT*>(a.col);
+    const float* __restrict__ minv_g = static_cast<const float*>(a.minv);
+    const float* __restrict__ rowsum_g = static_cast<const float*>(a.rowsum);
+    NodeRec<float>* rec = static_cast<NodeRec<float>*>(a.rec);
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    const bool true_mode = a.tau_true_rr >= 0.0;
+    for (int k = threadIdx.x; k < se - sb; k += blockDim.x) {
+        const long long b0 = a.slice_ptr[sb + k];
+        s_slice[k] = make_int2(static_cast<int>(b0), static_cast<int>((a.slice_ptr[sb + k + 1] - b0) >> 5));
+    }
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        mi[t] = minv_g[r0 + t];
+        rsv[t] = rowsum_g[r0 + t];
+        dxv[t] = 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 5; ++k) s_clk[k] = 0;
+        s_clk[5] = globaltimer_ns();
+        if (lead) a.out->t_start_ns = s_clk[5];
+    }
+    __syncthreads();
+    auto clock = [&](int slot) {
+        if (lead) {
+            const long long t = globaltimer_ns();
+            s_clk[slot] += t - s_clk[5];
+            s_clk[5] = t;
+        }
+    };
+    int bank = 0;
+    auto next_bank = [&]() {
+        double* b = a.partial + static_cast<size_t>(bank) * 4 * gridDim.x;
+        bank ^= 1;
+        return b;
+    };
+    double* cur_bank = nullptr;
+
+    // x += dx for the band (FP64 accumulation of the FP32 increments), dx = 0
+    auto flush_dx = [&]() {
+        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+            a.x64[r0 + t] += static_cast<double>(dxv[t]);
+            dxv[t] = 0.0f;
+        }
+    };
+
+    // ---- residual phase: r = b - A x in FP64 (x of neighbours from global memory), rounded
+    //      into shared r; z = M^-1 r into the record (init also clears p) ----
+    auto residual_phase = [&](bool init) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int s = sb + warp; s < se; s += wpb) {
+            const int row = s * 32 + lane;
+            const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
+            const double rt = a.b64[row] - y;
+            const float r_ = static_cast<float>(rt);
+            const float z_ = mi[row - r0] * r_;
+            rv[row - r0] = r_;
+            if (init) store_rec(rec + row, z_, 0.0f);
+            else rec[row].z = z_;
+            acc[0] += static_cast<double>(r_) * static_cast<double>(z_);
+            acc[1] += static_cast<double>(r_) * static_cast<double>(r_);
+            acc[2] += rt * rt;
+        }
+        cur_bank = next_bank();
+        publish<3>(acc, s_red, cur_bank);
+    };
+
+    residual_phase(true);
+    if (!bar.sync(&s_flag)) return;
+    grid_totals(cur_bank, 3, s_tot);
+    double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
+    double rr_at_replace = rr, best_true = true_rr;
+    double pap = 0.0, alpha = 0.0, beta = 0.0;
+    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
+    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const int flush_every = a.flush_every > 0 ? a.flush_every : 16;
+    clock(4);
+
+    if (converged_now) {
+        status = XPLUS_CONVERGED;
+    } else {
+        for (int it = 0; it < a.max_iters; ++it) {
+            if (bad(rz) || bad(rr) || fabs(rz) <= kBreakdownEps) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            const float be = static_cast<float>(beta);
+            // ---- phase A: window p' = z + beta p, then Ap' from shared memory ----
+            {
+                for (int t = threadIdx.x; t < wn; t += blockDim.x) {
+                    const NodeRec<float> nr = load_rec(rec + w0 + t);
+                    pw[t] = node_pnew(nr.z, be, nr.p);
+                }
+                __syncthreads();
+                double acc[1] = {0.0};
+                for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
+                    int2 sl[NS];
+                    int row[NS];
+                    float pi[NS], y[NS];
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        const int s = s0 + k * wpb;
+                        const bool on = s < se;
+                        sl[k] = on ? s_slice[s - sb] : make_int2(0, 0);
+                        row[k] = on ? s * 32 + lane : -1;
+                        pi[k] = on ? pw[row[k] - w0] : 0.0f;
+                    }
+                    sell_rows_smem<VT, CHUNK, IT, NS>(sl, row, lane, col, val, pw, w0, pi, y);
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        if (row[k] < 0) continue;
+                        const int t = row[k] - r0;
+                        const float yy = y[k] + rsv[t] * pi[k];
+                        apv[t] = yy;
+                        acc[0] += static_cast<double>(pi[k]) * static_cast<double>(yy);
+                    }
+                }
+                cur_bank = next_bank();
+                publish<1>(acc, s_red, cur_bank);
+            }
+            clock(0);
+            if (!bar.sync(&s_flag)) return;
+            grid_totals(cur_bank, 1, s_tot);
+            clock(1);
+            pap = s_tot[0];
+            if (bad(pap) || fabs(pap) <= kBreakdownEps) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            const double rz_old = rz;
+            alpha = rz / pap;
+            if (bad(alpha)) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            // ---- phase B: dx += alpha p', r -= alpha Ap', z = M^-1 r, record {z, p'} ----
+            {
+                double acc[2] = {0.0, 0.0};
+                const float al = static_cast<float>(alpha);
+                const bool flush = (it + 1) % flush_every == 0;
+                for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+                    const float pv = pw[r0 + t - w0];
+                    const float d = __fmaf_rn(al, pv, dxv[t]);
+                    const float r_ = rv[t] - al * apv[t];
+                    const float z_ = mi[t] * r_;
+                    rv[t] = r_;
+                    if (flush) {
+                        a.x64[r0 + t] += static_cast<double>(d);
+                        dxv[t] = 0.0f;
+                    } else {
+                        dxv[t] = d;
+                    }
+                    store_rec(rec + r0 + t, z_, pv);
+                    acc[0] += static_cast<double>(r_) * static_cast<double>(z_);
+                    acc[1] += static_cast<double>(r_) * static_cast<double>(r_);
+                }
+                cur_bank = next_bank();
+                publish<2>(acc, s_red, cur_bank);
+            }
+            clock(2);
+            if (!bar.sync(&s_flag)) return;
+            grid_totals(cur_bank, 2, s_tot);
+            clock(3);
+            double rz_new = s_tot[0], rr_new = s_tot[1];
+            iterations = it + 1;
+            if (bad(rz_new) || bad(rr_new)) {
+                rz = rz_new;
+                rr = rr_new;
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            bool do_replace = false;
+            if (true_mode) {
+                if (rr_new <= a.tau_true_rr) do_replace = true;
+                if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
+                if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = true;
+            }
+            if (do_replace) {
+                flush_dx();
+                if (!bar.sync(&s_flag)) return;
+                residual_phase(false);
+                if (!bar.sync(&s_flag)) return;
+                grid_totals(cur_bank, 3, s_tot);
+                clock(4);
+                rz_new = s_tot[0];
+                rr_new = s_tot[1];
+                true_rr = s_tot[2];
+                ++replacements;
+                rr_at_replace = rr_new;
+                if (true_rr < 0.9 * best_true) {
+                    best_true = true_rr;
+                    stagnant = 0;
+                } else if (++stagnant >= 8) {
+                    stagnated = 1;
+                }
+            }
+            if (lead && a.trace && it < a.trace_cap) {
+                double* t = a.trace + 5 * static_cast<size_t>(it);
+                t[0] = alpha;
+                t[1] = rz_new / rz_old;
+                t[2] = rz_new;
+                t[3] = rr_new;
+                t[4] = sqrt(rr_new > 0.0 ? rr_new : 0.0);
+            }
+            rz = rz_new;
+            rr = rr_new;
+            if (true_mode ? (do_replace && true_rr <= a.tau_true_rr) : (rr <= a.tau_rr)) {
+                status = XPLUS_CONVERGED;
+                break;
+            }
+            if (stagnated) break;
+            if (fabs(rz_old) <= kBreakdownEps) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            beta = rz / rz_old;
+            if (bad(beta)) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+        }
+    }
+    if (status == XPLUS_MAX_ITER && !true_mode && rr <= a.tau_rr) status = XPLUS_CONVERGED;
+
+    // ---- exit: fold dx into x, then the FP64 true residual of the final x ----
+    flush_dx();
+    if (!bar.sync(&s_flag)) return;
+    {
+        double acc[1] = {0.0};
+        for (int s = sb + warp; s < se; s += wpb) {
+            const int row = s * 32 + lane;
+            const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
+            const double rt = a.b64[row] - y;
+            acc[0] += rt * rt;
+        }
+        cur_bank = next_bank();
+        publish<1>(acc, s_red, cur_bank);
+    }
+    if (!bar.sync(&s_flag)) return;
+    if (blockIdx.x == 0) {
+        grid_totals(cur_bank, 1, s_tot);
+        if (threadIdx.x == 0) {
+            PcgOut* o = a.out;
+            o->status = status;
+            o->iterations = iterations;
+            o->replacements = replacements;
+            o->stagnated = stagnated;
+            o->rz = rz;
+            o->rr = rr;
+            o->pap = pap;
+            o->alpha = alpha;
+            o->true_rr = s_tot[0];
+            o->t_end_ns = globaltimer_ns();
+            for (int k = 0; k < 4; ++k) o->t_phase[k] = s_clk[k];
+        }
+    }
+}
+
+template <typename F>
+bool resident_dispatch(const KernelKey& k, F&& f) {
+    if (k.xt != XPLUS_F32 || !k.diag || k.gtg) return false;
+    auto with_it = [&](auto* vt, auto chunk) {
+        if (k.idx16) f(vt, chunk, static_cast<short*>(nullptr));
+        else f(vt, chunk, static_cast<int*>(nullptr));
+        return true;
+    };
+    auto with_chunk = [&](auto* vt) {
+        switch (k.chunk) {
+            case 1: return with_it(vt, std::integral_constant<int, 1>());
+            case 2: return with_it(vt, std::integral_constant<int, 2>());
+            case 4: return with_it(vt, std::integral_constant<int, 4>());
+        }
+        return false;
+    };
+    if (k.vt == XPLUS_F32) return with_chunk(static_cast<float*>(nullptr));
+    if (k.vt == XPLUS_BF16) return with_chunk(static_cast<__nv_bfloat16*>(nullptr));
+    return false;
+}
+
+}  // namespace
+
+bool resident_supported(const KernelKey& k) {
+    return resident_dispatch(k, [](auto*, auto, auto*) {});
+}
+
+cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, int tpb, bool* fits) {
+    *fits = false;
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa{};
+    bool ok = resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
+        using VT = std::remove_pointer_t<decltype(vt)>;
+        using IT = std::remove_pointer_t<decltype(it)>;
+        e = cudaFuncGetAttributes(&fa, pcg_resident_kernel<VT, decltype(chunk)::value, IT>);
+    });
+    if (!ok) return cudaSuccess;
+    if (e != cudaSuccess) return e;
+    if (smem_bytes + fa.sharedSizeBytes > static_cast<size_t>(optin)) return cudaSuccess;
+    if (tpb > fa.maxThreadsPerBlock) return cudaSuccess;
+    resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
+        using VT = std::remove_pointer_t<decltype(vt)>;
+        using IT = std::remove_pointer_t<decltype(it)>;
+        e = cudaFuncSetAttribute(pcg_resident_kernel<VT, decltype(chunk)::value, IT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes));
+    });
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
+        using VT = std::remove_pointer_t<decltype(vt)>;
+        using IT = std::remove_pointer_t<decltype(it)>;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, pcg_resident_kernel<VT, decltype(chunk)::value, IT>, tpb, smem_bytes);
+    });
+    if (e != cudaSuccess) return e;
+    *fits = per_sm >= 1;
+    return cudaSuccess;
+}
+
+cudaError_t resident_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, size_t smem_bytes,
+                            cudaStream_t s, const cudaAccessPolicyWindow& window) {
+    cudaError_t e = cudaErrorInvalidValue;
+    resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
+        using VT = std::remove_pointer_t<decltype(vt)>;
+        using IT = std::remove_pointer_t<decltype(it)>;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(tpb);
+        cfg.dynamicSmemBytes = smem_bytes;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[2];
+        int na = 0;
+        attr[na].id = cudaLaunchAttributeCooperative;
+        attr[na].val.cooperative = 1;
+        ++na;
+        if (window.num_bytes > 0) {
+            attr[na].id = cudaLaunchAttributeAccessPolicyWindow;
+            attr[na].val.accessPolicyWindow = window;
+            ++na;
+        }
+        cfg.attrs = attr;
+        cfg.numAttrs = na;
+        e = cudaLaunchKernelEx(&cfg, pcg_resident_kernel<VT, decltype(chunk)::value, IT>, a);
+    });
+    return e;
+}
+
+int resident_max_slices() { return kResSlices; }
+
+}  // namespace xplus

@@ -54,6 +54,9 @@ struct xplus_pcg {
     double* d_trace = nullptr;
     int trace_cap = 0;
     int grid = 0, tpb = 0;
+    bool resident = false;     // SM-resident kernel (pcg_resident.cu)
+    size_t smem_bytes = 0;
+    int2* d_win = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     xplus_metrics last{};
     double last_bnorm2 = 0.0;
@@ -276,7 +279,45 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         std::vector<unsigned char> mb = convert(minv, o.vector_type);
         cuda_check(cudaMemcpyAsync(h->d_minv, mb.data(), mb.size(), cudaMemcpyHostToDevice, st), "H2D");
         const int want_tpb = o.block_threads > 0 ? o.block_threads : 512;
-        cuda_check(pcg_grid(h->key, o.device, S.n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
+        // SM-resident kernel when its shared-memory band + halo fits one CTA per SM
+        if (o.resident && resident_supported(h->key)) {
+            int sms = 0;
+            cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device), "attr");
+            const int grid = sms;
+            const int per_block = (S.n_slices + grid - 1) / grid;
+            if (per_block <= resident_max_slices()) {
+                std::vector<int2> win(static_cast<size_t>(grid));
+                int max_wn = 0, max_nb = 0;
+                for (int b = 0; b < grid; ++b) {
+                    const int sb = b * per_block, se = std::min(S.n_slices, sb + per_block);
+                    if (se <= sb) {
+                        win[static_cast<size_t>(b)] = make_int2(0, 0);
+                        continue;
+                    }
+                    int lo = sb * 32, hi = se * 32;
+                    for (int64_t pos = S.slice_ptr[static_cast<size_t>(sb)]; pos < S.slice_ptr[static_cast<size_t>(se)]; ++pos) {
+                        lo = std::min(lo, S.col[static_cast<size_t>(pos)]);
+                        hi = std::max(hi, S.col[static_cast<size_t>(pos)] + 1);
+                    }
+                    win[static_cast<size_t>(b)] = make_int2(lo, hi - lo);
+                    max_wn = std::max(max_wn, hi - lo);
+                    max_nb = std::max(max_nb, (se - sb) * 32);
+                }
+                const size_t smem = sizeof(float) * (static_cast<size_t>(max_wn) + 5 * static_cast<size_t>(max_nb));
+                bool fits = false;
+                cuda_check(resident_prepare(h->key, o.device, smem, want_tpb, &fits), "resident_prepare");
+                if (fits) {
+                    h->resident = true;
+                    h->smem_bytes = smem;
+                    h->grid = grid;
+                    h->tpb = want_tpb;
+                    h->d_win = dalloc<int2>(h, win.size());
+                    cuda_check(cudaMemcpyAsync(h->d_win, win.data(), win.size() * sizeof(int2), cudaMemcpyHostToDevice, st), "H2D");
+                }
+            }
+        }
+        if (!h->resident)
+            cuda_check(pcg_grid(h->key, o.device, S.n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
         h->d_partial = dalloc<double>(h, static_cast<size_t>(8) * h->grid);
         cuda_check(cudaMemsetAsync(h->d_x64, 0, np * sizeof(double), st), "memset");
         cuda_check(cudaStreamSynchronize(st), "sync");
@@ -329,6 +370,8 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     a.trace_cap = trace_rows;
     a.max_iters = max_iters;
     a.debug_skip_block = h->debug_skip_block;
+    a.win = h->d_win;
+    a.flush_every = 16;
     a.timeout_ns = static_cast<long long>((h->opts.barrier_timeout_s > 0 ? h->opts.barrier_timeout_s : 2.0) * 1e9);
     if (tau_mode == XPLUS_TAU_ABS_RR) {
         a.tau_rr = tau;
@@ -344,7 +387,10 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_out, 0, sizeof(PcgOut), st), "memset");
     cuda_check(cudaEventRecord(h->ev0, st), "event");
-    cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st, h->window), "persistent PCG launch");
+    if (h->resident)
+        cuda_check(resident_launch(h->key, a, h->grid, h->tpb, h->smem_bytes, st, h->window), "resident PCG launch");
+    else
+        cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st, h->window), "persistent PCG launch");
     cuda_check(cudaEventRecord(h->ev1, st), "event");
     h->last_bnorm2 = bnorm2;
     h->pending = true;
@@ -407,6 +453,7 @@ void xplus_opts_default(xplus_opts* o) {
     o->row_sum_form = 1;
     o->index16 = 1;
     o->l2_persist = 1;
+    o->resident = 1;
 }
 
 int xplus_device_count(void) {

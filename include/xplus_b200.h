@@ -91,6 +91,9 @@ typedef struct xplus_opts {
     int resident;          /* FP32 vectors, row-sum form: use the SM-resident kernel (state and
                               the search direction's band + halo in shared memory) when one CTA
                               per SM holds it (default 1) */
+    int barriers_per_iter; /* SM-resident kernel: 1 (default) folds both dot products into one
+                              reduction by expanding r_{k+1}.z_{k+1} and r_{k+1}.r_{k+1} in alpha;
+                              2 reduces them after the update as the reference does */
 } xplus_opts;
 
 typedef struct xplus_metrics {
@@ -143,6 +146,9 @@ int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);
 /* Phase clock of the last solve, read from block 0's %globaltimer (ms, summed over the
  * iterations): {phase A work, grid-barrier wait after A, phase B work, wait after B}. */
 int xplus_pcg_last_phase_times(xplus_pcg* h, double* ms4);
+/* The same phase clock for every CTA of the last solve: ms[4*b + k], k as above; *blocks is
+ * the grid size (pass ms = NULL to query it). */
+int xplus_pcg_last_block_times(xplus_pcg* h, double* ms, int max_blocks, int* blocks);
 /* Per-iteration trace of the last xplus_pcg_solve that asked for a history: rows x 5
  * doubles {alpha, beta, rz, rr, sqrt(rr)}, the fields of GoldenIterationTrace
  * (src/CgSolverGolden.hpp:15-22).  rows <= the hist_len of that solve. */

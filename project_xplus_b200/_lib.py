@@ -27,7 +27,7 @@ class XplusOpts(C.Structure):
         ("replace_every", C.c_int), ("replace_drop", C.c_double), ("block_threads", C.c_int),
         ("blocks_per_sm", C.c_int), ("barrier_timeout_s", C.c_double), ("device", C.c_int),
         ("row_sum_form", C.c_int), ("index16", C.c_int), ("l2_persist", C.c_int),
-        ("resident", C.c_int),
+        ("resident", C.c_int), ("barriers_per_iter", C.c_int),
     ]
 
 
@@ -72,6 +72,7 @@ _SIGS = {
     "xplus_pcg_last_trace": (_i, [_p, _p, _i]),
     "xplus_pcg_debug_skip_arrival": (_i, [_p, _i]),
     "xplus_pcg_last_phase_times": (_i, [_p, _p]),
+    "xplus_pcg_last_block_times": (_i, [_p, _p, _i, _ip]),
     "xplus_pcg_spmv": (_i, [_p, _p, _p]),
     "xplus_pcg_spmv_device": (_i, [_p, _p, _p, _p]),
     "xplus_pcg_info": (_i, [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),

@@ -90,17 +90,26 @@ __device__ __forceinline__ double row_fp64(const PcgArgs& a, int s, int lane, in
     return y;
 }
 
-// Sum of the per-block partials of slot q (fixed order, same in every block).
+// Sum of the per-block partials of each slot q < nq (fixed order, same in every block).  Warp
+// q sums slot q, and each lane issues all its loads before adding, so the whole reduction is
+// one L2 round trip however many slots there are (nq <= number of warps).
 __device__ __forceinline__ void grid_totals(const double* partial, int nq, double* s_tot) {
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        for (int q = 0; q < nq; ++q) {
-            double v = 0.0;
-            for (int b = lane; b < static_cast<int>(gridDim.x); b += 32)
-                v += __ldcg(partial + static_cast<size_t>(q) * gridDim.x + b);
-            v = warp_sum(v);
-            if (lane == 0) s_tot[q] = v;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < nq) {
+        const double* src = partial + static_cast<size_t>(warp) * gridDim.x;
+        double v = 0.0;
+        for (int base = 0; base < static_cast<int>(gridDim.x); base += 256) {
+            double t[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int b = base + lane + 32 * k;
+                t[k] = b < static_cast<int>(gridDim.x) ? __ldcg(src + b) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v += t[k];
         }
+        v = warp_sum(v);
+        if (lane == 0) s_tot[warp] = v;
     }
     __syncthreads();
 }

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
     }
     __syncthreads();
     auto clock = [&](int slot) {
-        if (lead) {
+        if (threadIdx.x == 0) {
             const long long t = globaltimer_ns();
             s_clk[slot] += t - s_clk[5];
             s_clk[5] = t;
@@ -293,6 +293,8 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
         cur_bank = next_bank();
         publish<1>(acc, s_red, cur_bank);
     }
+    if (threadIdx.x == 0 && a.block_clk)
+        for (int k = 0; k < 4; ++k) a.block_clk[4 * static_cast<size_t>(blockIdx.x) + k] = s_clk[k];
     if (!bar.sync(&s_flag)) return;
     if (blockIdx.x == 0) {
         grid_totals(cur_bank, 1, s_tot);

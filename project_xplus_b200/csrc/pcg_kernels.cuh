@@ -56,6 +56,7 @@ struct PcgArgs {
     // and how often the FP32 solution increments are folded into x64
     const int2* win;
     int flush_every;
+    long long* block_clk;   // [gridDim.x][4] phase clock of every CTA (ns)
 };
 
 struct SpmvArgs {
@@ -82,9 +83,11 @@ cudaError_t pcg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, 
 bool resident_supported(const KernelKey& k);
 int resident_max_slices();
 // Sets the dynamic shared-memory opt-in and reports whether one CTA per SM fits.
-cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, int tpb, bool* fits);
+// one_sync: the one-barrier-per-iteration kernel (records {m r, m Ap, p} x 2 generations).
+cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, int tpb, bool one_sync,
+                             bool* fits);
 cudaError_t resident_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, size_t smem_bytes,
-                            cudaStream_t s, const cudaAccessPolicyWindow& window);
+                            bool one_sync, cudaStream_t s, const cudaAccessPolicyWindow& window);
 cudaError_t spmv_launch(const KernelKey& k, const SpmvArgs& a, const void* x, void* y,
                         cudaStream_t s);
 // dst[i] = (T) src[perm[i]] for i < n, 0 for n <= i < n_pad   (T per xt; f64 when xt==F64)

@@ -9,6 +9,7 @@
 // before every FP64 residual (which needs x of neighbouring rows).  Two grid barriers per
 // iteration, as in the global-memory kernel (pcg_kernels.cu), with the same control flow,
 // breakdown tests and status codes (kernels/cuper_pcg_control_kernel.cpp:1069-1235).
+// pcg_resident1_kernel below needs one grid barrier per iteration instead of two.
 //
 // Shared memory (floats): pw[wn] | r[nb] | ap[nb] | dx[nb] | minv[nb] | rowsum[nb].
 #include <cuda_bf16.h>
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
     }
     __syncthreads();
     auto clock = [&](int slot) {
-        if (lead) {
+        if (threadIdx.x == 0) {
             const long long t = globaltimer_ns();
             s_clk[slot] += t - s_clk[5];
             s_clk[5] = t;
@@ -333,6 +334,338 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
         cur_bank = next_bank();
         publish<1>(acc, s_red, cur_bank);
     }
+    if (threadIdx.x == 0 && a.block_clk)
+        for (int k = 0; k < 4; ++k) a.block_clk[4 * static_cast<size_t>(blockIdx.x) + k] = s_clk[k];
+    if (!bar.sync(&s_flag)) return;
+    if (blockIdx.x == 0) {
+        grid_totals(cur_bank, 1, s_tot);
+        if (threadIdx.x == 0) {
+            PcgOut* o = a.out;
+            o->status = status;
+            o->iterations = iterations;
+            o->replacements = replacements;
+            o->stagnated = stagnated;
+            o->rz = rz;
+            o->rr = rr;
+            o->pap = pap;
+            o->alpha = alpha;
+            o->true_rr = s_tot[0];
+            o->t_end_ns = globaltimer_ns();
+            for (int k = 0; k < 4; ++k) o->t_phase[k] = s_clk[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// One grid barrier per iteration.  Phase A of iteration k publishes, next to p'.Ap', the six
+// FP64 sums that give the NEXT r.z and r.r in closed form once alpha is known:
+//   r_{k+1} = r_k - alpha Ap'_k  =>  r.z = S(m r r) - 2 alpha S(m r Ap') + alpha^2 S(m Ap' Ap')
+//                                     r.r = S(r r)   - 2 alpha S(r Ap')   + alpha^2 S(Ap' Ap')
+// (m = M^-1), so alpha, beta and the convergence test all come out of one reduction.  Instead
+// of exchanging z_{k+1} through a second barrier, each row publishes {m r_k, m Ap'_k, p'_k}
+// (double-buffered by generation) and every reader rebuilds p'_{k+1} = (m r_k - alpha m Ap'_k)
+// + beta p'_k for its window with the same fused multiply-adds, bit-identical to the owner's.
+// ---------------------------------------------------------------------------------------
+constexpr int kPartials1 = 7;
+
+template <typename VT, int CHUNK, typename IT>
+__global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
+    constexpr int NS = kResNS;
+    extern __shared__ float smem[];
+    __shared__ double s_red[32 * kPartials1];
+    __shared__ double s_tot[kPartials1 + 1];
+    __shared__ int s_flag;
+    __shared__ int2 s_slice[kResSlices];
+    __shared__ long long s_clk[6];
+    GridBarrier bar{a.bar, a.err, a.timeout_ns, 0u, a.debug_skip_block};
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int per_block = (a.n_slices + gridDim.x - 1) / gridDim.x;
+    const int sb = blockIdx.x * per_block;
+    const int se = min(a.n_slices, sb + per_block);
+    const int r0 = sb * 32;
+    const int nb = max(0, se - sb) * 32;
+    const int2 win = a.win[blockIdx.x];
+    const int w0 = win.x, wn = win.y;  // w0 and wn are multiples of 4
+    float* pw = smem;
+    float* rv = pw + wn;
+    float* apv = rv + nb;
+    float* dxv = apv + nb;
+    float* mi = dxv + nb;
+    float* rsv = mi + nb;
+    const VT* __restrict__ val = static_cast<const VT*>(a.val);
+    const IT* __restrict__ col = static_cast<const IT*>(a.col);
+    const float* __restrict__ minv_g = static_cast<const float*>(a.minv);
+    const float* __restrict__ rowsum_g = static_cast<const float*>(a.rowsum);
+    float* recs = static_cast<float*>(a.rec);  // [gen][{m r, m Ap, p}][n_pad]
+    const size_t np = static_cast<size_t>(a.n_pad);
+    auto rec_zr = [&](int g) { return recs + (3 * static_cast<size_t>(g) + 0) * np; };
+    auto rec_za = [&](int g) { return recs + (3 * static_cast<size_t>(g) + 1) * np; };
+    auto rec_p = [&](int g) { return recs + (3 * static_cast<size_t>(g) + 2) * np; };
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    const bool true_mode = a.tau_true_rr >= 0.0;
+    for (int k = threadIdx.x; k < se - sb; k += blockDim.x) {
+        const long long b0 = a.slice_ptr[sb + k];
+        s_slice[k] = make_int2(static_cast<int>(b0), static_cast<int>((a.slice_ptr[sb + k + 1] - b0) >> 5));
+    }
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        mi[t] = minv_g[r0 + t];
+        rsv[t] = rowsum_g[r0 + t];
+        dxv[t] = 0.0f;
+        apv[t] = 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 5; ++k) s_clk[k] = 0;
+        s_clk[5] = globaltimer_ns();
+        if (lead) a.out->t_start_ns = s_clk[5];
+    }
+    __syncthreads();
+    auto clock = [&](int slot) {
+        if (threadIdx.x == 0) {
+            const long long t = globaltimer_ns();
+            s_clk[slot] += t - s_clk[5];
+            s_clk[5] = t;
+        }
+    };
+    int bank = 0;
+    auto next_bank = [&]() {
+        double* b = a.partial + static_cast<size_t>(bank) * 8 * gridDim.x;
+        bank ^= 1;
+        return b;
+    };
+    double* cur_bank = nullptr;
+    auto flush_dx = [&]() {
+        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+            a.x64[r0 + t] += static_cast<double>(dxv[t]);
+            dxv[t] = 0.0f;
+        }
+    };
+    // r = b - A x in FP64 into shared r; records of generation g get {m r, 0, p (kept, or 0)}
+    auto residual_phase = [&](bool init, int g) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int s = sb + warp; s < se; s += wpb) {
+            const int row = s * 32 + lane;
+            const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
+            const double rt = a.b64[row] - y;
+            const float r_ = static_cast<float>(rt);
+            const float z_ = mi[row - r0] * r_;
+            rv[row - r0] = r_;
+            rec_zr(g)[row] = z_;
+            rec_za(g)[row] = 0.0f;
+            if (init) rec_p(g)[row] = 0.0f;
+            acc[0] += static_cast<double>(r_) * static_cast<double>(z_);
+            acc[1] += static_cast<double>(r_) * static_cast<double>(r_);
+            acc[2] += rt * rt;
+        }
+        cur_bank = next_bank();
+        publish<3>(acc, s_red, cur_bank);
+    };
+    // the pending update of the previous iteration: dx += alpha p', r -= alpha Ap'
+    auto apply_update = [&](float al) {
+        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+            const float pv = pw[r0 + t - w0];
+            dxv[t] = __fmaf_rn(al, pv, dxv[t]);
+            rv[t] = rv[t] - al * apv[t];
+        }
+    };
+
+    int gen = 0;
+    residual_phase(true, gen);
+    if (!bar.sync(&s_flag)) return;
+    grid_totals(cur_bank, 3, s_tot);
+    double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
+    double rr_at_replace = rr, best_true = true_rr;
+    double pap = 0.0, alpha = 0.0, beta = 0.0;
+    double pend = 0.0;  // alpha of the update not yet applied to x and r (0: none)
+    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
+    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const int flush_every = a.flush_every > 0 ? a.flush_every : 16;
+    clock(4);
+
+    if (converged_now) {
+        status = XPLUS_CONVERGED;
+    } else {
+        for (int it = 0; it < a.max_iters; ++it) {
+            if (bad(rz) || bad(rr) || fabs(rz) <= kBreakdownEps) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            // ---- apply the previous update to the band, then the new window p' ----
+            const float al_prev = static_cast<float>(pend);
+            if (pend != 0.0) {
+                apply_update(al_prev);
+                if (it % flush_every == 0) flush_dx();
+                __syncthreads();
+            }
+            pend = 0.0;
+            {
+                const float be = static_cast<float>(beta);
+                const float4* zr4 = reinterpret_cast<const float4*>(rec_zr(gen) + w0);
+                const float4* za4 = reinterpret_cast<const float4*>(rec_za(gen) + w0);
+                const float4* p4 = reinterpret_cast<const float4*>(rec_p(gen) + w0);
+                float4* pw4 = reinterpret_cast<float4*>(pw);
+                for (int t = threadIdx.x; t < (wn >> 2); t += blockDim.x) {
+                    const float4 z = zr4[t], q = za4[t], p = p4[t];
+                    float4 o;
+                    o.x = __fmaf_rn(be, p.x, __fmaf_rn(-al_prev, q.x, z.x));
+                    o.y = __fmaf_rn(be, p.y, __fmaf_rn(-al_prev, q.y, z.y));
+                    o.z = __fmaf_rn(be, p.z, __fmaf_rn(-al_prev, q.z, z.z));
+                    o.w = __fmaf_rn(be, p.w, __fmaf_rn(-al_prev, q.w, z.w));
+                    pw4[t] = o;
+                }
+                __syncthreads();
+            }
+            // ---- Ap' from shared memory ----
+            for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
+                int2 sl[NS];
+                int row[NS];
+                float pi[NS], y[NS];
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    const int s = s0 + k * wpb;
+                    const bool on = s < se;
+                    sl[k] = on ? s_slice[s - sb] : make_int2(0, 0);
+                    row[k] = on ? s * 32 + lane : -1;
+                    pi[k] = on ? pw[row[k] - w0] : 0.0f;
+                }
+                sell_rows_smem<VT, CHUNK, IT, NS>(sl, row, lane, col, val, pw, w0, pi, y);
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    if (row[k] < 0) continue;
+                    const int t = row[k] - r0;
+                    apv[t] = y[k] + rsv[t] * pi[k];
+                }
+            }
+            __syncthreads();
+            // ---- records of the next generation and the seven sums ----
+            {
+                double acc[kPartials1] = {0, 0, 0, 0, 0, 0, 0};
+                const int g1 = gen ^ 1;
+                float* zr1 = rec_zr(g1);
+                float* za1 = rec_za(g1);
+                float* p1 = rec_p(g1);
+                for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+                    const float pv = pw[r0 + t - w0];
+                    const float r_ = rv[t], ap_ = apv[t], m = mi[t];
+                    const float mr = m * r_, ma = m * ap_;
+                    zr1[r0 + t] = mr;
+                    za1[r0 + t] = ma;
+                    p1[r0 + t] = pv;
+                    const double dr = r_, da = ap_, dm = m;
+                    acc[0] += static_cast<double>(pv) * da;
+                    acc[1] += dm * dr * dr;
+                    acc[2] += dm * dr * da;
+                    acc[3] += dm * da * da;
+                    acc[4] += dr * dr;
+                    acc[5] += dr * da;
+                    acc[6] += da * da;
+                }
+                cur_bank = next_bank();
+                publish<kPartials1>(acc, s_red, cur_bank);
+            }
+            clock(0);
+            if (!bar.sync(&s_flag)) return;
+            grid_totals(cur_bank, kPartials1, s_tot);
+            clock(1);
+            gen ^= 1;
+            pap = s_tot[0];
+            if (bad(pap) || fabs(pap) <= kBreakdownEps) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            const double rz_old = rz;
+            alpha = rz / pap;
+            if (bad(alpha)) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            pend = alpha;
+            double rz_new = s_tot[1] - 2.0 * alpha * s_tot[2] + alpha * alpha * s_tot[3];
+            double rr_new = s_tot[4] - 2.0 * alpha * s_tot[5] + alpha * alpha * s_tot[6];
+            iterations = it + 1;
+            if (bad(rz_new) || bad(rr_new)) {
+                rz = rz_new;
+                rr = rr_new;
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            bool do_replace = false;
+            if (true_mode) {
+                if (rr_new <= a.tau_true_rr) do_replace = true;
+                if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
+                if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = true;
+            }
+            if (do_replace) {
+                apply_update(static_cast<float>(pend));
+                pend = 0.0;
+                __syncthreads();
+                flush_dx();
+                if (!bar.sync(&s_flag)) return;
+                residual_phase(false, gen);
+                if (!bar.sync(&s_flag)) return;
+                grid_totals(cur_bank, 3, s_tot);
+                clock(4);
+                rz_new = s_tot[0];
+                rr_new = s_tot[1];
+                true_rr = s_tot[2];
+                ++replacements;
+                rr_at_replace = rr_new;
+                if (true_rr < 0.9 * best_true) {
+                    best_true = true_rr;
+                    stagnant = 0;
+                } else if (++stagnant >= 8) {
+                    stagnated = 1;
+                }
+            }
+            if (lead && a.trace && it < a.trace_cap) {
+                double* t = a.trace + 5 * static_cast<size_t>(it);
+                t[0] = alpha;
+                t[1] = rz_new / rz_old;
+                t[2] = rz_new;
+                t[3] = rr_new;
+                t[4] = sqrt(rr_new > 0.0 ? rr_new : 0.0);
+            }
+            rz = rz_new;
+            rr = rr_new;
+            if (true_mode ? (do_replace && true_rr <= a.tau_true_rr) : (rr <= a.tau_rr)) {
+                status = XPLUS_CONVERGED;
+                break;
+            }
+            if (stagnated) break;
+            if (fabs(rz_old) <= kBreakdownEps) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+            beta = rz / rz_old;
+            if (bad(beta)) {
+                status = XPLUS_BREAKDOWN;
+                break;
+            }
+        }
+    }
+    if (status == XPLUS_MAX_ITER && !true_mode && rr <= a.tau_rr) status = XPLUS_CONVERGED;
+
+    // ---- exit: the pending update, dx into x, then the FP64 true residual ----
+    if (pend != 0.0) {
+        apply_update(static_cast<float>(pend));
+        __syncthreads();
+    }
+    flush_dx();
+    if (!bar.sync(&s_flag)) return;
+    {
+        double acc[1] = {0.0};
+        for (int s = sb + warp; s < se; s += wpb) {
+            const int row = s * 32 + lane;
+            const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
+            const double rt = a.b64[row] - y;
+            acc[0] += rt * rt;
+        }
+        cur_bank = next_bank();
+        publish<1>(acc, s_red, cur_bank);
+    }
+    if (threadIdx.x == 0 && a.block_clk)
+        for (int k = 0; k < 4; ++k) a.block_clk[4 * static_cast<size_t>(blockIdx.x) + k] = s_clk[k];
     if (!bar.sync(&s_flag)) return;
     if (blockIdx.x == 0) {
         grid_totals(cur_bank, 1, s_tot);
@@ -380,7 +713,13 @@ bool resident_supported(const KernelKey& k) {
     return resident_dispatch(k, [](auto*, auto, auto*) {});
 }
 
-cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, int tpb, bool* fits) {
+template <typename VT, int CHUNK, typename IT>
+auto resident_fn(bool one_sync) {
+    return one_sync ? pcg_resident1_kernel<VT, CHUNK, IT> : pcg_resident_kernel<VT, CHUNK, IT>;
+}
+
+cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, int tpb, bool one_sync,
+                             bool* fits) {
     *fits = false;
     int optin = 0;
     cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -389,7 +728,7 @@ cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, 
     bool ok = resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
         using VT = std::remove_pointer_t<decltype(vt)>;
         using IT = std::remove_pointer_t<decltype(it)>;
-        e = cudaFuncGetAttributes(&fa, pcg_resident_kernel<VT, decltype(chunk)::value, IT>);
+        e = cudaFuncGetAttributes(&fa, resident_fn<VT, decltype(chunk)::value, IT>(one_sync));
     });
     if (!ok) return cudaSuccess;
     if (e != cudaSuccess) return e;
@@ -398,7 +737,7 @@ cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, 
     resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
         using VT = std::remove_pointer_t<decltype(vt)>;
         using IT = std::remove_pointer_t<decltype(it)>;
-        e = cudaFuncSetAttribute(pcg_resident_kernel<VT, decltype(chunk)::value, IT>,
+        e = cudaFuncSetAttribute(resident_fn<VT, decltype(chunk)::value, IT>(one_sync),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes));
     });
     if (e != cudaSuccess) return e;
@@ -407,7 +746,7 @@ cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, 
         using VT = std::remove_pointer_t<decltype(vt)>;
         using IT = std::remove_pointer_t<decltype(it)>;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, pcg_resident_kernel<VT, decltype(chunk)::value, IT>, tpb, smem_bytes);
+            &per_sm, resident_fn<VT, decltype(chunk)::value, IT>(one_sync), tpb, smem_bytes);
     });
     if (e != cudaSuccess) return e;
     *fits = per_sm >= 1;
@@ -415,7 +754,7 @@ cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, 
 }
 
 cudaError_t resident_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, size_t smem_bytes,
-                            cudaStream_t s, const cudaAccessPolicyWindow& window) {
+                            bool one_sync, cudaStream_t s, const cudaAccessPolicyWindow& window) {
     cudaError_t e = cudaErrorInvalidValue;
     resident_dispatch(k, [&](auto* vt, auto chunk, auto* it) {
         using VT = std::remove_pointer_t<decltype(vt)>;
@@ -437,7 +776,7 @@ cudaError_t resident_launch(const KernelKey& k, const PcgArgs& a, int grid, int 
         }
         cfg.attrs = attr;
         cfg.numAttrs = na;
-        e = cudaLaunchKernelEx(&cfg, pcg_resident_kernel<VT, decltype(chunk)::value, IT>, a);
+        e = cudaLaunchKernelEx(&cfg, resident_fn<VT, decltype(chunk)::value, IT>(one_sync), a);
     });
     return e;
 }

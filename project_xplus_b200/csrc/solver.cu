@@ -55,8 +55,10 @@ struct xplus_pcg {
     int trace_cap = 0;
     int grid = 0, tpb = 0;
     bool resident = false;     // SM-resident kernel (pcg_resident.cu)
+    bool one_sync = false;     // its one-barrier-per-iteration form
     size_t smem_bytes = 0;
     int2* d_win = nullptr;
+    long long* d_block_clk = nullptr;  // per-CTA phase clock [grid][4]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     xplus_metrics last{};
     double last_bnorm2 = 0.0;
@@ -228,7 +230,8 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         h->d_minv = dalloc<unsigned char>(h, np * xs);
         h->d_b64 = dalloc<double>(h, np);
         h->d_x64 = dalloc<double>(h, np);
-        h->d_rec = dalloc<unsigned char>(h, np * xs * 2);
+        // {z, p} records, or for the one-barrier resident kernel {m r, m Ap, p} x 2 generations
+        h->d_rec = dalloc<unsigned char>(h, np * std::max<size_t>(xs * 2, 6 * sizeof(float)));
         h->d_r = dalloc<unsigned char>(h, np * xs);
         h->d_ap = dalloc<unsigned char>(h, np * xs);
         h->d_sx = dalloc<unsigned char>(h, np * xs);
@@ -299,13 +302,16 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
                         lo = std::min(lo, S.col[static_cast<size_t>(pos)]);
                         hi = std::max(hi, S.col[static_cast<size_t>(pos)] + 1);
                     }
+                    lo &= ~3;                                        // 16-byte aligned window
+                    hi = std::min(S.n_pad, (hi + 3) & ~3);
                     win[static_cast<size_t>(b)] = make_int2(lo, hi - lo);
                     max_wn = std::max(max_wn, hi - lo);
                     max_nb = std::max(max_nb, (se - sb) * 32);
                 }
                 const size_t smem = sizeof(float) * (static_cast<size_t>(max_wn) + 5 * static_cast<size_t>(max_nb));
                 bool fits = false;
-                cuda_check(resident_prepare(h->key, o.device, smem, want_tpb, &fits), "resident_prepare");
+                h->one_sync = o.barriers_per_iter != 2;
+                cuda_check(resident_prepare(h->key, o.device, smem, want_tpb, h->one_sync, &fits), "resident_prepare");
                 if (fits) {
                     h->resident = true;
                     h->smem_bytes = smem;
@@ -318,7 +324,8 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         }
         if (!h->resident)
             cuda_check(pcg_grid(h->key, o.device, S.n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
-        h->d_partial = dalloc<double>(h, static_cast<size_t>(8) * h->grid);
+        h->d_partial = dalloc<double>(h, static_cast<size_t>(16) * h->grid);
+        h->d_block_clk = dalloc<long long>(h, static_cast<size_t>(4) * h->grid);
         cuda_check(cudaMemsetAsync(h->d_x64, 0, np * sizeof(double), st), "memset");
         cuda_check(cudaStreamSynchronize(st), "sync");
         h->last.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -371,6 +378,7 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     a.max_iters = max_iters;
     a.debug_skip_block = h->debug_skip_block;
     a.win = h->d_win;
+    a.block_clk = h->d_block_clk;
     a.flush_every = 16;
     a.timeout_ns = static_cast<long long>((h->opts.barrier_timeout_s > 0 ? h->opts.barrier_timeout_s : 2.0) * 1e9);
     if (tau_mode == XPLUS_TAU_ABS_RR) {
@@ -388,7 +396,8 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     cuda_check(cudaMemsetAsync(h->d_out, 0, sizeof(PcgOut), st), "memset");
     cuda_check(cudaEventRecord(h->ev0, st), "event");
     if (h->resident)
-        cuda_check(resident_launch(h->key, a, h->grid, h->tpb, h->smem_bytes, st, h->window), "resident PCG launch");
+        cuda_check(resident_launch(h->key, a, h->grid, h->tpb, h->smem_bytes, h->one_sync, st, h->window),
+                   "resident PCG launch");
     else
         cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st, h->window), "persistent PCG launch");
     cuda_check(cudaEventRecord(h->ev1, st), "event");
@@ -454,6 +463,7 @@ void xplus_opts_default(xplus_opts* o) {
     o->index16 = 1;
     o->l2_persist = 1;
     o->resident = 1;
+    o->barriers_per_iter = 1;
 }
 
 int xplus_device_count(void) {
@@ -556,6 +566,19 @@ int xplus_pcg_last_phase_times(xplus_pcg* h, double* ms4) {
         require(h && ms4, XPLUS_ERR_ARG, "null argument");
         collect(h, nullptr);
         for (int k = 0; k < 4; ++k) ms4[k] = static_cast<double>(h->phase_ns[k]) * 1e-6;
+    });
+}
+
+int xplus_pcg_last_block_times(xplus_pcg* h, double* ms, int max_blocks, int* blocks) {
+    return guarded([&] {
+        require(h && blocks, XPLUS_ERR_ARG, "null argument");
+        collect(h, nullptr);
+        *blocks = h->grid;
+        if (!ms) return;
+        const int nb = std::min(max_blocks, h->grid);
+        std::vector<long long> t(static_cast<size_t>(4) * h->grid);
+        cuda_check(cudaMemcpy(t.data(), h->d_block_clk, t.size() * sizeof(long long), cudaMemcpyDeviceToHost), "D2H");
+        for (int k = 0; k < 4 * nb; ++k) ms[k] = static_cast<double>(t[static_cast<size_t>(k)]) * 1e-6;
     });
 }
 

@@ -50,6 +50,7 @@ extern "C" {
 #define XPLUS_F32 0
 #define XPLUS_BF16 1
 #define XPLUS_F64 2
+#define XPLUS_F16 3          /* FP16 values with one power-of-two scale per matrix (row-sum form) */
 
 /* ---- tolerance semantics ---- */
 #define XPLUS_TAU_ABS_RR 0   /* stop when the recurrence rr = ||r||^2 <= tau (the reference's
@@ -62,7 +63,11 @@ extern "C" {
 #define XPLUS_PREC_GTG 1     /* M^-1 = G^T G, G lower-triangular on A's lower pattern */
 
 typedef struct xplus_opts {
-    int value_type;        /* XPLUS_F32 | XPLUS_BF16 | XPLUS_F64: matrix values in the SpMV */
+    int value_type;        /* XPLUS_F32 | XPLUS_BF16 | XPLUS_F16 | XPLUS_F64: matrix values in the
+                              SpMV.  The 16-bit types need row_sum_form.  FP16 (11-bit significand,
+                              values divided by one power-of-two scale) keeps stiffness matrices
+                              within ~1% of A; BF16 (8-bit) perturbs them by ~4%, which stalls or
+                              diverges the inner PCG on large FEM systems */
     int vector_type;       /* XPLUS_F32 | XPLUS_F64: x, r, p, Ap storage in the inner loop */
     int slice_height;      /* SELL-C-sigma C; must be 32 */
     int sigma;             /* SELL sort window (rows); multiple of 32, or 1 for no sorting */
@@ -91,6 +96,9 @@ typedef struct xplus_opts {
     int resident;          /* FP32 vectors, row-sum form: use the SM-resident kernel (state and
                               the search direction's band + halo in shared memory) when one CTA
                               per SM holds it (default 1) */
+    int restart_on_replace; /* after an FP64 residual replacement: 1 restarts the search direction
+                              (p = z), 0 keeps it; -1 (default) restarts only for 16-bit values,
+                              whose inexact operator breaks the conjugacy a kept p relies on */
     int barriers_per_iter; /* SM-resident kernel: 1 (default) folds both dot products into one
                               reduction by expanding r_{k+1}.z_{k+1} and r_{k+1}.r_{k+1} in alpha;
                               2 reduces them after the update as the reference does */

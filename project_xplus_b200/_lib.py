@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libxplus_b200.so"
 
 XPLUS_CONVERGED, XPLUS_MAX_ITER, XPLUS_BREAKDOWN, XPLUS_TIMEOUT = 0, 1, 2, 3
 XPLUS_OK, XPLUS_ERR_ARG, XPLUS_ERR_CUDA, XPLUS_ERR_DATA, XPLUS_ERR_IO, XPLUS_ERR_NOMEM = 0, 10, 11, 12, 13, 14
-XPLUS_F32, XPLUS_BF16, XPLUS_F64 = 0, 1, 2
+XPLUS_F32, XPLUS_BF16, XPLUS_F64, XPLUS_F16 = 0, 1, 2, 3
 XPLUS_TAU_ABS_RR, XPLUS_TAU_REL_TRUE = 0, 1
 XPLUS_NOALLOC_MAX_N = 4194304
 
@@ -27,7 +27,7 @@ class XplusOpts(C.Structure):
         ("replace_every", C.c_int), ("replace_drop", C.c_double), ("block_threads", C.c_int),
         ("blocks_per_sm", C.c_int), ("barrier_timeout_s", C.c_double), ("device", C.c_int),
         ("row_sum_form", C.c_int), ("index16", C.c_int), ("l2_persist", C.c_int),
-        ("resident", C.c_int), ("barriers_per_iter", C.c_int),
+        ("resident", C.c_int), ("restart_on_replace", C.c_int), ("barriers_per_iter", C.c_int),
     ]
 
 

@@ -2,6 +2,7 @@
 // shared by the sm_100a kernels.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -76,6 +77,33 @@ struct ChunkLoad<__nv_bfloat16, 4> {
     }
 };
 
+__device__ __forceinline__ float f16_lo(uint32_t w) {
+    return __half2float(__ushort_as_half(static_cast<unsigned short>(w & 0xFFFFu)));
+}
+__device__ __forceinline__ float f16_hi(uint32_t w) {
+    return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
+}
+template <>
+struct ChunkLoad<__half, 1> {
+    static __device__ __forceinline__ void run(const __half* p, float* o) {
+        o[0] = __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p))));
+    }
+};
+template <>
+struct ChunkLoad<__half, 2> {
+    static __device__ __forceinline__ void run(const __half* p, float* o) {
+        const uint32_t v = __ldg(reinterpret_cast<const unsigned int*>(p));
+        o[0] = f16_lo(v); o[1] = f16_hi(v);
+    }
+};
+template <>
+struct ChunkLoad<__half, 4> {
+    static __device__ __forceinline__ void run(const __half* p, float* o) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+        o[0] = f16_lo(v.x); o[1] = f16_hi(v.x); o[2] = f16_lo(v.y); o[3] = f16_hi(v.y);
+    }
+};
+
 // Column loads: absolute int32 columns, or int16 offsets from the row (lossless when the
 // bandwidth of the ordered matrix is below 32768) returned as absolute columns.
 template <int CHUNK, typename IT>
@@ -122,6 +150,7 @@ struct ColLoad<4, short> {
 // The arithmetic type of a matrix value: bf16 values are widened to float.
 template <typename VT> struct ValArith { using type = VT; };
 template <> struct ValArith<__nv_bfloat16> { using type = float; };
+template <> struct ValArith<__half> { using type = float; };
 
 // ---------------------------------------------------------------------------------------
 // Reductions in FP64 with a fixed combination order (results identical in every block).

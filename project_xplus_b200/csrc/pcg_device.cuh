@@ -85,7 +85,8 @@ __device__ __forceinline__ double row_fp64(const PcgArgs& a, int s, int lane, in
     } else {
         y = sell_row<VT, CHUNK, DIFF, IT, double, double>(a.slice_ptr, col, static_cast<const VT*>(a.val),
                                                           s, lane, a.x64, xi);
-        if (DIFF) y += static_cast<double>(static_cast<const XT*>(a.rowsum)[row]) * xi;
+        if (DIFF) y = y * static_cast<double>(a.val_scale) +
+                      static_cast<double>(static_cast<const XT*>(a.rowsum)[row]) * xi;
     }
     return y;
 }

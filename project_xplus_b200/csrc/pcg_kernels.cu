@@ -16,6 +16,7 @@
 // iterations, or when ||r|| fell by a set factor.  The control flow, breakdown tests and
 // status codes follow kernels/cuper_pcg_control_kernel.cpp:1069-1235.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
 #pragma unroll
                     for (int k = 0; k < NS; ++k) {
                         if (row[k] < 0) continue;
-                        if (DIFF) y[k] += rowsum[row[k]] * pi[k];
+                        if (DIFF) y[k] = y[k] * static_cast<XT>(a.val_scale) + rowsum[row[k]] * pi[k];
                         ap[row[k]] = y[k];
                         acc[0] += static_cast<double>(pi[k]) * static_cast<double>(y[k]);
                     }
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = rz / rz_old;
+            beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SpmvArgs a, const XT* __
     const XT xi = x[row];
     XT acc = sell_row<VT, CHUNK, DIFF, IT, XT, XT>(a.slice_ptr, static_cast<const IT*>(a.col),
                                                    static_cast<const VT*>(a.val), s, lane, x, xi);
-    if (DIFF) acc += static_cast<const XT*>(a.rowsum)[row] * xi;
+    if (DIFF) acc = acc * static_cast<XT>(a.val_scale) + static_cast<const XT*>(a.rowsum)[row] * xi;
     y[row] = acc;
 }
 
@@ -343,8 +344,8 @@ __global__ void scatter_kernel(const double* __restrict__ src, double* __restric
 }
 
 // ---- dispatch over (value type, vector type, chunk, row-sum form, index width) ----
-// Instantiated combinations: FP32 values in either form, BF16 values in the row-sum form only,
-// FP64 values in the plain form only.
+// Instantiated combinations: FP32 values in either form, BF16 and FP16 values in the row-sum
+// form only, FP64 values in the plain form only.
 template <typename XT, int CHUNK, bool DIFF, typename IT, typename F>
 bool with_vt(int vt, F&& f) {
     using C = std::integral_constant<int, CHUNK>;
@@ -353,6 +354,9 @@ bool with_vt(int vt, F&& f) {
         case XPLUS_F32: f(static_cast<float*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true;
         case XPLUS_BF16:
             if constexpr (DIFF) { f(static_cast<__nv_bfloat16*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true; }
+            return false;
+        case XPLUS_F16:
+            if constexpr (DIFF) { f(static_cast<__half*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true; }
             return false;
         case XPLUS_F64:
             if constexpr (!DIFF) { f(static_cast<double*>(nullptr), static_cast<XT*>(nullptr), C(), D(), static_cast<IT*>(nullptr)); return true; }

@@ -25,6 +25,7 @@ struct PcgArgs {
     const long long* slice_ptr;
     const void* col;        // int32 columns or int16 row offsets (KernelKey::idx16)
     const void* val;        // VT, slots
+    float val_scale;        // stored off-diagonal values are a_ij / val_scale (1 except FP16)
     const double* val64;    // FP64 copy in the same layout (nullable)
     const void* rowsum;     // XT, n_pad: row sums s_i = sum_j a_ij (row-sum form only)
     const double* diag64;   // FP64 diagonal when the slots hold off-diagonals only
@@ -50,6 +51,7 @@ struct PcgArgs {
     int max_iters;
     int replace_every;
     double replace_drop;    // rr ratio that triggers a replacement (0: off)
+    int restart_on_replace; // 1: beta = 0 after a replacement (search direction restarts)
     long long timeout_ns;
     int debug_skip_block;   // test-only fault injection: block that skips its first arrival
     // SM-resident kernel only: per-CTA shared window {first row, rows} of the search direction,
@@ -65,6 +67,7 @@ struct SpmvArgs {
     const void* col;
     const void* val;
     const void* rowsum;     // row-sum form only
+    float val_scale;
 };
 
 // vt: XPLUS_F32/BF16/F64 ; xt: XPLUS_F32/F64 ; chunk 1/2/4 ; diag = row-sum form ; gtg

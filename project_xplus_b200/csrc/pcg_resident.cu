@@ -13,6 +13,7 @@
 //
 // Shared memory (floats): pw[wn] | r[nb] | ap[nb] | dx[nb] | minv[nb] | rowsum[nb].
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                     for (int k = 0; k < NS; ++k) {
                         if (row[k] < 0) continue;
                         const int t = row[k] - r0;
-                        const float yy = y[k] + rsv[t] * pi[k];
+                        const float yy = y[k] * a.val_scale + rsv[t] * pi[k];
                         apv[t] = yy;
                         acc[0] += static_cast<double>(pi[k]) * static_cast<double>(yy);
                     }
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = rz / rz_old;
+            beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;
@@ -534,7 +535,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 for (int k = 0; k < NS; ++k) {
                     if (row[k] < 0) continue;
                     const int t = row[k] - r0;
-                    apv[t] = y[k] + rsv[t] * pi[k];
+                    apv[t] = y[k] * a.val_scale + rsv[t] * pi[k];
                 }
             }
             __syncthreads();
@@ -637,7 +638,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = rz / rz_old;
+            beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;
@@ -704,6 +705,7 @@ bool resident_dispatch(const KernelKey& k, F&& f) {
     };
     if (k.vt == XPLUS_F32) return with_chunk(static_cast<float*>(nullptr));
     if (k.vt == XPLUS_BF16) return with_chunk(static_cast<__nv_bfloat16*>(nullptr));
+    if (k.vt == XPLUS_F16) return with_chunk(static_cast<__half*>(nullptr));
     return false;
 }
 

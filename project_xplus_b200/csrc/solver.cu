@@ -6,6 +6,7 @@
 // allocates 26 buffers and launches cuper_pcg_control_kernel once; here the host builds
 // SELL-C-sigma, uploads it once per handle and launches one cooperative kernel per solve.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -56,6 +57,7 @@ struct xplus_pcg {
     int grid = 0, tpb = 0;
     bool resident = false;     // SM-resident kernel (pcg_resident.cu)
     bool one_sync = false;     // its one-barrier-per-iteration form
+    double val_scale = 1.0;    // stored value = a_ij / val_scale (FP16)
     size_t smem_bytes = 0;
     int2* d_win = nullptr;
     long long* d_block_clk = nullptr;  // per-CTA phase clock [grid][4]
@@ -91,7 +93,7 @@ T* dalloc(xplus_pcg* h, size_t count) {
     return static_cast<T*>(p);
 }
 
-size_t elem_size(int t) { return t == XPLUS_F64 ? 8 : (t == XPLUS_BF16 ? 2 : 4); }
+size_t elem_size(int t) { return t == XPLUS_F64 ? 8 : ((t == XPLUS_BF16 || t == XPLUS_F16) ? 2 : 4); }
 
 void require_device(int device) {
     int count = 0;
@@ -108,19 +110,31 @@ void require_device(int device) {
     require(coop != 0, XPLUS_ERR_CUDA, "device does not support cooperative launch");
 }
 
-// Converts FP64 values to the storage type into a host byte buffer.
-std::vector<unsigned char> convert(const std::vector<double>& v, int type) {
+// Converts FP64 values to the storage type into a host byte buffer (FP16: v / scale).
+std::vector<unsigned char> convert(const std::vector<double>& v, int type, double scale = 1.0) {
     std::vector<unsigned char> out(v.size() * elem_size(type));
     if (type == XPLUS_F64) {
         std::memcpy(out.data(), v.data(), out.size());
     } else if (type == XPLUS_F32) {
         float* o = reinterpret_cast<float*>(out.data());
         for (size_t i = 0; i < v.size(); ++i) o[i] = static_cast<float>(v[i]);
+    } else if (type == XPLUS_F16) {
+        __half* o = reinterpret_cast<__half*>(out.data());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = __double2half(v[i] / scale);
     } else {
         __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(out.data());
         for (size_t i = 0; i < v.size(); ++i) o[i] = __double2bfloat16(v[i]);
     }
     return out;
+}
+
+// Power-of-two scale that puts the largest |value| just below 2^15, inside FP16's range with
+// the smallest values of a ~1e9 dynamic range still normal.
+double f16_scale(const std::vector<double>& v) {
+    double m = 0.0;
+    for (double x : v) m = std::max(m, std::fabs(x));
+    if (!(m > 0.0)) return 1.0;
+    return std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(m))) - 15);
 }
 
 void destroy(xplus_pcg* h) {
@@ -143,8 +157,8 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     xplus_opts o;
     xplus_opts_default(&o);
     if (opts_in) o = *opts_in;
-    require(o.value_type == XPLUS_F32 || o.value_type == XPLUS_BF16 || o.value_type == XPLUS_F64,
-            XPLUS_ERR_ARG, "bad value_type");
+    require(o.value_type == XPLUS_F32 || o.value_type == XPLUS_BF16 || o.value_type == XPLUS_F16 ||
+                o.value_type == XPLUS_F64, XPLUS_ERR_ARG, "bad value_type");
     require(o.vector_type == XPLUS_F32 || o.vector_type == XPLUS_F64, XPLUS_ERR_ARG, "bad vector_type");
     require(o.slice_height == 32, XPLUS_ERR_ARG, "slice_height must be 32");
     require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
@@ -162,7 +176,8 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     // s_i = sum_j a_ij (FP64 sum) are kept apart in the vector type, and the FP64 diagonal
     // stays apart for the true residual.
     const bool split = (o.value_type != XPLUS_F64) && o.row_sum_form;
-    require(o.value_type != XPLUS_BF16 || split, XPLUS_ERR_ARG, "BF16 values need row_sum_form");
+    require((o.value_type != XPLUS_BF16 && o.value_type != XPLUS_F16) || split, XPLUS_ERR_ARG,
+            "16-bit values need row_sum_form");
     SellHost S;
     sell_build(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
 
@@ -249,7 +264,8 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         else
             cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(cudaMemcpyAsync(h->d_perm, S.perm.data(), S.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
-        std::vector<unsigned char> vbytes = convert(S.val, o.value_type);
+        h->val_scale = o.value_type == XPLUS_F16 ? f16_scale(S.val) : 1.0;
+        std::vector<unsigned char> vbytes = convert(S.val, o.value_type, h->val_scale);
         cuda_check(cudaMemcpyAsync(h->d_val, vbytes.data(), vbytes.size(), cudaMemcpyHostToDevice, st), "H2D");
         const bool keep64 = o.keep_fp64 != 0 && o.value_type != XPLUS_F64;
         if (keep64) {
@@ -360,6 +376,7 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     a.slice_ptr = h->d_slice_ptr;
     a.col = h->d_col;
     a.val = h->d_val;
+    a.val_scale = static_cast<float>(h->val_scale);
     a.val64 = h->d_val64;
     a.rowsum = h->d_rowsum;
     a.diag64 = h->d_diag64;
@@ -390,6 +407,8 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
         a.tau_rr = a.tau_true_rr;
         a.replace_every = h->opts.replace_every;
         a.replace_drop = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
+        const bool low = h->opts.value_type == XPLUS_BF16 || h->opts.value_type == XPLUS_F16;
+        a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 1 : 0) : h->opts.restart_on_replace;
     }
     cuda_check(cudaMemsetAsync(h->d_bar, 0, sizeof(unsigned), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
@@ -464,6 +483,7 @@ void xplus_opts_default(xplus_opts* o) {
     o->l2_persist = 1;
     o->resident = 1;
     o->barriers_per_iter = 1;
+    o->restart_on_replace = -1;
 }
 
 int xplus_device_count(void) {
@@ -597,7 +617,8 @@ int xplus_pcg_spmv(xplus_pcg* h, const double* x, double* y) {
         const size_t nb = sizeof(double) * static_cast<size_t>(h->n);
         cuda_check(cudaMemcpyAsync(h->d_xio, x, nb, cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(gather_to_sell(h->opts.vector_type, h->d_xio, h->d_sx, h->d_perm, h->n, h->n_pad, st), "gather");
-        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_rowsum};
+        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_rowsum,
+                   static_cast<float>(h->val_scale)};
         cuda_check(spmv_launch(h->key, a, h->d_sx, h->d_sy, st), "spmv");
         // widen the SELL-order result to FP64 and scatter to original order
         std::vector<unsigned char> ys(static_cast<size_t>(h->n_pad) * elem_size(h->opts.vector_type));
@@ -617,7 +638,8 @@ int xplus_pcg_spmv_device(xplus_pcg* h, const void* d_x, void* d_y, void* stream
     return guarded([&] {
         require(h && d_x && d_y, XPLUS_ERR_ARG, "null argument");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
-        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_rowsum};
+        SpmvArgs a{h->n_pad, h->n_slices, h->d_slice_ptr, h->d_col, h->d_val, h->d_rowsum,
+                   static_cast<float>(h->val_scale)};
         cuda_check(spmv_launch(h->key, a, d_x, d_y, st), "spmv");
     });
 }

@@ -26,7 +26,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _lib
-from ._lib import (XPLUS_F32, XPLUS_F64, XPLUS_BF16, XPLUS_TAU_ABS_RR, XPLUS_TAU_REL_TRUE,
+from ._lib import (XPLUS_F32, XPLUS_F64, XPLUS_BF16, XPLUS_F16, XPLUS_TAU_ABS_RR, XPLUS_TAU_REL_TRUE,
                    STATUS_NAMES, XplusError, check, lib, ptr)
 
 
@@ -150,7 +150,8 @@ def log_iteration(iteration: int, alpha: float, beta: float, rz: float, rr: floa
 
 
 _TYPES = {"f32": XPLUS_F32, "fp32": XPLUS_F32, "float32": XPLUS_F32, "bf16": XPLUS_BF16,
-          "bfloat16": XPLUS_BF16, "f64": XPLUS_F64, "fp64": XPLUS_F64, "float64": XPLUS_F64}
+          "bfloat16": XPLUS_BF16, "f64": XPLUS_F64, "fp64": XPLUS_F64, "float64": XPLUS_F64,
+          "f16": XPLUS_F16, "fp16": XPLUS_F16, "float16": XPLUS_F16}
 
 
 def _type(t) -> int:
@@ -164,7 +165,7 @@ class PcgSolver:
                  sigma=256, chunk=4, keep_fp64=True, replace_every=0, replace_drop=1e-2,
                  block_threads=0, blocks_per_sm=0, barrier_timeout_s=2.0, device=0,
                  row_sum_form=True, index16=True, l2_persist=True, resident=True,
-                 barriers_per_iter=1):
+                 barriers_per_iter=1, restart_on_replace=-1):
         self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
         self.col_idx = np.ascontiguousarray(col_idx, np.int32)
         self.values = np.ascontiguousarray(values, np.float64)
@@ -174,7 +175,8 @@ class PcgSolver:
             keep_fp64=int(keep_fp64), replace_every=replace_every, replace_drop=replace_drop,
             block_threads=block_threads, blocks_per_sm=blocks_per_sm,
             barrier_timeout_s=barrier_timeout_s, device=device, row_sum_form=int(row_sum_form), index16=int(index16),
-            l2_persist=int(l2_persist), resident=int(resident), barriers_per_iter=int(barriers_per_iter))
+            l2_persist=int(l2_persist), resident=int(resident), barriers_per_iter=int(barriers_per_iter),
+            restart_on_replace=int(restart_on_replace))
         h = C.c_void_p()
         check(lib.xplus_pcg_create(ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), self.n,
                                    C.byref(self.opts), C.byref(h)))

@@ -193,6 +193,51 @@ int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double
                       double tau, int max_iters, int n, void* stream);
 
 /* ------------------------------------------------------------------------------------
+ * Batched solver: many independent SPD systems in one persistent launch.  The reference
+ * solves one system per launch (host/cuper_control_xrt_host.cpp:205-272, one
+ * cuper_pcg_control_kernel run per dataset); a caller with many systems looped over
+ * CsrDataset::load + run.  Here all systems are resident at once and thread-block clusters
+ * take them from a device work queue, largest first.  Each system follows the single-system
+ * iteration (row-sum form, FP32 vectors, FP64 solution and FP64 residual replacement) and
+ * gets its own status / iterations / FP64 true residual.  Vectors b and x are the systems'
+ * vectors concatenated in the order they were given, each in its original row order.
+ * ------------------------------------------------------------------------------------ */
+typedef struct xplus_batch xplus_batch;
+
+/* nsys systems, system k given as CSR (row_ptrs[k][ns[k]+1], col_idxs[k], values[k], FP64).
+ * opts: value_type F32 | BF16 | F16, vector_type F32, sigma, chunk, index16, replace_drop,
+ * replace_every, restart_on_replace, device; the others are ignored.  The launch shape starts
+ * at clusters of 4 CTAs x 512 threads (xplus_batch_set_launch / xplus_batch_autotune). */
+int xplus_batch_create(int nsys, const int* const* row_ptrs, const int* const* col_idxs,
+                       const double* const* values, const int* ns, const xplus_opts* opts,
+                       xplus_batch** out);
+int xplus_batch_destroy(xplus_batch* h);
+/* cluster in {1, 2, 4, 8} CTAs, block_threads in {128, 256, 512}; the grid is as many
+ * clusters as the device holds at once.  XPLUS_ERR_CUDA when the shape cannot launch. */
+int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads);
+/* Times every launch shape on `iters` PCG iterations of every system and keeps the fastest. */
+int xplus_batch_autotune(xplus_batch* h, int iters, int* cluster, int* block_threads, double* best_ms);
+/* Blocking solve with host vectors of length sum(ns) (x0 NULL: zeros).  tau / tau_mode /
+ * max_iters as xplus_pcg_solve, applied to every system (relative tolerances per system). */
+int xplus_batch_solve(xplus_batch* h, const double* b, const double* x0, double tau, int tau_mode,
+                      int max_iters, double* x_out);
+/* Asynchronous solve on device vectors (d_x: x0 in, x out) enqueued on `stream` (NULL: the
+ * handle's stream) as one CUDA graph (gather, persistent launch, scatter).  The graph is
+ * captured on the first call and replayed while d_b, d_x, tau, tau_mode, max_iters and the
+ * launch shape stay the same. */
+int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, double tau, int tau_mode,
+                             int max_iters, void* stream);
+/* Outcome of the last solve, per system (each array nullable, nsys long): status, inner
+ * iterations, FP64 residual replacements, FP64 true relative residual, device time from the
+ * system's start to its end; kernel_ms: device time of the whole solve. */
+int xplus_batch_results(xplus_batch* h, int* status, int* iterations, int* replacements, double* true_rel,
+                        double* system_ms, double* kernel_ms);
+/* Total rows and stored nonzeros, launch shape, and the bytes one SpMV over every system
+ * moves in the stored format (off-diagonal value + index, row sums, x read, y written). */
+int xplus_batch_info(xplus_batch* h, int64_t* total_n, int64_t* total_nnz, int* cluster, int* block_threads,
+                     int* grid, int64_t* spmv_bytes);
+
+/* ------------------------------------------------------------------------------------
  * Multi-kernel ABI: the five "kernel functions" of archived/include/cg_kernels.hpp:9-54
  * with the same names and arguments, run on the GPU.  Pointers may be device pointers
  * (zero copy) or plain host pointers (staged through device buffers), so the reference's

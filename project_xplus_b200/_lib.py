@@ -95,6 +95,14 @@ _SIGS = {
     "update_xrz_kernel": (None, [_p, _p, _p, _p, _p, _p, _p, _d, _i]),
     "update_p_kernel": (None, [_p, _p, _d, _i]),
     "xplus_update_xrz_noalloc": (_i, [_p, _p, _p, _p, _p, _p, _p, _d, _i, _p]),
+    "xplus_batch_create": (_i, [_i, _p, _p, _p, _p, C.POINTER(XplusOpts), C.POINTER(_p)]),
+    "xplus_batch_destroy": (_i, [_p]),
+    "xplus_batch_set_launch": (_i, [_p, _i, _i]),
+    "xplus_batch_autotune": (_i, [_p, _i, _ip, _ip, _dp]),
+    "xplus_batch_solve": (_i, [_p, _p, _p, _d, _i, _i, _p]),
+    "xplus_batch_solve_device": (_i, [_p, _p, _p, _d, _i, _i, _p]),
+    "xplus_batch_results": (_i, [_p, _p, _p, _p, _p, _p, _dp]),
+    "xplus_batch_info": (_i, [_p, C.POINTER(_i64), C.POINTER(_i64), _ip, _ip, _ip, C.POINTER(_i64)]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -1,0 +1,999 @@
+// batch.cu -- many independent SPD systems solved by one persistent launch.
+//
+// The systems' SELL-C-sigma images are concatenated into one slice list (each system keeps
+// its own sigma-sort and padding; columns are global rows, or int16 offsets from the row).
+// A launch of thread-block clusters takes systems from a device work queue, largest first
+// (nnz * sqrt(n), a proxy for work = nnz x iterations): rank 0 of a cluster pops the next
+// system id with one atomicAdd and the cluster's CTAs split that system's slices.  Each
+// system runs the Jacobi-PCG iteration of pcg_kernels.cu (row-sum form, FP32 vectors, FP64
+// solution and FP64 residual replacement) with cluster barriers in place of grid barriers
+// and dot products reduced through distributed shared memory in cluster-rank order, so every
+// CTA of the cluster takes the same control decisions.  No wait spans two clusters, so the
+// launch needs no co-residency: clusters that start late simply find the queue shorter.
+// Control flow, breakdown tests and status codes: kernels/cuper_pcg_control_kernel.cpp:1069-1235.
+#include <cooperative_groups.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <type_traits>
+#include <vector>
+
+#include "common.hpp"
+#include "device_common.cuh"
+#include "pcg_device.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace xplus {
+namespace {
+
+using namespace dev;
+
+struct BatchArgs {
+    int nsys;
+    const int* order;         // queue: system ids in the order they are taken
+    int* head;                // queue head (atomic), zero at launch
+    const int* sys_slice0;    // [nsys + 1] first global slice of each system
+    const int* sys_n;         // rows of each system
+    const float* sys_scale;   // stored off-diagonal value = a_ij / scale (FP16), else 1
+    const long long* slice_ptr;
+    const void* col;          // int32 global rows or int16 offsets from the row
+    const void* val;          // off-diagonal weights (row-sum form), VT
+    const double* val64;      // FP64 copy of the off-diagonals, same layout
+    const double* diag64;     // FP64 diagonal
+    const float* rowsum;      // s_i = sum_j a_ij
+    const float* minv;        // 1 / a_ii
+    const double* b64;
+    double* x64;
+    NodeRec<float>* rec;      // {z, p} per row
+    float* r;
+    float* ap;
+    double tau;
+    int tau_mode;             // XPLUS_TAU_ABS_RR | XPLUS_TAU_REL_TRUE
+    int max_iters;            // <= 0: max(4n, 1000) per system
+    int replace_every;
+    double replace_drop2;     // squared ||r|| drop that triggers a replacement (0: off)
+    int restart_on_replace;
+    int* out_status;
+    int* out_iters;
+    int* out_repl;
+    double* out_true_rel;
+    long long* out_ns;        // device time of each system (first pop to exit residual)
+};
+
+__device__ __forceinline__ NodeRec<float> ldcg_rec(const NodeRec<float>* q) {
+    const float2 v = __ldcg(reinterpret_cast<const float2*>(q));
+    return NodeRec<float>{v.x, v.y};
+}
+
+// Sum of NV per-thread values over the cluster: block tree, then the per-CTA partials read
+// through distributed shared memory in rank order (same result in every CTA).  Two banks of
+// partials: a CTA that runs ahead writes the other bank, and a bank is rewritten only after
+// the next cluster barrier, by which time every reader has finished with it.
+template <int NV>
+__device__ __forceinline__ void cluster_sum(cg::cluster_group& cl, double (&v)[NV], double* s_red,
+                                            double (*s_part)[4], double* s_tot, int& pbank) {
+    block_sum<NV>(v, s_red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) s_part[pbank][q] = v[q];
+    cl.sync();
+    if (threadIdx.x < NV) {
+        const int cs = static_cast<int>(cl.num_blocks());
+        double t = 0.0;
+        for (int rk = 0; rk < cs; ++rk) t += *cl.map_shared_rank(&s_part[pbank][threadIdx.x], rk);
+        s_tot[threadIdx.x] = t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = s_tot[q];
+    pbank ^= 1;
+}
+
+// FP64 row of A times x: stored off-diagonals (FP64 copy) plus the exact diagonal.  x of
+// neighbouring rows is read through L2 (another CTA of the cluster wrote it).
+template <int CHUNK, typename IT>
+__device__ __forceinline__ double batch_row64(const BatchArgs& a, int s, int lane) {
+    const long long base = a.slice_ptr[s];
+    const int w = static_cast<int>((a.slice_ptr[s + 1] - base) >> 5);
+    const int row = s * 32 + lane;
+    const double* vp = a.val64 + base + lane * CHUNK;
+    const IT* cp = static_cast<const IT*>(a.col) + base + lane * CHUNK;
+    double acc = 0.0;
+    for (int c = 0; c < w; c += CHUNK) {
+        double v[CHUNK];
+        int cc[CHUNK];
+        ChunkLoad<double, CHUNK>::run(vp, v);
+        ColLoad<CHUNK, IT>::run(cp, row, cc);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) acc += v[q] * __ldcg(a.x64 + cc[q]);
+        vp += 32 * CHUNK;
+        cp += 32 * CHUNK;
+    }
+    return acc + a.diag64[row] * __ldcg(a.x64 + row);
+}
+
+template <typename VT, int CHUNK, typename IT>
+__global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
+    constexpr int NS = 2;  // slices of one warp in flight together
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ double s_red[32 * 4];
+    __shared__ double s_part[2][4];
+    __shared__ double s_tot[4];
+    __shared__ int s_item[2];
+    const int crank = static_cast<int>(cl.block_rank());
+    const int csize = static_cast<int>(cl.num_blocks());
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const VT* __restrict__ val = static_cast<const VT*>(a.val);
+    const IT* __restrict__ col = static_cast<const IT*>(a.col);
+    int pbank = 0, ibank = 0;
+
+    for (;;) {
+        if (crank == 0 && threadIdx.x == 0) s_item[ibank] = atomicAdd(a.head, 1);
+        cl.sync();
+        const int qi = *cl.map_shared_rank(&s_item[ibank], 0);
+        ibank ^= 1;
+        if (qi >= a.nsys) {
+            // every CTA has read rank 0's queue item before any CTA of the cluster exits: a
+            // CTA's shared memory must outlive all distributed-shared-memory reads of it
+            cl.sync();
+            break;
+        }
+        const long long t_begin = globaltimer_ns();
+        const int sys = a.order[qi];
+        const int S0 = a.sys_slice0[sys];
+        const int ns = a.sys_slice0[sys + 1] - S0;
+        const int per = (ns + csize - 1) / csize;
+        const int sb = S0 + min(ns, crank * per);
+        const int se = S0 + min(ns, (crank + 1) * per);
+        const int n = a.sys_n[sys];
+        const float vscale = a.sys_scale[sys];
+        const int max_iters = a.max_iters > 0 ? a.max_iters : max(4 * n, 1000);
+        const bool true_mode = a.tau_mode == XPLUS_TAU_REL_TRUE;
+
+        // residual phase: r = b - A x in FP64 rounded to FP32, z = M^-1 r into the record
+        // (init also clears p); totals r.z, r.r, ||b - A x||^2, ||b||^2
+        auto residual_phase = [&](bool init, double (&acc)[4]) {
+            acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+            for (int s = sb + warp; s < se; s += wpb) {
+                const int row = s * 32 + lane;
+                const double bv = a.b64[row];
+                const double rt = bv - batch_row64<CHUNK, IT>(a, s, lane);
+                const float rv = static_cast<float>(rt);
+                const float zv = a.minv[row] * rv;
+                a.r[row] = rv;
+                if (init) store_rec(a.rec + row, zv, 0.0f);
+                else a.rec[row].z = zv;
+                acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
+                acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
+                acc[2] += rt * rt;
+                acc[3] += bv * bv;
+            }
+            cluster_sum<4>(cl, acc, s_red, s_part, s_tot, pbank);
+        };
+
+        double tot[4];
+        residual_phase(true, tot);
+        double rz = tot[0], rr = tot[1], true_rr = tot[2];
+        const double bb = tot[3];
+        const double tau_true_rr = a.tau * a.tau * bb;
+        double rr_at_replace = rr, best_true = true_rr;
+        double pap = 0.0, alpha = 0.0, beta = 0.0;
+        int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0;
+        bool stagnated = false;
+        const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau);
+
+        if (converged_now) {
+            status = XPLUS_CONVERGED;
+        } else {
+            for (int it = 0; it < max_iters; ++it) {
+                if (bad(rz) || bad(rr) || fabs(rz) <= kBreakdownEps) {
+                    status = XPLUS_BREAKDOWN;
+                    break;
+                }
+                const float be = static_cast<float>(beta);
+                // ---- phase A: p' = z + beta p (neighbours' p' recomputed), Ap', p'.Ap' ----
+                {
+                    double acc[1] = {0.0};
+                    for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
+                        int2 sl[NS];
+                        int row[NS];
+                        float pi[NS], y[NS];
+                        int wmax = 0;
+#pragma unroll
+                        for (int k = 0; k < NS; ++k) {
+                            const int s = s0 + k * wpb;
+                            const bool on = s < se;
+                            const long long p0 = on ? a.slice_ptr[s] : 0;
+                            sl[k] = on ? make_int2(static_cast<int>(p0), static_cast<int>((a.slice_ptr[s + 1] - p0) >> 5))
+                                       : make_int2(0, 0);
+                            row[k] = on ? s * 32 + lane : -1;
+                            wmax = max(wmax, sl[k].y);
+                            const NodeRec<float> me = on ? ldcg_rec(a.rec + row[k]) : NodeRec<float>{0.0f, 0.0f};
+                            pi[k] = node_pnew(me.z, be, me.p);
+                            y[k] = 0.0f;
+                        }
+                        for (int c = 0; c < wmax; c += 2 * CHUNK) {
+                            float v[NS][2][CHUNK];
+                            int cc[NS][2][CHUNK];
+#pragma unroll
+                            for (int k = 0; k < NS; ++k)
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                    if (c + h * CHUNK < sl[k].y) {
+                                        const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
+                                        ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
+                                        ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                                    } else {
+#pragma unroll
+                                        for (int q = 0; q < CHUNK; ++q) {
+                                            v[k][h][q] = 0.0f;
+                                            cc[k][h][q] = -1;
+                                        }
+                                    }
+                                }
+                            NodeRec<float> nb[NS][2][CHUNK];
+#pragma unroll
+                            for (int k = 0; k < NS; ++k)
+#pragma unroll
+                                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                                    for (int q = 0; q < CHUNK; ++q)
+                                        nb[k][h][q] = cc[k][h][q] >= 0 ? ldcg_rec(a.rec + cc[k][h][q])
+                                                                       : NodeRec<float>{0.0f, 0.0f};
+#pragma unroll
+                            for (int k = 0; k < NS; ++k)
+#pragma unroll
+                                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                                    for (int q = 0; q < CHUNK; ++q)
+                                        y[k] += v[k][h][q] * (node_pnew(nb[k][h][q].z, be, nb[k][h][q].p) - pi[k]);
+                        }
+#pragma unroll
+                        for (int k = 0; k < NS; ++k) {
+                            if (row[k] < 0) continue;
+                            const float yk = y[k] * vscale + a.rowsum[row[k]] * pi[k];
+                            a.ap[row[k]] = yk;
+                            acc[0] += static_cast<double>(pi[k]) * static_cast<double>(yk);
+                        }
+                    }
+                    cluster_sum<1>(cl, acc, s_red, s_part, s_tot, pbank);
+                    pap = acc[0];
+                }
+                if (bad(pap) || fabs(pap) <= kBreakdownEps) {
+                    status = XPLUS_BREAKDOWN;
+                    break;
+                }
+                const double rz_old = rz;
+                alpha = rz / pap;
+                if (bad(alpha)) {
+                    status = XPLUS_BREAKDOWN;
+                    break;
+                }
+                // ---- phase B: x += alpha p' (FP64), r -= alpha Ap', z = M^-1 r, r.z, r.r ----
+                double rz_new, rr_new;
+                {
+                    double acc[2] = {0.0, 0.0};
+                    const float al = static_cast<float>(alpha);
+                    for (int s = sb + warp; s < se; s += wpb) {
+                        const int row = s * 32 + lane;
+                        const NodeRec<float> me = ldcg_rec(a.rec + row);
+                        const float pv = node_pnew(me.z, be, me.p);
+                        a.x64[row] += alpha * static_cast<double>(pv);
+                        const float rv = a.r[row] - al * a.ap[row];
+                        const float zv = a.minv[row] * rv;
+                        a.r[row] = rv;
+                        store_rec(a.rec + row, zv, pv);
+                        acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
+                        acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
+                    }
+                    cluster_sum<2>(cl, acc, s_red, s_part, s_tot, pbank);
+                    rz_new = acc[0];
+                    rr_new = acc[1];
+                }
+                iterations = it + 1;
+                if (bad(rz_new) || bad(rr_new)) {
+                    rz = rz_new;
+                    rr = rr_new;
+                    status = XPLUS_BREAKDOWN;
+                    break;
+                }
+                bool do_replace = false;
+                if (true_mode) {
+                    if (rr_new <= tau_true_rr) do_replace = true;
+                    if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
+                    if (a.replace_drop2 > 0.0 && rr_new <= a.replace_drop2 * rr_at_replace) do_replace = true;
+                }
+                if (do_replace) {
+                    double t4[4];
+                    residual_phase(false, t4);
+                    rz_new = t4[0];
+                    rr_new = t4[1];
+                    true_rr = t4[2];
+                    ++replacements;
+                    rr_at_replace = rr_new;
+                    if (true_rr < 0.9 * best_true) {
+                        best_true = true_rr;
+                        stagnant = 0;
+                    } else if (++stagnant >= 8) {
+                        stagnated = true;
+                    }
+                }
+                rz = rz_new;
+                rr = rr_new;
+                if (true_mode ? (do_replace && true_rr <= tau_true_rr) : (rr <= a.tau)) {
+                    status = XPLUS_CONVERGED;
+                    break;
+                }
+                if (stagnated) break;
+                if (fabs(rz_old) <= kBreakdownEps) {
+                    status = XPLUS_BREAKDOWN;
+                    break;
+                }
+                beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
+                if (bad(beta)) {
+                    status = XPLUS_BREAKDOWN;
+                    break;
+                }
+            }
+        }
+        if (status == XPLUS_MAX_ITER && !true_mode && rr <= a.tau) status = XPLUS_CONVERGED;
+
+        // exit: FP64 true residual of the final x
+        double fin[1] = {0.0};
+        for (int s = sb + warp; s < se; s += wpb) {
+            const int row = s * 32 + lane;
+            const double rt = a.b64[row] - batch_row64<CHUNK, IT>(a, s, lane);
+            fin[0] += rt * rt;
+        }
+        cluster_sum<1>(cl, fin, s_red, s_part, s_tot, pbank);
+        if (crank == 0 && threadIdx.x == 0) {
+            a.out_status[sys] = status;
+            a.out_iters[sys] = iterations;
+            a.out_repl[sys] = replacements;
+            a.out_true_rel[sys] = bb > 0.0 ? sqrt(fin[0] / bb) : sqrt(fin[0]);
+            a.out_ns[sys] = globaltimer_ns() - t_begin;
+        }
+    }
+}
+
+// dst[i] = src[map[i]] (0 where map[i] < 0: padding rows)
+__global__ void batch_gather_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                    const int* __restrict__ map, int rows) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < rows) {
+        const int m = map[i];
+        dst[i] = m >= 0 ? src[m] : 0.0;
+    }
+}
+
+__global__ void batch_scatter_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                     const int* __restrict__ map, int rows) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < rows) {
+        const int m = map[i];
+        if (m >= 0) dst[m] = src[i];
+    }
+}
+
+using BatchKernel = void (*)(BatchArgs);
+
+template <typename VT, typename IT>
+BatchKernel pick_chunk(int chunk) {
+    switch (chunk) {
+        case 1: return pcg_batch_kernel<VT, 1, IT>;
+        case 2: return pcg_batch_kernel<VT, 2, IT>;
+        case 4: return pcg_batch_kernel<VT, 4, IT>;
+    }
+    return nullptr;
+}
+template <typename IT>
+BatchKernel pick_vt(int vt, int chunk) {
+    switch (vt) {
+        case XPLUS_F32: return pick_chunk<float, IT>(chunk);
+        case XPLUS_BF16: return pick_chunk<__nv_bfloat16, IT>(chunk);
+        case XPLUS_F16: return pick_chunk<__half, IT>(chunk);
+    }
+    return nullptr;
+}
+BatchKernel pick_kernel(int vt, int chunk, bool idx16) {
+    return idx16 ? pick_vt<short>(vt, chunk) : pick_vt<int>(vt, chunk);
+}
+
+}  // namespace
+}  // namespace xplus
+
+struct xplus_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    xplus_opts opts{};
+    int nsys = 0;
+    int rows = 0;          // concatenated SELL rows (padding included)
+    int n_slices = 0;
+    int64_t total_n = 0, total_nnz = 0, slots = 0;
+    bool idx16 = true;
+    xplus::BatchKernel kernel = nullptr;
+    int cluster = 4, tpb = 512, grid = 0;
+    std::vector<int> sys_n;
+    std::vector<int64_t> sys_off;   // original-order offsets of each system in b / x
+    // device data
+    int* d_order = nullptr;
+    int* d_head = nullptr;
+    int* d_slice0 = nullptr;
+    int* d_sysn = nullptr;
+    float* d_scale = nullptr;
+    long long* d_slice_ptr = nullptr;
+    void* d_col = nullptr;
+    void* d_val = nullptr;
+    double* d_val64 = nullptr;
+    double* d_diag64 = nullptr;
+    float* d_rowsum = nullptr;
+    float* d_minv = nullptr;
+    int* d_map = nullptr;
+    double* d_b64 = nullptr;
+    double* d_x64 = nullptr;
+    void* d_rec = nullptr;
+    float* d_r = nullptr;
+    float* d_ap = nullptr;
+    double* d_bio = nullptr;
+    double* d_xio = nullptr;
+    int* d_status = nullptr;
+    int* d_iters = nullptr;
+    int* d_repl = nullptr;
+    double* d_true_rel = nullptr;
+    long long* d_ns = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // CUDA graph of the last device solve, replayed while its arguments stay the same
+    cudaGraphExec_t gexec = nullptr;
+    const double* g_b = nullptr;
+    double* g_x = nullptr;
+    double g_tau = 0.0;
+    int g_mode = -1, g_iters = 0, g_cluster = 0, g_tpb = 0;
+    bool pending = false;
+    double last_ms = 0.0;
+    std::vector<void*> allocations;
+};
+
+namespace xplus {
+namespace {
+
+void bcheck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+template <typename T>
+T* balloc(xplus_batch* h, size_t count) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 256));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    h->allocations.push_back(p);
+    return static_cast<T*>(p);
+}
+
+template <typename T>
+void upload(xplus_batch* h, T* dst, const std::vector<T>& src) {
+    bcheck(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream), "H2D");
+}
+
+void batch_destroy(xplus_batch* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    for (void* p : h->allocations) cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaGetLastError();
+    delete h;
+}
+
+// Clusters of `cluster` CTAs of `tpb` threads that the device holds at once (0: not launchable).
+int active_clusters(xplus_batch* h, int cluster, int tpb) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster);
+    cfg.blockDim = dim3(tpb);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int num = 0;
+    if (cudaOccupancyMaxActiveClusters(&num, h->kernel, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return num;
+}
+
+void set_launch(xplus_batch* h, int cluster, int tpb) {
+    require(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8, XPLUS_ERR_ARG,
+            "cluster must be 1, 2, 4 or 8");
+    require(tpb == 128 || tpb == 256 || tpb == 512, XPLUS_ERR_ARG, "block_threads must be 128, 256 or 512");
+    const int num = active_clusters(h, cluster, tpb);
+    require(num > 0, XPLUS_ERR_CUDA, "cluster shape not launchable on this device");
+    h->cluster = cluster;
+    h->tpb = tpb;
+    h->grid = num * cluster;
+}
+
+void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_idxs,
+                  const double* const* values, const int* ns, const xplus_opts* opts_in, xplus_batch** out) {
+    require(nsys > 0 && row_ptrs && col_idxs && values && ns && out, XPLUS_ERR_ARG, "null argument or nsys <= 0");
+    xplus_opts o;
+    xplus_opts_default(&o);
+    if (opts_in) o = *opts_in;
+    require(o.value_type == XPLUS_F32 || o.value_type == XPLUS_BF16 || o.value_type == XPLUS_F16, XPLUS_ERR_ARG,
+            "batch value_type must be F32, BF16 or F16");
+    require(o.vector_type == XPLUS_F32, XPLUS_ERR_ARG, "batch vectors are FP32");
+    require(o.slice_height == 32, XPLUS_ERR_ARG, "slice_height must be 32");
+    require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
+    require(o.sigma >= 1, XPLUS_ERR_ARG, "sigma must be >= 1");
+    for (int k = 0; k < nsys; ++k) {
+        require(row_ptrs[k] && col_idxs[k] && values[k] && ns[k] > 0, XPLUS_ERR_ARG, "bad system " + std::to_string(k));
+        validate_csr(ns[k], row_ptrs[k], col_idxs[k], row_ptrs[k][ns[k]]);
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, "no CUDA device available (the solver has no CPU path)");
+    }
+    require(o.device >= 0 && o.device < count, XPLUS_ERR_ARG, "device ordinal out of range");
+    cudaDeviceProp prop;
+    bcheck(cudaGetDeviceProperties(&prop, o.device), "cudaGetDeviceProperties");
+    require(prop.major == 10, XPLUS_ERR_CUDA, "this build targets sm_100 (B200) devices only");
+    bcheck(cudaSetDevice(o.device), "cudaSetDevice");
+
+    // per-system SELL images in parallel (row-sum form: off-diagonals in the slots)
+    std::vector<SellHost> S(static_cast<size_t>(nsys));
+    std::vector<std::vector<double>> diag(static_cast<size_t>(nsys));
+    std::vector<std::string> errs(static_cast<size_t>(nsys));
+    std::vector<int> codes(static_cast<size_t>(nsys), 0);
+    {
+        const int nt = std::max(1, std::min<int>(nsys, static_cast<int>(std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                for (int k = t; k < nsys; k += nt) {
+                    try {
+                        const size_t K = static_cast<size_t>(k);
+                        diag[K].resize(static_cast<size_t>(ns[k]));
+                        jacobi_diag(ns[k], row_ptrs[k], col_idxs[k], values[k], diag[K].data());
+                        for (double d : diag[K])
+                            require(std::fabs(d) > 1.0e-30, XPLUS_ERR_DATA, "zero diagonal entry while building Jacobi inverse");
+                        sell_build(ns[k], row_ptrs[k], col_idxs[k], values[k], 32, o.sigma, o.chunk, 1, S[K]);
+                    } catch (const Error& e) {
+                        codes[static_cast<size_t>(k)] = e.code;
+                        errs[static_cast<size_t>(k)] = e.what();
+                    } catch (const std::exception& e) {
+                        codes[static_cast<size_t>(k)] = XPLUS_ERR_ARG;
+                        errs[static_cast<size_t>(k)] = e.what();
+                    }
+                }
+            });
+        for (auto& th : pool) th.join();
+        for (int k = 0; k < nsys; ++k)
+            if (codes[static_cast<size_t>(k)]) throw Error(codes[static_cast<size_t>(k)], "system " + std::to_string(k) + ": " + errs[static_cast<size_t>(k)]);
+    }
+
+    auto* h = new xplus_batch();
+    h->device = o.device;
+    try {
+        h->opts = o;
+        h->nsys = nsys;
+        h->sys_n.assign(ns, ns + nsys);
+        h->sys_off.assign(static_cast<size_t>(nsys) + 1, 0);
+        std::vector<int> slice0(static_cast<size_t>(nsys) + 1, 0);
+        int64_t slots = 0;
+        for (int k = 0; k < nsys; ++k) {
+            const size_t K = static_cast<size_t>(k);
+            h->sys_off[K + 1] = h->sys_off[K] + ns[k];
+            require(static_cast<int64_t>(slice0[K]) + S[K].n_slices < (1LL << 26), XPLUS_ERR_ARG, "batch too large");
+            slice0[K + 1] = slice0[K] + S[K].n_slices;
+            slots += S[K].slots;
+            h->total_nnz += row_ptrs[k][ns[k]];
+        }
+        h->total_n = h->sys_off[static_cast<size_t>(nsys)];
+        h->n_slices = slice0[static_cast<size_t>(nsys)];
+        h->rows = h->n_slices * 32;
+        h->slots = slots;
+        require(slots < (1LL << 31) && h->total_n < (1LL << 31), XPLUS_ERR_ARG, "batch too large (2^31 slots)");
+        // int16 offsets when every system's ordered bandwidth allows
+        bool idx16 = o.index16 != 0;
+        for (int k = 0; k < nsys && idx16; ++k) {
+            const SellHost& s = S[static_cast<size_t>(k)];
+            for (int sl = 0; sl < s.n_slices && idx16; ++sl)
+                for (int64_t pos = s.slice_ptr[static_cast<size_t>(sl)]; pos < s.slice_ptr[static_cast<size_t>(sl) + 1]; ++pos) {
+                    const int lane = static_cast<int>(((pos - s.slice_ptr[static_cast<size_t>(sl)]) % (32 * o.chunk)) / o.chunk);
+                    const int d = s.col[static_cast<size_t>(pos)] - (sl * 32 + lane);
+                    if (d < -32768 || d > 32767) {
+                        idx16 = false;
+                        break;
+                    }
+                }
+        }
+        h->idx16 = idx16;
+        h->kernel = pick_kernel(o.value_type, o.chunk, idx16);
+        require(h->kernel != nullptr, XPLUS_ERR_ARG, "no batch kernel for these options");
+
+        // concatenated host image
+        const size_t R = static_cast<size_t>(h->rows);
+        std::vector<long long> sp(static_cast<size_t>(h->n_slices) + 1, 0);
+        std::vector<int> col32;
+        std::vector<short> col16;
+        if (idx16) col16.resize(static_cast<size_t>(slots));
+        else col32.resize(static_cast<size_t>(slots));
+        std::vector<double> v64(static_cast<size_t>(slots));
+        std::vector<double> d64(R, 0.0), rs(R, 0.0), mi(R, 0.0);
+        std::vector<int> map(R, -1);
+        std::vector<float> scale(static_cast<size_t>(nsys), 1.0f);
+        std::vector<unsigned char> vbytes(static_cast<size_t>(slots) * (o.value_type == XPLUS_F32 ? 4 : 2));
+        int64_t base = 0;
+        for (int k = 0; k < nsys; ++k) {
+            const size_t K = static_cast<size_t>(k);
+            const SellHost& s = S[K];
+            const int r0 = slice0[K] * 32;
+            for (int sl = 0; sl < s.n_slices; ++sl)
+                sp[static_cast<size_t>(slice0[K] + sl)] = base + s.slice_ptr[static_cast<size_t>(sl)];
+            double vmax = 0.0;
+            for (double x : s.val) vmax = std::max(vmax, std::fabs(x));
+            const double sc = (o.value_type == XPLUS_F16 && vmax > 0.0)
+                                  ? std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(vmax))) - 15) : 1.0;
+            scale[K] = static_cast<float>(sc);
+            for (int sl = 0; sl < s.n_slices; ++sl)
+                for (int64_t pos = s.slice_ptr[static_cast<size_t>(sl)]; pos < s.slice_ptr[static_cast<size_t>(sl) + 1]; ++pos) {
+                    const size_t g = static_cast<size_t>(base + pos);
+                    const int lane = static_cast<int>(((pos - s.slice_ptr[static_cast<size_t>(sl)]) % (32 * o.chunk)) / o.chunk);
+                    const int c = s.col[static_cast<size_t>(pos)];
+                    if (idx16) col16[g] = static_cast<short>(c - (sl * 32 + lane));
+                    else col32[g] = r0 + c;
+                    const double v = s.val[static_cast<size_t>(pos)];
+                    v64[g] = v;
+                    if (o.value_type == XPLUS_F32) reinterpret_cast<float*>(vbytes.data())[g] = static_cast<float>(v);
+                    else if (o.value_type == XPLUS_F16) reinterpret_cast<__half*>(vbytes.data())[g] = __double2half(v / sc);
+                    else reinterpret_cast<__nv_bfloat16*>(vbytes.data())[g] = __double2bfloat16(v);
+                }
+            base += s.slots;
+            for (int i = 0; i < s.n; ++i) {
+                const int old = s.perm[static_cast<size_t>(i)];
+                const size_t gi = static_cast<size_t>(r0 + i);
+                const double d = diag[K][static_cast<size_t>(old)];
+                d64[gi] = d;
+                mi[gi] = 1.0 / d;
+                double acc = 0.0;
+                for (int q = row_ptrs[k][old]; q < row_ptrs[k][old + 1]; ++q) acc += values[k][q];
+                rs[gi] = acc;
+                map[gi] = static_cast<int>(h->sys_off[K] + old);
+            }
+        }
+        sp[static_cast<size_t>(h->n_slices)] = base;
+        // queue: largest first by nnz * sqrt(n) (PCG iterations grow like sqrt(n) on these grids)
+        std::vector<int> order(static_cast<size_t>(nsys));
+        for (int k = 0; k < nsys; ++k) order[static_cast<size_t>(k)] = k;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            const double wa = static_cast<double>(row_ptrs[a][ns[a]]) * std::sqrt(static_cast<double>(ns[a]));
+            const double wb = static_cast<double>(row_ptrs[b][ns[b]]) * std::sqrt(static_cast<double>(ns[b]));
+            return wa > wb;
+        });
+
+        bcheck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        bcheck(cudaEventCreate(&h->ev0), "cudaEventCreate");
+        bcheck(cudaEventCreate(&h->ev1), "cudaEventCreate");
+        std::vector<int> sysn(ns, ns + nsys);
+        std::vector<float> rsf(rs.begin(), rs.end()), mif(mi.begin(), mi.end());
+        h->d_order = balloc<int>(h, order.size());
+        h->d_head = balloc<int>(h, 1);
+        h->d_slice0 = balloc<int>(h, slice0.size());
+        h->d_sysn = balloc<int>(h, sysn.size());
+        h->d_scale = balloc<float>(h, scale.size());
+        h->d_slice_ptr = balloc<long long>(h, sp.size());
+        h->d_col = balloc<unsigned char>(h, static_cast<size_t>(slots) * (idx16 ? 2 : 4));
+        h->d_val = balloc<unsigned char>(h, vbytes.size());
+        h->d_val64 = balloc<double>(h, v64.size());
+        h->d_diag64 = balloc<double>(h, R);
+        h->d_rowsum = balloc<float>(h, R);
+        h->d_minv = balloc<float>(h, R);
+        h->d_map = balloc<int>(h, R);
+        h->d_b64 = balloc<double>(h, R);
+        h->d_x64 = balloc<double>(h, R);
+        h->d_rec = balloc<NodeRec<float>>(h, R);
+        h->d_r = balloc<float>(h, R);
+        h->d_ap = balloc<float>(h, R);
+        h->d_bio = balloc<double>(h, static_cast<size_t>(h->total_n));
+        h->d_xio = balloc<double>(h, static_cast<size_t>(h->total_n));
+        h->d_status = balloc<int>(h, static_cast<size_t>(nsys));
+        h->d_iters = balloc<int>(h, static_cast<size_t>(nsys));
+        h->d_repl = balloc<int>(h, static_cast<size_t>(nsys));
+        h->d_true_rel = balloc<double>(h, static_cast<size_t>(nsys));
+        h->d_ns = balloc<long long>(h, static_cast<size_t>(nsys));
+        upload(h, h->d_order, order);
+        upload(h, h->d_slice0, slice0);
+        upload(h, h->d_sysn, sysn);
+        upload(h, h->d_scale, scale);
+        upload(h, h->d_slice_ptr, sp);
+        if (idx16) upload(h, static_cast<short*>(h->d_col), col16);
+        else upload(h, static_cast<int*>(h->d_col), col32);
+        upload(h, static_cast<unsigned char*>(h->d_val), vbytes);
+        upload(h, h->d_val64, v64);
+        upload(h, h->d_diag64, d64);
+        upload(h, h->d_rowsum, rsf);
+        upload(h, h->d_minv, mif);
+        upload(h, h->d_map, map);
+        bcheck(cudaMemsetAsync(h->d_x64, 0, R * sizeof(double), h->stream), "memset");
+        bcheck(cudaMemsetAsync(h->d_rec, 0, R * sizeof(NodeRec<float>), h->stream), "memset");
+        bcheck(cudaStreamSynchronize(h->stream), "sync");
+        set_launch(h, 4, 512);
+        *out = h;
+    } catch (...) {
+        batch_destroy(h);
+        throw;
+    }
+}
+
+// Enqueues head reset, the persistent launch (no gather / scatter): b64 and x64 are set.
+void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int cluster, int tpb, int grid,
+                    cudaStream_t st) {
+    BatchArgs a{};
+    a.nsys = h->nsys;
+    a.order = h->d_order;
+    a.head = h->d_head;
+    a.sys_slice0 = h->d_slice0;
+    a.sys_n = h->d_sysn;
+    a.sys_scale = h->d_scale;
+    a.slice_ptr = h->d_slice_ptr;
+    a.col = h->d_col;
+    a.val = h->d_val;
+    a.val64 = h->d_val64;
+    a.diag64 = h->d_diag64;
+    a.rowsum = h->d_rowsum;
+    a.minv = h->d_minv;
+    a.b64 = h->d_b64;
+    a.x64 = h->d_x64;
+    a.rec = static_cast<NodeRec<float>*>(h->d_rec);
+    a.r = h->d_r;
+    a.ap = h->d_ap;
+    a.tau = tau;
+    a.tau_mode = tau_mode;
+    a.max_iters = max_iters;
+    a.replace_every = h->opts.replace_every;
+    a.replace_drop2 = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
+    const bool low = h->opts.value_type != XPLUS_F32;
+    a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 1 : 0) : h->opts.restart_on_replace;
+    a.out_status = h->d_status;
+    a.out_iters = h->d_iters;
+    a.out_repl = h->d_repl;
+    a.out_true_rel = h->d_true_rel;
+    a.out_ns = h->d_ns;
+    bcheck(cudaMemsetAsync(h->d_head, 0, sizeof(int), st), "memset");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(tpb);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    bcheck(cudaLaunchKernelEx(&cfg, h->kernel, a), "batch PCG launch");
+}
+
+void check_tau(double tau, int tau_mode) {
+    require(tau > 0.0 && tau == tau, XPLUS_ERR_ARG, "tau must be positive");
+    require(tau_mode == XPLUS_TAU_ABS_RR || tau_mode == XPLUS_TAU_REL_TRUE, XPLUS_ERR_ARG, "bad tau_mode");
+}
+
+// gather b and x (device, original order), solve, scatter x back
+void enqueue_solve(xplus_batch* h, const double* d_b, double* d_x, double tau, int tau_mode, int max_iters,
+                   cudaStream_t st) {
+    const int threads = 256, blocks = (h->rows + threads - 1) / threads;
+    batch_gather_kernel<<<blocks, threads, 0, st>>>(d_b, h->d_b64, h->d_map, h->rows);
+    bcheck(cudaGetLastError(), "gather");
+    batch_gather_kernel<<<blocks, threads, 0, st>>>(d_x, h->d_x64, h->d_map, h->rows);
+    bcheck(cudaGetLastError(), "gather");
+    enqueue_kernel(h, tau, tau_mode, max_iters, h->cluster, h->tpb, h->grid, st);
+    batch_scatter_kernel<<<blocks, threads, 0, st>>>(h->d_x64, d_x, h->d_map, h->rows);
+    bcheck(cudaGetLastError(), "scatter");
+}
+
+void collect(xplus_batch* h) {
+    if (!h->pending) return;
+    bcheck(cudaEventSynchronize(h->ev1), "sync");
+    float ms = 0.0f;
+    bcheck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
+    h->last_ms = ms;
+    h->pending = false;
+}
+
+}  // namespace
+}  // namespace xplus
+
+using namespace xplus;
+
+extern "C" {
+
+int xplus_batch_create(int nsys, const int* const* row_ptrs, const int* const* col_idxs,
+                       const double* const* values, const int* ns, const xplus_opts* opts,
+                       xplus_batch** out) {
+    return guarded([&] { batch_create(nsys, row_ptrs, col_idxs, values, ns, opts, out); });
+}
+
+int xplus_batch_destroy(xplus_batch* h) {
+    return guarded([&] { batch_destroy(h); });
+}
+
+int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        set_launch(h, cluster, block_threads);
+    });
+}
+
+int xplus_batch_solve(xplus_batch* h, const double* b, const double* x0, double tau, int tau_mode,
+                      int max_iters, double* x_out) {
+    return guarded([&] {
+        require(h && b && x_out, XPLUS_ERR_ARG, "null argument");
+        check_tau(tau, tau_mode);
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = h->stream;
+        const size_t nb = sizeof(double) * static_cast<size_t>(h->total_n);
+        bcheck(cudaMemcpyAsync(h->d_bio, b, nb, cudaMemcpyHostToDevice, st), "H2D");
+        if (x0) bcheck(cudaMemcpyAsync(h->d_xio, x0, nb, cudaMemcpyHostToDevice, st), "H2D");
+        else bcheck(cudaMemsetAsync(h->d_xio, 0, nb, st), "memset");
+        bcheck(cudaEventRecord(h->ev0, st), "event");
+        enqueue_solve(h, h->d_bio, h->d_xio, tau, tau_mode, max_iters, st);
+        bcheck(cudaEventRecord(h->ev1, st), "event");
+        h->pending = true;
+        bcheck(cudaMemcpyAsync(x_out, h->d_xio, nb, cudaMemcpyDeviceToHost, st), "D2H");
+        bcheck(cudaStreamSynchronize(st), "sync");
+        collect(h);
+    });
+}
+
+int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, double tau, int tau_mode,
+                             int max_iters, void* stream) {
+    return guarded([&] {
+        require(h && d_b && d_x, XPLUS_ERR_ARG, "null argument");
+        check_tau(tau, tau_mode);
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+        const bool same = h->gexec && h->g_b == d_b && h->g_x == d_x && h->g_tau == tau && h->g_mode == tau_mode &&
+                          h->g_iters == max_iters && h->g_cluster == h->cluster && h->g_tpb == h->tpb;
+        if (!same) {
+            if (h->gexec) {
+                bcheck(cudaGraphExecDestroy(h->gexec), "graph destroy");
+                h->gexec = nullptr;
+            }
+            // capture on the handle's own stream; the executable graph runs on any stream
+            bcheck(cudaStreamSynchronize(h->stream), "sync");
+            bcheck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            cudaGraph_t graph = nullptr;
+            try {
+                enqueue_solve(h, d_b, d_x, tau, tau_mode, max_iters, h->stream);
+            } catch (...) {
+                cudaStreamEndCapture(h->stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            bcheck(cudaStreamEndCapture(h->stream, &graph), "end capture");
+            const cudaError_t e = cudaGraphInstantiate(&h->gexec, graph, 0);
+            cudaGraphDestroy(graph);
+            bcheck(e, "graph instantiate");
+            h->g_b = d_b;
+            h->g_x = d_x;
+            h->g_tau = tau;
+            h->g_mode = tau_mode;
+            h->g_iters = max_iters;
+            h->g_cluster = h->cluster;
+            h->g_tpb = h->tpb;
+        }
+        bcheck(cudaEventRecord(h->ev0, st), "event");
+        bcheck(cudaGraphLaunch(h->gexec, st), "graph launch");
+        bcheck(cudaEventRecord(h->ev1, st), "event");
+        h->pending = true;
+    });
+}
+
+int xplus_batch_results(xplus_batch* h, int* status, int* iterations, int* replacements, double* true_rel,
+                        double* system_ms, double* kernel_ms) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        collect(h);
+        const size_t K = static_cast<size_t>(h->nsys);
+        if (status) bcheck(cudaMemcpy(status, h->d_status, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        if (iterations) bcheck(cudaMemcpy(iterations, h->d_iters, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        if (replacements) bcheck(cudaMemcpy(replacements, h->d_repl, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        if (true_rel) bcheck(cudaMemcpy(true_rel, h->d_true_rel, K * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        if (system_ms) {
+            std::vector<long long> t(K);
+            bcheck(cudaMemcpy(t.data(), h->d_ns, K * sizeof(long long), cudaMemcpyDeviceToHost), "D2H");
+            for (size_t k = 0; k < K; ++k) system_ms[k] = static_cast<double>(t[k]) * 1e-6;
+        }
+        if (kernel_ms) *kernel_ms = h->last_ms;
+    });
+}
+
+int xplus_batch_autotune(xplus_batch* h, int iters, int* cluster, int* block_threads, double* best_ms) {
+    return guarded([&] {
+        require(h && iters > 0, XPLUS_ERR_ARG, "bad argument");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        cudaStream_t st = h->stream;
+        // a fixed number of iterations per system on b = 1, x = 0 (absolute tolerance that no
+        // system reaches, so every configuration does the same work)
+        std::vector<double> ones(static_cast<size_t>(h->rows), 0.0);
+        std::vector<int> map(static_cast<size_t>(h->rows));
+        bcheck(cudaMemcpy(map.data(), h->d_map, map.size() * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        for (size_t i = 0; i < map.size(); ++i) ones[i] = map[i] >= 0 ? 1.0 : 0.0;
+        double best = 1e300;
+        int bc = h->cluster, bt = h->tpb;
+        const int clusters[4] = {1, 2, 4, 8};
+        const int threads[3] = {128, 256, 512};
+        for (int c : clusters)
+            for (int t : threads) {
+                const int num = active_clusters(h, c, t);
+                if (num <= 0) continue;
+                double ms_min = 1e300;
+                for (int rep = 0; rep < 2; ++rep) {
+                    bcheck(cudaMemcpyAsync(h->d_b64, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+                    bcheck(cudaMemsetAsync(h->d_x64, 0, ones.size() * sizeof(double), st), "memset");
+                    bcheck(cudaEventRecord(h->ev0, st), "event");
+                    enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, c, t, num * c, st);
+                    bcheck(cudaEventRecord(h->ev1, st), "event");
+                    bcheck(cudaEventSynchronize(h->ev1), "sync");
+                    float ms = 0.0f;
+                    bcheck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
+                    ms_min = std::min(ms_min, static_cast<double>(ms));
+                }
+                if (ms_min < best) {
+                    best = ms_min;
+                    bc = c;
+                    bt = t;
+                }
+            }
+        require(best < 1e300, XPLUS_ERR_CUDA, "no launchable cluster shape");
+        set_launch(h, bc, bt);
+        if (cluster) *cluster = bc;
+        if (block_threads) *block_threads = bt;
+        if (best_ms) *best_ms = best;
+    });
+}
+
+int xplus_batch_info(xplus_batch* h, int64_t* total_n, int64_t* total_nnz, int* cluster, int* block_threads,
+                     int* grid, int64_t* spmv_bytes) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        if (total_n) *total_n = h->total_n;
+        if (total_nnz) *total_nnz = h->total_nnz;
+        if (cluster) *cluster = h->cluster;
+        if (block_threads) *block_threads = h->tpb;
+        if (grid) *grid = h->grid;
+        if (spmv_bytes) {
+            // one SpMV over every system in the stored format, padding excluded: off-diagonal
+            // entries (value + index), row sums, x read and y written
+            const int64_t sv = h->opts.value_type == XPLUS_F32 ? 4 : 2;
+            const int64_t si = h->idx16 ? 2 : 4;
+            *spmv_bytes = (h->total_nnz - h->total_n) * (sv + si) + h->total_n * 12;
+        }
+    });
+}
+
+}  // extern "C"

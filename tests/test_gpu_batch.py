@@ -1,0 +1,152 @@
+"""Batched solver (xplus_batch_*): every system of a batch solved in one persistent launch
+reaches the FP64 true-residual tolerance, agrees with the single-system solver and with the
+FP64 oracle solve, and the graph-captured device path and the autotuner give the same answers."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems(specs):
+    from project_xplus_b200 import generators as g
+    out = []
+    for side, sigma, seed in specs:
+        d, xt = g.fem2d(side, sigma=sigma, jitter=0.3, seed=seed, x_seed=seed)
+        out.append((d, xt))
+    return out
+
+
+SPECS = [(12, 1.0, 1), (45, 2.0, 2), (20, 0.5, 3), (64, 2.5, 4), (33, 1.5, 5), (7, 1.0, 6), (96, 1.2, 7)]
+
+
+@pytest.fixture(scope="module")
+def batch_systems():
+    return _systems(SPECS)
+
+
+def _make(batch_systems, **kw):
+    from project_xplus_b200.batch import BatchSolver
+    return BatchSolver([(d.row_ptr, d.col_idx, d.values) for d, _ in batch_systems], **kw)
+
+
+def _b(batch_systems):
+    return np.concatenate([d.b for d, _ in batch_systems])
+
+
+@pytest.mark.parametrize("vt", ["f32", "f16"])
+def test_every_system_converges(gpu, batch_systems, vt):
+    s = _make(batch_systems, values_dtype=vt)
+    r = s.solve(_b(batch_systems), tau=1e-8)
+    assert list(r["status"]) == [0] * len(SPECS), r["status_names"]
+    assert np.all(r["true_rel"] <= 1e-8)
+    for (d, xt), x in zip(batch_systems, s.split(r["x"])):
+        # the solution itself: the same residual check on the host, in FP64
+        res = np.linalg.norm(d.b - _spmv(d, x)) / np.linalg.norm(d.b)
+        assert res <= 1.5e-8
+    assert r["kernel_ms"] > 0 and np.all(r["system_ms"] > 0)
+
+
+def _spmv(d, x):
+    y = np.zeros(d.n)
+    rows = np.repeat(np.arange(d.n), np.diff(d.row_ptr))
+    np.add.at(y, rows, d.values * x[d.col_idx])
+    return y
+
+
+def test_matches_single_system_solver(gpu, batch_systems):
+    """Same iteration, same FP32/FP64 split: iteration counts agree with the single-system
+    persistent kernel up to the order of the dot-product sums, and both solutions are within
+    the tolerance's reach of the FP64 oracle solution."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.linalg import spsolve
+
+    from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
+    s = _make(batch_systems)
+    r = s.solve(_b(batch_systems), tau=1e-8)
+    for k, ((d, xt), x) in enumerate(zip(batch_systems, s.split(r["x"]))):
+        single = PcgSolver(d.row_ptr, d.col_idx, d.values, resident=False)
+        rs = single.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+        single.close()
+        assert rs.converged
+        it_b, it_s = int(r["iterations"][k]), rs.iterations
+        assert abs(it_b - it_s) <= max(3, 0.05 * it_s), (k, it_b, it_s)
+        A = csr_matrix((d.values, d.col_idx, d.row_ptr), shape=(d.n, d.n))
+        x64 = spsolve(A.tocsc(), d.b)
+        scale = np.linalg.norm(x64)
+        err_b = np.linalg.norm(x - x64) / scale
+        err_s = np.linalg.norm(rs.solution - x64) / scale
+        assert err_b <= 10 * max(err_s, 1e-9), (k, err_b, err_s)
+
+
+def test_x0_and_absolute_tolerance(gpu, batch_systems):
+    from project_xplus_b200 import XPLUS_TAU_ABS_RR
+    s = _make(batch_systems)
+    b = _b(batch_systems)
+    rng = np.random.default_rng(0)
+    x0 = rng.uniform(-1, 1, s.total_n)
+    r = s.solve(b, x0, tau=1e-12, tau_mode=XPLUS_TAU_ABS_RR)
+    assert list(r["status"]) == [0] * len(SPECS)
+    # x0 = the exact solution converges at once
+    xs = np.concatenate([xt for _, xt in batch_systems])
+    r2 = s.solve(b, xs, tau=1e-12, tau_mode=XPLUS_TAU_ABS_RR)
+    assert list(r2["iterations"]) == [0] * len(SPECS)
+    # max_iters caps every system: status 1 (max_iter)
+    r3 = s.solve(b, tau=1e-30, tau_mode=XPLUS_TAU_ABS_RR, max_iters=5)
+    assert list(r3["status"]) == [1] * len(SPECS) and list(r3["iterations"]) == [5] * len(SPECS)
+
+
+def test_device_graph_path(gpu, batch_systems):
+    import torch
+    s = _make(batch_systems)
+    b = _b(batch_systems)
+    host = s.solve(b, tau=1e-8)
+    st = torch.cuda.Stream()
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros_like(d_b)
+    for rep in range(3):  # first call captures the graph, the next ones replay it
+        d_x.zero_()
+        torch.cuda.synchronize()
+        s.solve_device(d_b, d_x, tau=1e-8, stream=st)
+        st.synchronize()
+        r = s.results()
+        assert list(r["status"]) == [0] * len(SPECS)
+        np.testing.assert_array_equal(d_x.cpu().numpy(), host["x"])  # deterministic
+
+
+def test_launch_shapes_and_autotune(gpu, batch_systems):
+    from project_xplus_b200 import XplusError
+    from project_xplus_b200.batch import autotune_build
+    s = _make(batch_systems)
+    b = _b(batch_systems)
+    xs = []
+    for cl, tpb in ((1, 512), (2, 256), (8, 128)):
+        s.set_launch(cl, tpb)
+        info = s.info()
+        assert info["cluster"] == cl and info["block_threads"] == tpb and info["grid"] % cl == 0
+        r = s.solve(b, tau=1e-8)
+        assert list(r["status"]) == [0] * len(SPECS)
+        xs.append(r["x"])
+    with pytest.raises(XplusError):
+        s.set_launch(3, 512)
+    t = s.autotune(iters=20)
+    assert t["cluster"] in (1, 2, 4, 8) and t["block_threads"] in (128, 256, 512) and t["ms"] > 0
+    assert s.solve(b, tau=1e-8)["status"].tolist() == [0] * len(SPECS)
+    best, info = autotune_build([(d.row_ptr, d.col_idx, d.values) for d, _ in batch_systems], b,
+                                sigmas=(1, 256), chunks=(2, 4), iters=10)
+    assert len(info["table"]) == 4
+    assert best.solve(b, tau=1e-8)["status"].tolist() == [0] * len(SPECS)
+    best.close()
+
+
+def test_many_uneven_systems(gpu):
+    """More systems than clusters, sides log-uniform in [45, 128]: the queue hands out every
+    system exactly once and each converges."""
+    from project_xplus_b200 import generators as g
+    from project_xplus_b200.batch import BatchSolver
+    sides, sigmas = g.batch_sides(96, 45, 128, seed=11)
+    systems = [g.fem2d(int(sd), sigma=float(sg), seed=100 + k, x_seed=100 + k)[0]
+               for k, (sd, sg) in enumerate(zip(sides, sigmas))]
+    s = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems])
+    r = s.solve(np.concatenate([d.b for d in systems]), tau=1e-8)
+    assert np.all(r["status"] == 0) and np.all(r["true_rel"] <= 1e-8)
+    assert np.all(r["iterations"] > 0)

@@ -34,6 +34,10 @@ METRIC = "time-to-1e-8 rel. residual: learned/mixed vs plain Jacobi-PCG; SpMV HB
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 FP64_CG_ITERATIONS = 5581
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the SM-resident kernel per
+# iteration on the 1108x1108 system: 742.2 MB over a captured launch of 100 iterations
+# (ncu --set full of `python -m project_xplus_b200.profile_case --grid 1108 --iters 100`).
+RESIDENT1_DRAM_BYTES_PER_ITER = 742.2e6 / 100
 
 
 def parse():
@@ -48,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison solves")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched solve")
     return ap.parse_args()
 
 
@@ -75,15 +80,16 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index):
+    def __init__(self, device_index, append=False):
         self.dev = device_index
         self.proc = None
+        self.append = append
         self.path = ROOT / "gpurun_out" / f"clocks_rank{device_index}.csv"
 
     def __enter__(self):
         try:
             self.path.parent.mkdir(exist_ok=True)
-            self.f = open(self.path, "w")
+            self.f = open(self.path, "a" if self.append else "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
@@ -246,6 +252,7 @@ def run_b200(args):
         one_solve()
         torch.cuda.synchronize()
     m0 = metrics()
+    kernel_name = xp.solver.KERNEL_NAMES.get(int(m0.reserved[2]), "unknown")
     barrier(pg, dev)
     torch.cuda.synchronize()
     step_ms, kern_ms, iters, repls, relres = [], [], [], [], []
@@ -325,6 +332,7 @@ def run_b200(args):
         iters_c = C.c_int()
         mm = _lib.XplusMetrics()
         e2e_ms = []
+        clk_e2e = Clocks(local, append=True).__enter__()
         for k in range(args.warmup + args.steps):
             flush.fill_(1.0)
             torch.cuda.synchronize()
@@ -335,6 +343,7 @@ def run_b200(args):
             dt = (time.perf_counter() - t0) * 1e3
             if k >= args.warmup:
                 e2e_ms.append(dt)
+        clk_e2e.__exit__(None, None, None)
         e2e_tot = max_over_ranks(pg, sum(e2e_ms), dev)
         e2e = {"value": world * args.steps / (e2e_tot / 1e3), "unit": "solves/s",
                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n + 128,
@@ -372,6 +381,8 @@ def run_b200(args):
                          f"the full system, extrapolated to {ref_iters:.0f} iterations (the FP64 CG iteration "
                          f"count to 1e-8); {per_it * 1e3:.1f} ms/iteration"}
 
+    batch = None if args.no_batch else run_batch(args, world, rank, pg, dev, stream, flush)
+
     clocks = clk.summary()
     if rank == 0:
         line = {
@@ -384,12 +395,18 @@ def run_b200(args):
             "spmv": {"cold_gbs": spmv_cold_gbs, "warm_gbs": spmv_warm_gbs, "cold_ms": cold_ms, "warm_ms": warm_ms,
                      "bytes": spmv_bytes, "frac_cold": spmv_cold_gbs / hbm, "peak_kind": hbm_kind},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
-                         "kernel": "pcg_persistent_kernel<float,float,4,true,short>",
+                         "frac": achieved / hbm,
+                         "traffic": (RESIDENT1_DRAM_BYTES_PER_ITER * it_mean
+                                     if kernel_name == "pcg_resident1_kernel" and args.grid == 1108 else None),
+                         "traffic_note": "ncu DRAM bytes of a 100-iteration capture of this kernel on this system, "
+                                         "scaled by the iterations of one launch; the matrix stays in L2 and the "
+                                         "vectors in shared memory, so traffic is ~6% of the streaming model",
+                         "kernel": f"{kernel_name}<float,4,short> (FP32 values + vectors, row-sum form)",
                          "bytes_model": "8*nnz + 52*n per iteration (FP32 PCG) + 12*nnz + 28*n per FP64 residual",
                          "peak_kind": hbm_kind,
                          "bytes_per_launch": bytes_launch, "launch_ms": kern_mean},
             "compare": compare,
+            "batch": batch,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": 4 * args.steps,
@@ -400,6 +417,58 @@ def run_b200(args):
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+def run_batch(args, world, rank, pg, dev, stream, flush):
+    """The batched workload: 512 2D P1-FEM systems, grid side log-uniform in [45, 256] and
+    conductivity sigma log-uniform in [0.5, 2.5] (seeded), FP32 values and vectors, 1e-8 FP64
+    true relative residual each, one graph-captured persistent launch per step.  With N ranks
+    the systems are split by estimated work (no collective); the time is the max over ranks."""
+    import torch
+
+    from project_xplus_b200 import generators as g
+    from project_xplus_b200.batch import BatchSolver, shard_systems, system_work
+    sides, sigmas = g.batch_sides(512, 45, 256, seed=3)
+    works = [system_work(int(sd) ** 2, 7 * int(sd) ** 2) for sd in sides]
+    mine = shard_systems(works, world, rank)
+    systems = [g.fem2d(int(sides[k]), sigma=float(sigmas[k]), seed=1000 + k, x_seed=1000 + k)[0] for k in mine]
+    s = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems], values_dtype="f32")
+    tune = s.autotune(iters=0, tau=args.tol)
+    info = s.info()
+    b = torch.from_numpy(np.concatenate([d.b for d in systems])).to(dev)
+    x = torch.zeros_like(b)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        x.zero_()
+        s.solve_device(b, x, tau=args.tol, stream=stream)
+        stream.synchronize()
+    barrier(pg, dev)
+    ms = []
+    clk = Clocks(dev.index, append=True).__enter__()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        x.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.solve_device(b, x, tau=args.tol, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    clk.__exit__(None, None, None)
+    r = s.results()
+    if not np.all(r["status"] == 0):
+        raise SystemExit(f"batch: {int((r['status'] != 0).sum())} systems did not converge")
+    tot = max_over_ranks(pg, sum(ms), dev)
+    s.close()
+    return {"workload": "512 x 2d-p1fem, side log-uniform [45,256], sigma log-uniform [0.5,2.5], fp32, tol 1e-8",
+            "systems": len(sides), "sum_n": int(sum(int(sd) ** 2 for sd in sides)),
+            "value": len(sides) * args.steps / (tot / 1e3), "unit": "systems/s", "ms_per_step": tot / args.steps,
+            "scaling": "strong (systems split over ranks)", "iterations_total": int(r["iterations"].sum()),
+            "iterations_max": int(r["iterations"].max()), "max_true_rel_residual": float(r["true_rel"].max()),
+            "launch": {"cluster": info["cluster"], "block_threads": info["block_threads"], "grid": info["grid"],
+                       "autotune_ms": tune["ms"]},
+            "graph": True}
 
 
 def main():

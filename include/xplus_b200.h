@@ -113,7 +113,9 @@ typedef struct xplus_metrics {
     double true_rel_residual;   /* FP64 ||b - A x|| / ||b|| at exit (when the FP64 copy exists) */
     double kernel_ms;           /* device time of the solve launch(es) */
     double setup_ms;            /* host+device time of xplus_pcg_create */
-    double reserved[4];
+    double reserved[4];         /* [0] stagnation stop (1/0), [1] device time from the kernel's
+                                   own clock (ms), [2] kernel: 0 global-memory persistent,
+                                   1 SM-resident two-barrier, 2 SM-resident one-barrier */
 } xplus_metrics;
 
 typedef struct xplus_pcg xplus_pcg;      /* one SPD system resident on one GPU */
@@ -215,8 +217,12 @@ int xplus_batch_destroy(xplus_batch* h);
 /* cluster in {1, 2, 4, 8} CTAs, block_threads in {128, 256, 512}; the grid is as many
  * clusters as the device holds at once.  XPLUS_ERR_CUDA when the shape cannot launch. */
 int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads);
-/* Times every launch shape on `iters` PCG iterations of every system and keeps the fastest. */
-int xplus_batch_autotune(xplus_batch* h, int iters, int* cluster, int* block_threads, double* best_ms);
+/* The launch-shape autotuner: times every cluster x block_threads shape that launches and keeps
+ * the fastest, on b = 1, x0 = 0 for every system.  iters > 0: that many PCG iterations per
+ * system; iters <= 0: every system solved to FP64 true relative residual tau (0 < tau < 1),
+ * so the queue's makespan is what is timed.  Returns the shape and its time (min of 2 runs). */
+int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, int* block_threads,
+                         double* best_ms);
 /* Blocking solve with host vectors of length sum(ns) (x0 NULL: zeros).  tau / tau_mode /
  * max_iters as xplus_pcg_solve, applied to every system (relative tolerances per system). */
 int xplus_batch_solve(xplus_batch* h, const double* b, const double* x0, double tau, int tau_mode,

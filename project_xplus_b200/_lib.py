@@ -98,7 +98,7 @@ _SIGS = {
     "xplus_batch_create": (_i, [_i, _p, _p, _p, _p, C.POINTER(XplusOpts), C.POINTER(_p)]),
     "xplus_batch_destroy": (_i, [_p]),
     "xplus_batch_set_launch": (_i, [_p, _i, _i]),
-    "xplus_batch_autotune": (_i, [_p, _i, _ip, _ip, _dp]),
+    "xplus_batch_autotune": (_i, [_p, _i, _d, _ip, _ip, _dp]),
     "xplus_batch_solve": (_i, [_p, _p, _p, _d, _i, _i, _p]),
     "xplus_batch_solve_device": (_i, [_p, _p, _p, _d, _i, _i, _p]),
     "xplus_batch_results": (_i, [_p, _p, _p, _p, _p, _p, _dp]),

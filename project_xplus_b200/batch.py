@@ -93,9 +93,10 @@ class BatchSolver:
     def set_launch(self, cluster: int, block_threads: int) -> None:
         check(lib.xplus_batch_set_launch(self._h, int(cluster), int(block_threads)))
 
-    def autotune(self, iters: int = 50) -> dict:
+    def autotune(self, iters: int = 0, tau: float = 1e-8) -> dict:
+        """Launch shape: fixed `iters` iterations per system, or (iters=0) full solves to tau."""
         cl, tpb, ms = C.c_int(), C.c_int(), C.c_double()
-        check(lib.xplus_batch_autotune(self._h, int(iters), C.byref(cl), C.byref(tpb), C.byref(ms)))
+        check(lib.xplus_batch_autotune(self._h, int(iters), float(tau), C.byref(cl), C.byref(tpb), C.byref(ms)))
         return dict(cluster=cl.value, block_threads=tpb.value, ms=ms.value)
 
     def split(self, x) -> list[np.ndarray]:
@@ -131,18 +132,18 @@ class BatchSolver:
                     status_names=[STATUS_NAMES.get(int(s), "unknown") for s in st])
 
 
-def autotune_build(systems, b, *, sigmas=(32, 256, 1024), chunks=(2, 4), iters=50, values_dtype="f32",
+def autotune_build(systems, b, *, sigmas=(32, 256, 1024), chunks=(2, 4), iters=0, tau=1e-8, values_dtype="f32",
                    **kw) -> tuple[BatchSolver, dict]:
     """The batch autotuner: every (sigma, chunk) SELL layout is built, each one's launch shape
-    is tuned by xplus_batch_autotune on `iters` fixed iterations, and the fastest layout is
-    kept.  Slice height stays 32 (one warp lane per row).  Returns the chosen solver and a
+    is tuned by xplus_batch_autotune (full solves to `tau`, or `iters` fixed iterations), and
+    the fastest layout is kept.  Slice height stays 32 (one warp lane per row).  Returns the chosen solver and a
     table of what was timed.  `b` is unused by the timing (the tuner solves b = 1) and kept so
     a caller can solve right away."""
     best, table = None, []
     for sg in sigmas:
         for ch in chunks:
             s = BatchSolver(systems, values_dtype=values_dtype, sigma=sg, chunk=ch, **kw)
-            t = s.autotune(iters)
+            t = s.autotune(iters, tau)
             table.append(dict(sigma=sg, chunk=ch, **t))
             if best is None or t["ms"] < best[1]["ms"]:
                 if best is not None:

@@ -932,13 +932,16 @@ int xplus_batch_results(xplus_batch* h, int* status, int* iterations, int* repla
     });
 }
 
-int xplus_batch_autotune(xplus_batch* h, int iters, int* cluster, int* block_threads, double* best_ms) {
+int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, int* block_threads,
+                         double* best_ms) {
     return guarded([&] {
-        require(h && iters > 0, XPLUS_ERR_ARG, "bad argument");
+        require(h && (iters > 0 || (tau > 0.0 && tau < 1.0)), XPLUS_ERR_ARG, "bad argument");
         bcheck(cudaSetDevice(h->device), "cudaSetDevice");
         cudaStream_t st = h->stream;
-        // a fixed number of iterations per system on b = 1, x = 0 (absolute tolerance that no
-        // system reaches, so every configuration does the same work)
+        // b = 1, x = 0 for every system; either a fixed number of iterations per system (an
+        // absolute tolerance no system reaches, so every shape does the same work), or every
+        // system solved to the FP64 true relative residual tau (the makespan that matters)
+        const bool fixed = iters > 0;
         std::vector<double> ones(static_cast<size_t>(h->rows), 0.0);
         std::vector<int> map(static_cast<size_t>(h->rows));
         bcheck(cudaMemcpy(map.data(), h->d_map, map.size() * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
@@ -956,7 +959,8 @@ int xplus_batch_autotune(xplus_batch* h, int iters, int* cluster, int* block_thr
                     bcheck(cudaMemcpyAsync(h->d_b64, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
                     bcheck(cudaMemsetAsync(h->d_x64, 0, ones.size() * sizeof(double), st), "memset");
                     bcheck(cudaEventRecord(h->ev0, st), "event");
-                    enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, c, t, num * c, st);
+                    if (fixed) enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, c, t, num * c, st);
+                    else enqueue_kernel(h, tau, XPLUS_TAU_REL_TRUE, 0, c, t, num * c, st);
                     bcheck(cudaEventRecord(h->ev1, st), "event");
                     bcheck(cudaEventSynchronize(h->ev1), "sync");
                     float ms = 0.0f;

@@ -445,6 +445,7 @@ void collect(xplus_pcg* h, xplus_metrics* m) {
         L.kernel_ms = ms;
         L.reserved[0] = o.stagnated;
         L.reserved[1] = static_cast<double>(o.t_end_ns - o.t_start_ns) * 1e-6;
+        L.reserved[2] = h->resident ? (h->one_sync ? 2.0 : 1.0) : 0.0;
         h->phase_ns[0] = o.t_phase[0];
         h->phase_ns[1] = o.t_phase[1];
         h->phase_ns[2] = o.t_phase[2];

@@ -37,6 +37,7 @@ class run_defaults:  # noqa: N801  (mirrors the reference namespace)
 
 
 kBreakdownEps = 1.0e-30
+KERNEL_NAMES = {0: "pcg_persistent_kernel", 1: "pcg_resident_kernel", 2: "pcg_resident1_kernel"}
 kMaxN = 1024  # the reference multi-kernel cap; the GPU path has none
 
 
@@ -233,7 +234,7 @@ class PcgSolver:
             residual_rel=res_rel, iteration_trace=tr, replacements=m.replacements,
             kernel_ms=m.kernel_ms, setup_ms=m.setup_ms,
             metrics=dict(rz=m.rz, rr=m.rr, pap=m.pap, alpha=m.alpha, stagnated=bool(m.reserved[0]),
-                         device_ms=m.reserved[1]))
+                         device_ms=m.reserved[1], kernel=KERNEL_NAMES.get(int(m.reserved[2]), "unknown")))
 
     def spmv(self, x) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64)

@@ -130,6 +130,8 @@ def test_launch_shapes_and_autotune(gpu, batch_systems):
         s.set_launch(3, 512)
     t = s.autotune(iters=20)
     assert t["cluster"] in (1, 2, 4, 8) and t["block_threads"] in (128, 256, 512) and t["ms"] > 0
+    t = s.autotune(tau=1e-8)
+    assert t["ms"] > 0 and s.info()["cluster"] == t["cluster"]
     assert s.solve(b, tau=1e-8)["status"].tolist() == [0] * len(SPECS)
     best, info = autotune_build([(d.row_ptr, d.col_idx, d.values) for d, _ in batch_systems], b,
                                 sigmas=(1, 256), chunks=(2, 4), iters=10)

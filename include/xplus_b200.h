@@ -195,6 +195,64 @@ int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double
                       double tau, int max_iters, int n, void* stream);
 
 /* ------------------------------------------------------------------------------------
+ * Factorized preconditioner M^-1 = G^T G (no counterpart in the reference, whose only
+ * preconditioner is Jacobi, host/pcg_common.hpp:42-54).  G is lower-triangular on A's lower
+ * pattern in the row order given to xplus_pcg_create; its values are passed in "g_low" order:
+ * A's CSR order of the entries with col <= row (n_glow values, the diagonal included).  The
+ * solve applies G^T G as two more sliced SpMVs (no triangular solves) and keeps the FP64
+ * residual replacement; Jacobi-PCG takes over inside the same launch when the G^T G solve
+ * stagnates or reaches fallback_iters iterations (0: only on stagnation).  Needs FP32 vectors,
+ * FP32 or FP16 values, row_sum_form and keep_fp64.  reserved[3] of the metrics holds the
+ * iteration of the switch to Jacobi (-1: none).
+ * ------------------------------------------------------------------------------------ */
+/* G from host values (g_low NULL: back to Jacobi).  row_ptr / col_idx: the CSR pattern given
+ * to xplus_pcg_create (the G layouts are built from it once). */
+int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* g_low,
+                      int fallback_iters);
+/* G predicted on the GPU by the learned network (parameters as xplus_gnn_get_params returns
+ * them) from the CSR given to xplus_pcg_create; infer_ms (nullable) gets the host+device
+ * time of the inference. */
+int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
+                      const float* params, int fallback_iters, double* infer_ms);
+/* The handle's current G in g_low order (g_low NULL: only *n_glow). */
+int xplus_pcg_get_gtg(xplus_pcg* h, double* g_low, int64_t* n_glow);
+/* Exact factorized sparse approximate inverse on A's lower pattern (host, no GPU): row i
+ * solves A[P_i, P_i] g = e_i over P_i = {j <= i : a_ij != 0}, scaled to (G A G^T)_ii = 1.
+ * The non-learned G of the same form, in g_low order. */
+int xplus_fsai_lower(int n, const int* row_ptr, const int* col_idx, const double* values, double* g_low);
+
+/* ------------------------------------------------------------------------------------
+ * Learned-preconditioner trainer (no counterpart in the reference).  A 3-layer message-
+ * passing network (hidden width 32) over A's graph predicts G: inputs log a_ii (centred),
+ * sum_j |a_ij| / a_ii - 1 and a_ij / sqrt(a_ii a_jj); separate message weights for lower
+ * and upper neighbours; G_ij = (w . relu(P h_i + bp + Q h_j + c e_ij) + bw) / sqrt(a_jj),
+ * G_ii = exp(wd . h_i + bwd) / sqrt(a_ii).  Loss sum_p ||G A G^T v_p - v_p||^2 / (K n) over K
+ * probe vectors v ~ N(0, I).  Forward, backward and Adam run on the GPU (FP32 arithmetic,
+ * parameters rounded to BF16 in the forward pass, FP32 master copy).
+ * ------------------------------------------------------------------------------------ */
+typedef struct xplus_gnn_trainer xplus_gnn_trainer;
+/* Number of parameters (floats); returns the count, not a status. */
+int xplus_gnn_param_count(void);
+/* Training systems as CSR (like xplus_batch_create); `probes` = K per step (1..64). */
+int xplus_gnn_trainer_create(int nsys, const int* const* row_ptrs, const int* const* col_idxs,
+                             const double* const* values, const int* ns, int probes, int device,
+                             xplus_gnn_trainer** out);
+int xplus_gnn_trainer_destroy(xplus_gnn_trainer* t);
+/* Parameters in and out (FP32 master copy); setting them resets the Adam state. */
+int xplus_gnn_set_params(xplus_gnn_trainer* t, const float* params);
+int xplus_gnn_get_params(xplus_gnn_trainer* t, float* params);
+/* Loss on system `sys` with the probes of `seed`, and its gradient (grad nullable). */
+int xplus_gnn_loss_grad(xplus_gnn_trainer* t, int sys, uint64_t seed, double* loss, float* grad);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with a caller-given gradient. */
+int xplus_gnn_adam(xplus_gnn_trainer* t, const float* grad, double lr);
+/* `steps` Adam steps, one system per step (a seeded shuffle every epoch), probes from `seed`
+ * and the step, learning rate cosine-decayed from lr to lr_final; losses (nullable) gets the
+ * loss of every step. */
+int xplus_gnn_train(xplus_gnn_trainer* t, int steps, double lr, double lr_final, uint64_t seed, double* losses);
+/* G of system `sys` under the current parameters, in g_low order (g_low NULL: only *n_glow). */
+int xplus_gnn_predict(xplus_gnn_trainer* t, int sys, double* g_low, int64_t* n_glow);
+
+/* ------------------------------------------------------------------------------------
  * Batched solver: many independent SPD systems in one persistent launch.  The reference
  * solves one system per launch (host/cuper_control_xrt_host.cpp:205-272, one
  * cuper_pcg_control_kernel run per dataset); a caller with many systems looped over

@@ -95,6 +95,19 @@ _SIGS = {
     "update_xrz_kernel": (None, [_p, _p, _p, _p, _p, _p, _p, _d, _i]),
     "update_p_kernel": (None, [_p, _p, _d, _i]),
     "xplus_update_xrz_noalloc": (_i, [_p, _p, _p, _p, _p, _p, _p, _d, _i, _p]),
+    "xplus_pcg_set_gtg": (_i, [_p, _p, _p, _p, _i]),
+    "xplus_pcg_set_gnn": (_i, [_p, _p, _p, _p, _p, _i, _dp]),
+    "xplus_pcg_get_gtg": (_i, [_p, _p, C.POINTER(_i64)]),
+    "xplus_fsai_lower": (_i, [_i, _p, _p, _p, _p]),
+    "xplus_gnn_param_count": (_i, []),
+    "xplus_gnn_trainer_create": (_i, [_i, _p, _p, _p, _p, _i, _i, C.POINTER(_p)]),
+    "xplus_gnn_trainer_destroy": (_i, [_p]),
+    "xplus_gnn_set_params": (_i, [_p, _p]),
+    "xplus_gnn_get_params": (_i, [_p, _p]),
+    "xplus_gnn_loss_grad": (_i, [_p, _i, _u64, _dp, _p]),
+    "xplus_gnn_adam": (_i, [_p, _p, _d]),
+    "xplus_gnn_train": (_i, [_p, _i, _d, _d, _u64, _p]),
+    "xplus_gnn_predict": (_i, [_p, _i, _p, C.POINTER(_i64)]),
     "xplus_batch_create": (_i, [_i, _p, _p, _p, _p, C.POINTER(XplusOpts), C.POINTER(_p)]),
     "xplus_batch_destroy": (_i, [_p]),
     "xplus_batch_set_launch": (_i, [_p, _i, _i]),

@@ -1,0 +1,792 @@
+// gnn.cu -- the learned preconditioner M^-1 = G^T G: a 3-layer message-passing network over
+// A's graph predicts G on A's lower pattern; forward, probe loss, backward and Adam are the
+// kernels below, all hand-written (FP32 arithmetic, parameters rounded to BF16 for the forward).
+//
+// Network (H = 32), in the row order of the system:
+//   x_i = [log a_ii - mean log a_kk, sum_j |a_ij| / a_ii - 1],  e_ij = a_ij / sqrt(a_ii a_jj)
+//   h = relu(W0 x + b0)
+//   3 x: s_i = Wa h_i + ba + sum_{j<i} e_ij Wl h_j + sum_{j>i} e_ij Wu h_j ; h_i += relu(s_i)
+//   lower edge (i, j<i): Ghat_ij = w . relu(P h_i + bp + Q h_j + c e_ij) + bw
+//   diagonal:            Ghat_ii = exp(wd . h_i + bwd)
+//   G = Ghat D^-1/2 (an untrained network with a zero output layer gives Jacobi)
+// Loss over K probes v ~ N(0, I): L = sum ||G A G^T v - v||^2 / (K n).
+// Lower and upper neighbours have their own message weights because G is lower-triangular in
+// the given order: what G_ij should be depends on which neighbours precede row i.
+//
+// Layouts: node arrays are [n][32] row-major (one warp per node, lane = feature, 128-byte
+// rows); probe arrays are [n][K].  Weight-gradient sums over nodes or edges go through fixed
+// per-block partials and a fixed-order final sum, so gradients are deterministic.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "common.hpp"
+#include "gnn.hpp"
+
+namespace xplus {
+namespace gnn {
+namespace {
+
+constexpr int H = kHidden;
+constexpr int kRedBlocks = 256;  // blocks of every deterministic reduction (upper bound)
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void k_round_params(const float* __restrict__ master, float* __restrict__ wr, int P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) wr[i] = __bfloat162float(__float2bfloat16_rn(master[i]));
+}
+
+// h0 = relu(W0 x + b0): thread per (node, feature)
+__global__ void k_input(const float* __restrict__ x, const float* __restrict__ W0, const float* __restrict__ b0,
+                        float* __restrict__ h0, int n) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<long long>(n) * H) return;
+    const int i = static_cast<int>(t / H), f = static_cast<int>(t % H);
+    const float v = fmaf(W0[2 * f], x[2 * i], fmaf(W0[2 * f + 1], x[2 * i + 1], b0[f]));
+    h0[t] = fmaxf(v, 0.0f);
+}
+
+// Up to three products Y_m = W_m h (+ b_m) per node; W_m [H][H] row-major (out, in), staged
+// transposed in shared memory so lane `out` reads a conflict-free column.
+struct Lin3 {
+    const float* W[3];
+    const float* b[3];
+    float* Y[3];
+    int count;
+};
+
+__global__ void __launch_bounds__(256) k_node_lin(const float* __restrict__ h, Lin3 L, int n) {
+    __shared__ float WT[3][H * H];
+    for (int q = threadIdx.x; q < L.count * H * H; q += blockDim.x) {
+        const int m = q / (H * H), r = q % (H * H), o = r / H, k = r % H;
+        WT[m][k * H + o] = L.W[m][r];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
+        const float hv = h[static_cast<size_t>(i) * H + lane];
+        float acc[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll 8
+        for (int k = 0; k < H; ++k) {
+            const float hk = __shfl_sync(0xffffffffu, hv, k);
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+                if (m < L.count) acc[m] = fmaf(hk, WT[m][k * H + lane], acc[m]);
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+            if (m < L.count) L.Y[m][static_cast<size_t>(i) * H + lane] = acc[m] + (L.b[m] ? L.b[m][lane] : 0.0f);
+    }
+}
+
+// Transposed products for the backward pass: dX = sum_m D_m W_m (+ dexp (x) wd), W_m [H][H]
+// row-major staged as is (lane `in` reads W[out][in], conflict-free).  dX = accumulate ? dX + . : .
+struct BackLin {
+    const float* W[3];
+    const float* D[3];
+    int count;
+    const float* dexp;  // optional per-node scalar times wd
+    const float* wd;
+    int accumulate;
+};
+
+__global__ void __launch_bounds__(256) k_node_backlin(BackLin B, float* __restrict__ dX, int n) {
+    __shared__ float Ws[3][H * H];
+    for (int q = threadIdx.x; q < B.count * H * H; q += blockDim.x) Ws[q / (H * H)][q % (H * H)] = B.W[q / (H * H)][q % (H * H)];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
+        float acc = B.accumulate ? dX[static_cast<size_t>(i) * H + lane] : 0.0f;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            if (m >= B.count) break;
+            const float dv = B.D[m][static_cast<size_t>(i) * H + lane];
+#pragma unroll 8
+            for (int o = 0; o < H; ++o) acc = fmaf(__shfl_sync(0xffffffffu, dv, o), Ws[m][o * H + lane], acc);
+        }
+        if (B.dexp) acc = fmaf(B.dexp[i], B.wd[lane], acc);
+        dX[static_cast<size_t>(i) * H + lane] = acc;
+    }
+}
+
+// s_i = a_i + sum_{j<i} e_ij hl_j + sum_{j>i} e_ij hu_j ;  h_out = h_in + relu(s)
+__global__ void k_aggregate(const int* __restrict__ adj_ptr, const int* __restrict__ adj_col,
+                            const float* __restrict__ adj_e, const float* __restrict__ a,
+                            const float* __restrict__ hl, const float* __restrict__ hu,
+                            const float* __restrict__ h_in, float* __restrict__ s, float* __restrict__ h_out, int n) {
+    const int lane = threadIdx.x & 31;
+    const int i = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    float acc = a[static_cast<size_t>(i) * H + lane];
+    for (int q = adj_ptr[i]; q < adj_ptr[i + 1]; ++q) {
+        const int j = adj_col[q];
+        const float* src = j < i ? hl : hu;
+        acc = fmaf(adj_e[q], src[static_cast<size_t>(j) * H + lane], acc);
+    }
+    if (s) s[static_cast<size_t>(i) * H + lane] = acc;
+    h_out[static_cast<size_t>(i) * H + lane] = h_in[static_cast<size_t>(i) * H + lane] + fmaxf(acc, 0.0f);
+}
+
+// Edge head and diagonal: warp per row i; lower edges of row i in CSR order.
+__global__ void k_head(const int* __restrict__ low_ptr, const int* __restrict__ low_col,
+                       const float* __restrict__ low_e, const float* __restrict__ ph, const float* __restrict__ qh,
+                       const float* __restrict__ h, const float* __restrict__ isq, const float* __restrict__ wr,
+                       ParamOffsets off, float* __restrict__ zpre, float* __restrict__ go, float* __restrict__ gval,
+                       float* __restrict__ gd, float* __restrict__ gdiag, int n) {
+    const int lane = threadIdx.x & 31;
+    const int i = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    const float c = wr[off.c + lane], w = wr[off.w + lane], bw = wr[off.bw];
+    const float phv = ph[static_cast<size_t>(i) * H + lane];
+    for (int k = low_ptr[i]; k < low_ptr[i + 1]; ++k) {
+        const int j = low_col[k];
+        const float zp = phv + qh[static_cast<size_t>(j) * H + lane] + c * low_e[k];
+        if (zpre) zpre[static_cast<size_t>(k) * H + lane] = zp;
+        const float g = warp_sum_f(w * fmaxf(zp, 0.0f)) + bw;
+        if (lane == 0) {
+            if (go) go[k] = g;
+            gval[k] = g * isq[j];
+        }
+    }
+    const float t = warp_sum_f(wr[off.wd + lane] * h[static_cast<size_t>(i) * H + lane]) + wr[off.bwd];
+    if (lane == 0) {
+        const float e = expf(t);
+        if (gd) gd[i] = e;
+        gdiag[i] = e * isq[i];
+    }
+}
+
+// ---- probe-vector products (thread per (row, probe)) ----
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    unsigned long long z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void k_probes(float* __restrict__ v, long long count, unsigned long long seed) {
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const unsigned long long s = seed * 0xD1B54A32D192ED03ull;
+    const unsigned long long a = splitmix64(s ^ (2ull * static_cast<unsigned long long>(q)));
+    const unsigned long long b = splitmix64(s ^ (2ull * static_cast<unsigned long long>(q) + 1ull));
+    const double u1 = (static_cast<double>(a >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+    const double u2 = (static_cast<double>(b >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+    v[q] = static_cast<float>(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2));
+}
+
+// out = G in (- sub):  row i: gdiag_i in_i + sum_{k in low(i)} gval_k in_{col k}
+__global__ void k_g_apply(const int* __restrict__ low_ptr, const int* __restrict__ low_col,
+                          const float* __restrict__ gval, const float* __restrict__ gdiag,
+                          const float* __restrict__ in, const float* __restrict__ sub, float* __restrict__ out,
+                          int n, int K) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<long long>(n) * K) return;
+    const int i = static_cast<int>(t / K), p = static_cast<int>(t % K);
+    float acc = gdiag[i] * in[t];
+    for (int k = low_ptr[i]; k < low_ptr[i + 1]; ++k) acc = fmaf(gval[k], in[static_cast<size_t>(low_col[k]) * K + p], acc);
+    out[t] = sub ? acc - sub[t] : acc;
+}
+
+// out = G^T in:  row j: gdiag_j in_j + sum_{k in up(j)} gval_k in_{row k}
+__global__ void k_gt_apply(const int* __restrict__ up_ptr, const int* __restrict__ up_k,
+                           const int* __restrict__ up_row, const float* __restrict__ gval,
+                           const float* __restrict__ gdiag, const float* __restrict__ in, float* __restrict__ out,
+                           int n, int K) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<long long>(n) * K) return;
+    const int j = static_cast<int>(t / K), p = static_cast<int>(t % K);
+    float acc = gdiag[j] * in[t];
+    for (int q = up_ptr[j]; q < up_ptr[j + 1]; ++q)
+        acc = fmaf(gval[up_k[q]], in[static_cast<size_t>(up_row[q]) * K + p], acc);
+    out[t] = acc;
+}
+
+__global__ void k_a_apply(const int* __restrict__ a_ptr, const int* __restrict__ a_col, const float* __restrict__ a_val,
+                          const float* __restrict__ in, float* __restrict__ out, int n, int K) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<long long>(n) * K) return;
+    const int i = static_cast<int>(t / K), p = static_cast<int>(t % K);
+    float acc = 0.0f;
+    for (int q = a_ptr[i]; q < a_ptr[i + 1]; ++q) acc = fmaf(a_val[q], in[static_cast<size_t>(a_col[q]) * K + p], acc);
+    out[t] = acc;
+}
+
+// dL/dGhat: lower edge k = (i, j): dgo_k = scale isq_j sum_p (r_ip w2_jp + v_ip y_jp);
+// diagonal: dexp_i = dgd_i * gd_i with dgd_i = scale isq_i sum_p (r_ip w2_ip + v_ip y_ip)
+__global__ void k_dG(const int* __restrict__ low_row, const int* __restrict__ low_col, const float* __restrict__ isq,
+                     const float* __restrict__ r, const float* __restrict__ w2, const float* __restrict__ v,
+                     const float* __restrict__ y, const float* __restrict__ gd, float* __restrict__ dgo,
+                     float* __restrict__ dexp, int n_low, int n, int K, float scale) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_low) {
+        const int i = low_row[t], j = low_col[t];
+        float acc = 0.0f;
+        for (int p = 0; p < K; ++p)
+            acc += r[static_cast<size_t>(i) * K + p] * w2[static_cast<size_t>(j) * K + p] +
+                   v[static_cast<size_t>(i) * K + p] * y[static_cast<size_t>(j) * K + p];
+        dgo[t] = scale * isq[j] * acc;
+    } else if (t < n_low + n) {
+        const int i = t - n_low;
+        float acc = 0.0f;
+        for (int p = 0; p < K; ++p)
+            acc += r[static_cast<size_t>(i) * K + p] * w2[static_cast<size_t>(i) * K + p] +
+                   v[static_cast<size_t>(i) * K + p] * y[static_cast<size_t>(i) * K + p];
+        dexp[i] = scale * isq[i] * acc * gd[i];
+    }
+}
+
+// dph_i = sum_{k in low(i)} dgo_k w .* [zpre_k > 0] ; dqh_j = sum_{k in up(j)} (same)
+__global__ void k_head_back(const int* __restrict__ low_ptr, const int* __restrict__ up_ptr, const int* __restrict__ up_k,
+                            const float* __restrict__ zpre, const float* __restrict__ dgo, const float* __restrict__ wr,
+                            ParamOffsets off, float* __restrict__ dph, float* __restrict__ dqh, int n) {
+    const int lane = threadIdx.x & 31;
+    const int i = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    const float w = wr[off.w + lane];
+    float a = 0.0f, b = 0.0f;
+    for (int k = low_ptr[i]; k < low_ptr[i + 1]; ++k)
+        if (zpre[static_cast<size_t>(k) * H + lane] > 0.0f) a = fmaf(dgo[k], w, a);
+    for (int q = up_ptr[i]; q < up_ptr[i + 1]; ++q) {
+        const int k = up_k[q];
+        if (zpre[static_cast<size_t>(k) * H + lane] > 0.0f) b = fmaf(dgo[k], w, b);
+    }
+    dph[static_cast<size_t>(i) * H + lane] = a;
+    dqh[static_cast<size_t>(i) * H + lane] = b;
+}
+
+// Layer backward through the aggregation: ds = dh .* [s > 0] for the own row, and
+// dhl_j = sum_{i in N(j), i > j} e_ij ds_i ; dhu_j = sum_{i in N(j), i < j} e_ij ds_i.
+__global__ void k_agg_back(const int* __restrict__ adj_ptr, const int* __restrict__ adj_col,
+                           const float* __restrict__ adj_e, const float* __restrict__ dh, const float* __restrict__ s,
+                           float* __restrict__ ds, float* __restrict__ dhl, float* __restrict__ dhu, int n) {
+    const int lane = threadIdx.x & 31;
+    const int j = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (j >= n) return;
+    const size_t oj = static_cast<size_t>(j) * H + lane;
+    ds[oj] = s[oj] > 0.0f ? dh[oj] : 0.0f;
+    float l = 0.0f, u = 0.0f;
+    for (int q = adj_ptr[j]; q < adj_ptr[j + 1]; ++q) {
+        const int i = adj_col[q];
+        const size_t oi = static_cast<size_t>(i) * H + lane;
+        const float d = s[oi] > 0.0f ? dh[oi] : 0.0f;
+        if (i > j) l = fmaf(adj_e[q], d, l);
+        else u = fmaf(adj_e[q], d, u);
+    }
+    dhl[oj] = l;
+    dhu[oj] = u;
+}
+
+// dX_in = dX .* [X > 0]  (relu of the input layer: h0 > 0 iff its pre-activation > 0)
+__global__ void k_relu_mask(const float* __restrict__ d, const float* __restrict__ x, float* __restrict__ out, long long count) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < count) out[t] = x[t] > 0.0f ? d[t] : 0.0f;
+}
+
+// ---- deterministic reductions ----
+// partial[b][o*KB + k] = sum_{i in chunk b} D[i][o] X[i][k]; partial[b][32*KB + o] = sum D[i][o]
+template <int KB>
+__global__ void __launch_bounds__(256) k_outer_partial(const float* __restrict__ D, const float* __restrict__ X,
+                                                       int n, int chunk, float* __restrict__ partial) {
+    __shared__ float Ds[32][H + 1];
+    __shared__ float Xs[32][KB + 1];
+    constexpr int NOUT = H * KB + H;
+    constexpr int PER = (NOUT + 255) / 256;
+    float acc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) acc[q] = 0.0f;
+    const int i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+    for (int base = i0; base < i1; base += 32) {
+        __syncthreads();
+        for (int q = threadIdx.x; q < 32 * H; q += 256) {
+            const int r = q / H, f = q % H, i = base + r;
+            Ds[r][f] = i < i1 ? D[static_cast<size_t>(i) * H + f] : 0.0f;
+        }
+        for (int q = threadIdx.x; q < 32 * KB; q += 256) {
+            const int r = q / KB, f = q % KB, i = base + r;
+            Xs[r][f] = i < i1 ? X[static_cast<size_t>(i) * KB + f] : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int o = threadIdx.x + 256 * q;
+            if (o < H * KB) {
+                const int a = o / KB, k = o % KB;
+                float s = acc[q];
+#pragma unroll 8
+                for (int r = 0; r < 32; ++r) s = fmaf(Ds[r][a], Xs[r][k], s);
+                acc[q] = s;
+            } else if (o < NOUT) {
+                const int a = o - H * KB;
+                float s = acc[q];
+#pragma unroll 8
+                for (int r = 0; r < 32; ++r) s += Ds[r][a];
+                acc[q] = s;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int o = threadIdx.x + 256 * q;
+        if (o < NOUT) partial[static_cast<size_t>(blockIdx.x) * NOUT + o] = acc[q];
+    }
+}
+
+// grad[dst_w + o] = sum_b partial[b][o] for o < nw ; grad[dst_b + o] = sum_b partial[b][nw + o] (dst_b >= 0)
+__global__ void k_partial_final(const float* __restrict__ partial, int blocks, int stride, int nw, int nb,
+                                float* __restrict__ grad, int dst_w, int dst_b) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nw + nb) return;
+    float s = 0.0f;
+    for (int b = 0; b < blocks; ++b) s += partial[static_cast<size_t>(b) * stride + o];
+    if (o < nw) grad[dst_w + o] = s;
+    else if (dst_b >= 0) grad[dst_b + (o - nw)] = s;
+}
+
+// Edge-head parameter partials over lower edges (warp per edge, grid-stride):
+//   dw[f] += dgo relu(zpre_f), dc[f] += dgo w_f [zpre_f > 0] e, dbw += dgo
+__global__ void __launch_bounds__(256) k_edge_partial(const float* __restrict__ zpre, const float* __restrict__ dgo,
+                                                      const float* __restrict__ low_e, const float* __restrict__ wr,
+                                                      ParamOffsets off, int n_low, float* __restrict__ partial) {
+    __shared__ float red[8][2 * H + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float w = wr[off.w + lane];
+    float aw = 0.0f, ac = 0.0f, ab = 0.0f;
+    for (int k = blockIdx.x * 8 + warp; k < n_low; k += gridDim.x * 8) {
+        const float z = zpre[static_cast<size_t>(k) * H + lane];
+        const float d = dgo[k];
+        aw = fmaf(d, fmaxf(z, 0.0f), aw);
+        if (z > 0.0f) ac = fmaf(d * w, low_e[k], ac);
+        ab += d;
+    }
+    red[warp][lane] = aw;
+    red[warp][H + lane] = ac;
+    if (lane == 0) red[warp][2 * H] = ab;
+    __syncthreads();
+    for (int o = threadIdx.x; o < 2 * H + 1; o += blockDim.x) {
+        float s = 0.0f;
+        for (int q = 0; q < 8; ++q) s += red[q][o];
+        partial[static_cast<size_t>(blockIdx.x) * (2 * H + 1) + o] = s;
+    }
+}
+
+// Node partials of a weighted column sum: out[f] = sum_i coef_i X[i][f], out[H] = sum_i coef_i
+__global__ void __launch_bounds__(256) k_vec_partial(const float* __restrict__ coef, const float* __restrict__ X, int n,
+                                                     float* __restrict__ partial) {
+    __shared__ float red[8][H + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float aw = 0.0f, ab = 0.0f;
+    for (int i = blockIdx.x * 8 + warp; i < n; i += gridDim.x * 8) {
+        const float c = coef[i];
+        aw = fmaf(c, X[static_cast<size_t>(i) * H + lane], aw);
+        ab += c;
+    }
+    red[warp][lane] = aw;
+    if (lane == 0) red[warp][H] = ab;
+    __syncthreads();
+    for (int o = threadIdx.x; o < H + 1; o += blockDim.x) {
+        float s = 0.0f;
+        for (int q = 0; q < 8; ++q) s += red[q][o];
+        partial[static_cast<size_t>(blockIdx.x) * (H + 1) + o] = s;
+    }
+}
+
+// loss partials: sum of squares of r over [count]
+__global__ void __launch_bounds__(256) k_sumsq_partial(const float* __restrict__ r, long long count, float* __restrict__ partial) {
+    __shared__ float red[8];
+    float s = 0.0f;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < count;
+         t += static_cast<long long>(gridDim.x) * blockDim.x)
+        s = fmaf(r[t], r[t], s);
+    s = warp_sum_f(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int q = 0; q < 8; ++q) t += red[q];
+        partial[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_loss_final(const float* __restrict__ partial, int blocks, double scale, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < blocks; ++b) s += static_cast<double>(partial[b]);
+        *out = s * scale;
+    }
+}
+
+__global__ void k_adam(float* __restrict__ theta, const float* __restrict__ grad, float* __restrict__ m,
+                       float* __restrict__ v, int P, float lr, float b1, float b2, float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const float g = grad[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * g;
+    const float vi = b2 * v[i] + (1.0f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    theta[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_to_glow(const float* __restrict__ gval, const float* __restrict__ gdiag, const int* __restrict__ pos_low,
+                          const int* __restrict__ pos_diag, double* __restrict__ g_low, int n_low, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_low) g_low[pos_low[t]] = gval[t];
+    else if (t < n_low + n) g_low[pos_diag[t - n_low]] = gdiag[t - n_low];
+}
+
+inline int blocks_for(long long count, int threads) {
+    return static_cast<int>((count + threads - 1) / threads);
+}
+
+}  // namespace
+
+ParamOffsets param_offsets() {
+    ParamOffsets o{};
+    int p = 0;
+    o.W0 = p; p += H * 2;
+    o.b0 = p; p += H;
+    for (int l = 0; l < kLayers; ++l) {
+        o.Wa[l] = p; p += H * H;
+        o.ba[l] = p; p += H;
+        o.Wl[l] = p; p += H * H;
+        o.Wu[l] = p; p += H * H;
+    }
+    o.P = p; p += H * H;
+    o.bp = p; p += H;
+    o.Q = p; p += H * H;
+    o.c = p; p += H;
+    o.w = p; p += H;
+    o.bw = p; p += 1;
+    o.wd = p; p += H;
+    o.bwd = p; p += 1;
+    o.total = p;
+    return o;
+}
+
+// ---------------------------------------------------------------------------------------
+// Host: graph construction (the single builder for training and for the solver's inference)
+// ---------------------------------------------------------------------------------------
+void HostGraph::build(int n_, const int* row_ptr, const int* col_idx, const double* values) {
+    n = n_;
+    std::vector<double> d(static_cast<size_t>(n), 0.0), rowabs(static_cast<size_t>(n), 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
+            rowabs[static_cast<size_t>(i)] += std::fabs(values[q]);
+            if (col_idx[q] == i) d[static_cast<size_t>(i)] += values[q];
+        }
+    for (int i = 0; i < n; ++i)
+        require(d[static_cast<size_t>(i)] > 0.0, XPLUS_ERR_DATA, "learned preconditioner needs a positive diagonal");
+    double mean_ld = 0.0;
+    for (double v : d) mean_ld += std::log(v);
+    mean_ld /= n;
+    x.resize(static_cast<size_t>(n) * 2);
+    isq.resize(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        x[2 * static_cast<size_t>(i)] = static_cast<float>(std::log(d[static_cast<size_t>(i)]) - mean_ld);
+        x[2 * static_cast<size_t>(i) + 1] = static_cast<float>(rowabs[static_cast<size_t>(i)] / d[static_cast<size_t>(i)] - 1.0);
+        isq[static_cast<size_t>(i)] = static_cast<float>(1.0 / std::sqrt(d[static_cast<size_t>(i)]));
+    }
+    adj_ptr.assign(static_cast<size_t>(n) + 1, 0);
+    low_ptr.assign(static_cast<size_t>(n) + 1, 0);
+    a_ptr.assign(row_ptr, row_ptr + n + 1);
+    a_col.assign(col_idx, col_idx + row_ptr[n]);
+    a_val.resize(static_cast<size_t>(row_ptr[n]));
+    for (int q = 0; q < row_ptr[n]; ++q) a_val[static_cast<size_t>(q)] = static_cast<float>(values[q]);
+    adj_col.clear(); adj_e.clear(); low_col.clear(); low_row.clear(); low_e.clear(); pos_low.clear();
+    pos_diag.assign(static_cast<size_t>(n), -1);
+    n_glow = 0;
+    for (int i = 0; i < n; ++i) {
+        // columns of row i in ascending order (stable for equal columns); kq[q - row_ptr[i]] is
+        // the lower-edge index of CSR entry q (-1 for the diagonal and the upper entries)
+        const int len = row_ptr[i + 1] - row_ptr[i];
+        std::vector<int> idx(static_cast<size_t>(len)), kq(static_cast<size_t>(len), -1);
+        std::iota(idx.begin(), idx.end(), row_ptr[i]);
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return col_idx[a] < col_idx[b]; });
+        for (int q : idx) {
+            const int j = col_idx[q];
+            if (j == i) continue;
+            const float e = static_cast<float>(values[q] / std::sqrt(d[static_cast<size_t>(i)] * d[static_cast<size_t>(j)]));
+            adj_col.push_back(j);
+            adj_e.push_back(e);
+            if (j < i) {
+                kq[static_cast<size_t>(q - row_ptr[i])] = static_cast<int>(low_col.size());
+                low_col.push_back(j);
+                low_row.push_back(i);
+                low_e.push_back(e);
+            }
+        }
+        adj_ptr[static_cast<size_t>(i) + 1] = static_cast<int>(adj_col.size());
+        low_ptr[static_cast<size_t>(i) + 1] = static_cast<int>(low_col.size());
+        pos_low.resize(low_col.size(), -1);
+        // positions of this row's G entries in A's CSR order of the entries with col <= row
+        bool diag_seen = false;
+        for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
+            const int j = col_idx[q];
+            if (j > i) continue;
+            if (j == i) {
+                require(!diag_seen, XPLUS_ERR_DATA, "duplicate diagonal entry");
+                diag_seen = true;
+                pos_diag[static_cast<size_t>(i)] = n_glow++;
+            } else {
+                pos_low[static_cast<size_t>(kq[static_cast<size_t>(q - row_ptr[i])])] = n_glow++;
+            }
+        }
+    }
+    pos_low.resize(low_col.size(), -1);
+    n_low = static_cast<int>(low_col.size());
+    n_adj = static_cast<int>(adj_col.size());
+    // lower edges grouped by column: up(j) = {k : low_col[k] == j}, by increasing row
+    up_ptr.assign(static_cast<size_t>(n) + 1, 0);
+    for (int k = 0; k < n_low; ++k) ++up_ptr[static_cast<size_t>(low_col[static_cast<size_t>(k)]) + 1];
+    for (int i = 0; i < n; ++i) up_ptr[static_cast<size_t>(i) + 1] += up_ptr[static_cast<size_t>(i)];
+    up_k.assign(static_cast<size_t>(n_low), 0);
+    up_row.assign(static_cast<size_t>(n_low), 0);
+    std::vector<int> fill(up_ptr.begin(), up_ptr.end() - 1);
+    for (int k = 0; k < n_low; ++k) {
+        const int j = low_col[static_cast<size_t>(k)];
+        const int at = fill[static_cast<size_t>(j)]++;
+        up_k[static_cast<size_t>(at)] = k;
+        up_row[static_cast<size_t>(at)] = low_row[static_cast<size_t>(k)];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Device graph + workspace
+// ---------------------------------------------------------------------------------------
+namespace {
+template <typename T>
+T* up(Arena& ar, const std::vector<T>& v, cudaStream_t st) {
+    T* p = ar.get<T>(std::max<size_t>(v.size(), 1));
+    if (!v.empty()) {
+        const cudaError_t e = cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) throw Error(XPLUS_ERR_CUDA, std::string("H2D: ") + cudaGetErrorString(e));
+    }
+    return p;
+}
+}  // namespace
+
+void* Arena::raw(size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    ptrs.push_back(p);
+    return p;
+}
+void Arena::release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+}
+
+void DevGraph::upload(const HostGraph& g, Arena& ar, cudaStream_t st) {
+    n = g.n;
+    n_low = g.n_low;
+    n_adj = g.n_adj;
+    n_glow = g.n_glow;
+    adj_ptr = up(ar, g.adj_ptr, st);
+    adj_col = up(ar, g.adj_col, st);
+    adj_e = up(ar, g.adj_e, st);
+    low_ptr = up(ar, g.low_ptr, st);
+    low_col = up(ar, g.low_col, st);
+    low_row = up(ar, g.low_row, st);
+    low_e = up(ar, g.low_e, st);
+    up_ptr = up(ar, g.up_ptr, st);
+    up_k = up(ar, g.up_k, st);
+    up_row = up(ar, g.up_row, st);
+    a_ptr = up(ar, g.a_ptr, st);
+    a_col = up(ar, g.a_col, st);
+    a_val = up(ar, g.a_val, st);
+    x = up(ar, g.x, st);
+    isq = up(ar, g.isq, st);
+    pos_low = up(ar, g.pos_low, st);
+    pos_diag = up(ar, g.pos_diag, st);
+}
+
+void Work::alloc(Arena& ar, int max_n, int max_low, int K_, bool train) {
+    K = K_;
+    const size_t nH = static_cast<size_t>(max_n) * H, lH = static_cast<size_t>(max_low) * H;
+    for (int l = 0; l <= kLayers; ++l) h[l] = ar.get<float>(nH);
+    for (int l = 0; l < kLayers; ++l) s[l] = train ? ar.get<float>(nH) : nullptr;
+    a = ar.get<float>(nH);
+    hl = ar.get<float>(nH);
+    hu = ar.get<float>(nH);
+    ph = ar.get<float>(nH);
+    qh = ar.get<float>(nH);
+    gval = ar.get<float>(static_cast<size_t>(max_low));
+    gdiag = ar.get<float>(static_cast<size_t>(max_n));
+    if (!train) return;
+    zpre = ar.get<float>(lH);
+    go = ar.get<float>(static_cast<size_t>(max_low));
+    gd = ar.get<float>(static_cast<size_t>(max_n));
+    const size_t nK = static_cast<size_t>(max_n) * K;
+    v = ar.get<float>(nK);
+    w1 = ar.get<float>(nK);
+    w2 = ar.get<float>(nK);
+    r = ar.get<float>(nK);
+    t = ar.get<float>(nK);
+    y = ar.get<float>(nK);
+    dgo = ar.get<float>(static_cast<size_t>(max_low));
+    dexp = ar.get<float>(static_cast<size_t>(max_n));
+    dh = ar.get<float>(nH);
+    dh2 = ar.get<float>(nH);
+    ds = ar.get<float>(nH);
+    dhl = ar.get<float>(nH);
+    dhu = ar.get<float>(nH);
+    dph = ar.get<float>(nH);
+    dqh = ar.get<float>(nH);
+    partial = ar.get<float>(static_cast<size_t>(kRedBlocks) * (H * H + H));
+    loss = ar.get<double>(1);
+}
+
+static void kcheck(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream_t st) {
+    const ParamOffsets off = param_offsets();
+    const int n = g.n;
+    const int nodes_blocks = blocks_for(static_cast<long long>(n) * 32, 256);
+    const int lin_blocks = std::min(blocks_for(n, 8), 148 * 8);
+    k_input<<<blocks_for(static_cast<long long>(n) * H, 256), 256, 0, st>>>(g.x, wr + off.W0, wr + off.b0, w.h[0], n);
+    kcheck("gnn input");
+    for (int l = 0; l < kLayers; ++l) {
+        Lin3 L{{wr + off.Wa[l], wr + off.Wl[l], wr + off.Wu[l]}, {wr + off.ba[l], nullptr, nullptr}, {w.a, w.hl, w.hu}, 3};
+        k_node_lin<<<lin_blocks, 256, 0, st>>>(w.h[l], L, n);
+        kcheck("gnn layer");
+        k_aggregate<<<nodes_blocks, 256, 0, st>>>(g.adj_ptr, g.adj_col, g.adj_e, w.a, w.hl, w.hu, w.h[l],
+                                                  train ? w.s[l] : nullptr, w.h[l + 1], n);
+        kcheck("gnn aggregate");
+    }
+    Lin3 L{{wr + off.P, wr + off.Q, nullptr}, {wr + off.bp, nullptr, nullptr}, {w.ph, w.qh, nullptr}, 2};
+    k_node_lin<<<lin_blocks, 256, 0, st>>>(w.h[kLayers], L, n);
+    kcheck("gnn head lin");
+    k_head<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.low_col, g.low_e, w.ph, w.qh, w.h[kLayers], g.isq, wr, off,
+                                         train ? w.zpre : nullptr, train ? w.go : nullptr, w.gval,
+                                         train ? w.gd : nullptr, w.gdiag, n);
+    kcheck("gnn head");
+}
+
+void g_to_low(const DevGraph& g, const Work& w, double* d_glow, cudaStream_t st) {
+    k_to_glow<<<blocks_for(static_cast<long long>(g.n_low) + g.n, 256), 256, 0, st>>>(w.gval, w.gdiag, g.pos_low, g.pos_diag,
+                                                                                    d_glow, g.n_low, g.n);
+    kcheck("gnn g_low");
+}
+
+static void outer_grad(const float* D, const float* X, int kb, int n, Work& w, float* grad, int dst_w, int dst_b,
+                       cudaStream_t st) {
+    const int chunk = std::max(32, ((n + kRedBlocks - 1) / kRedBlocks + 31) / 32 * 32);
+    const int blocks = (n + chunk - 1) / chunk;
+    const int nw = H * kb;
+    if (kb == H) k_outer_partial<H><<<blocks, 256, 0, st>>>(D, X, n, chunk, w.partial);
+    else k_outer_partial<2><<<blocks, 256, 0, st>>>(D, X, n, chunk, w.partial);
+    kcheck("gnn outer partial");
+    k_partial_final<<<blocks_for(nw + H, 128), 128, 0, st>>>(w.partial, blocks, nw + H, nw, dst_b >= 0 ? H : 0, grad,
+                                                              dst_w, dst_b);
+    kcheck("gnn outer final");
+}
+
+static void wd_grad(const float* coef, const float* X, int n, Work& w, float* grad, int dst_w, int dst_b,
+                    cudaStream_t st) {
+    const int blocks = std::max(1, std::min(kRedBlocks, blocks_for(n, 8)));
+    k_vec_partial<<<blocks, 256, 0, st>>>(coef, X, n, w.partial);
+    kcheck("gnn vec partial");
+    k_partial_final<<<1, 64, 0, st>>>(w.partial, blocks, H + 1, H, 1, grad, dst_w, dst_b);
+    kcheck("gnn vec final");
+}
+
+void loss_backward(const DevGraph& g, const float* wr, Work& w, float* grad, unsigned long long seed, cudaStream_t st) {
+    const ParamOffsets off = param_offsets();
+    const int n = g.n, K = w.K;
+    const long long nK = static_cast<long long>(n) * K;
+    const int pb = blocks_for(nK, 256);
+    k_probes<<<pb, 256, 0, st>>>(w.v, nK, seed);
+    kcheck("gnn probes");
+    // r = G A G^T v - v ; y = A G^T r
+    k_gt_apply<<<pb, 256, 0, st>>>(g.up_ptr, g.up_k, g.up_row, w.gval, w.gdiag, w.v, w.w1, n, K);
+    k_a_apply<<<pb, 256, 0, st>>>(g.a_ptr, g.a_col, g.a_val, w.w1, w.w2, n, K);
+    k_g_apply<<<pb, 256, 0, st>>>(g.low_ptr, g.low_col, w.gval, w.gdiag, w.w2, w.v, w.r, n, K);
+    k_gt_apply<<<pb, 256, 0, st>>>(g.up_ptr, g.up_k, g.up_row, w.gval, w.gdiag, w.r, w.t, n, K);
+    k_a_apply<<<pb, 256, 0, st>>>(g.a_ptr, g.a_col, g.a_val, w.t, w.y, n, K);
+    kcheck("gnn probe products");
+    const int lb = std::min(kRedBlocks, blocks_for(nK, 256));
+    k_sumsq_partial<<<lb, 256, 0, st>>>(w.r, nK, w.partial);
+    k_loss_final<<<1, 32, 0, st>>>(w.partial, lb, 1.0 / static_cast<double>(nK), w.loss);
+    kcheck("gnn loss");
+    if (!grad) return;
+    const float scale = 2.0f / static_cast<float>(nK);
+    k_dG<<<blocks_for(static_cast<long long>(g.n_low) + n, 256), 256, 0, st>>>(g.low_row, g.low_col, g.isq, w.r, w.w2, w.v,
+                                                                              w.y, w.gd, w.dgo, w.dexp, g.n_low, n, K, scale);
+    kcheck("gnn dG");
+    const int nodes_blocks = blocks_for(static_cast<long long>(n) * 32, 256);
+    const int lin_blocks = std::min(blocks_for(n, 8), 148 * 8);
+    k_head_back<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.up_ptr, g.up_k, w.zpre, w.dgo, wr, off, w.dph, w.dqh, n);
+    kcheck("gnn head back");
+    // edge-head parameters w, c, bw
+    {
+        const int eb = std::max(1, std::min(kRedBlocks, blocks_for(g.n_low, 8)));
+        k_edge_partial<<<eb, 256, 0, st>>>(w.zpre, w.dgo, g.low_e, wr, off, g.n_low, w.partial);
+        kcheck("gnn edge partial");
+        // partial rows: [dw (H) | dc (H) | dbw (1)]
+        k_partial_final<<<1, 128, 0, st>>>(w.partial, eb, 2 * H + 1, H, 0, grad, off.w, -1);
+        k_partial_final<<<1, 128, 0, st>>>(w.partial + H, eb, 2 * H + 1, H, 0, grad, off.c, -1);
+        k_partial_final<<<1, 32, 0, st>>>(w.partial + 2 * H, eb, 2 * H + 1, 1, 0, grad, off.bw, -1);
+        kcheck("gnn edge final");
+    }
+    const float* hL = w.h[kLayers];
+    outer_grad(w.dph, hL, H, n, w, grad, off.P, off.bp, st);
+    outer_grad(w.dqh, hL, H, n, w, grad, off.Q, -1, st);
+    // dh = dph P + dqh Q + dexp wd
+    BackLin B{{wr + off.P, wr + off.Q, nullptr}, {w.dph, w.dqh, nullptr}, 2, w.dexp, wr + off.wd, 0};
+    k_node_backlin<<<lin_blocks, 256, 0, st>>>(B, w.dh, n);
+    kcheck("gnn head backlin");
+    wd_grad(w.dexp, hL, n, w, grad, off.wd, off.bwd, st);
+    for (int l = kLayers - 1; l >= 0; --l) {
+        k_agg_back<<<nodes_blocks, 256, 0, st>>>(g.adj_ptr, g.adj_col, g.adj_e, w.dh, w.s[l], w.ds, w.dhl, w.dhu, n);
+        kcheck("gnn agg back");
+        const float* hin = w.h[l];
+        outer_grad(w.ds, hin, H, n, w, grad, off.Wa[l], off.ba[l], st);
+        outer_grad(w.dhl, hin, H, n, w, grad, off.Wl[l], -1, st);
+        outer_grad(w.dhu, hin, H, n, w, grad, off.Wu[l], -1, st);
+        // dh <- dh + ds Wa + dhl Wl + dhu Wu
+        BackLin Bl{{wr + off.Wa[l], wr + off.Wl[l], wr + off.Wu[l]}, {w.ds, w.dhl, w.dhu}, 3, nullptr, nullptr, 1};
+        k_node_backlin<<<lin_blocks, 256, 0, st>>>(Bl, w.dh, n);
+        kcheck("gnn layer backlin");
+    }
+    k_relu_mask<<<blocks_for(static_cast<long long>(n) * H, 256), 256, 0, st>>>(w.dh, w.h[0], w.dh2,
+                                                                              static_cast<long long>(n) * H);
+    kcheck("gnn input mask");
+    outer_grad(w.dh2, g.x, 2, n, w, grad, off.W0, off.b0, st);
+}
+
+void adam_step(float* theta, const float* grad, float* m, float* v, int P, float lr, int step, cudaStream_t st) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, static_cast<float>(step));
+    const float c2 = 1.0f - std::pow(b2, static_cast<float>(step));
+    k_adam<<<blocks_for(P, 256), 256, 0, st>>>(theta, grad, m, v, P, lr, b1, b2, 1e-8f, c1, c2);
+    kcheck("gnn adam");
+}
+
+void round_params(const float* master, float* wr, int P, cudaStream_t st) {
+    k_round_params<<<blocks_for(P, 256), 256, 0, st>>>(master, wr, P);
+    kcheck("gnn round");
+}
+
+}  // namespace gnn
+}  // namespace xplus

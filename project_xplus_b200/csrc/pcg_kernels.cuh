@@ -13,7 +13,7 @@ struct PcgOut {
     int stagnated;
     double rz, rr, pap, alpha;
     double true_rr;    // ||b - A x||^2 in FP64 at exit
-    double reserved;
+    double reserved;   // GTG kernel: iteration at which it fell back to Jacobi (-1: never)
     long long t_start_ns, t_end_ns;
     long long t_phase[4];  // block 0: phase A work, barrier wait, phase B work, barrier wait (ns)
 };
@@ -59,6 +59,10 @@ struct PcgArgs {
     const int2* win;
     int flush_every;
     long long* block_clk;   // [gridDim.x][4] phase clock of every CTA (ns)
+    // GTG kernel only: second residual buffer (XT, n_pad) and the iteration cap after which the
+    // learned preconditioner gives way to Jacobi (0: only on stagnation)
+    void* r2;
+    int g_fallback_iters;
 };
 
 struct SpmvArgs {
@@ -91,6 +95,13 @@ cudaError_t resident_prepare(const KernelKey& k, int device, size_t smem_bytes, 
                              bool* fits);
 cudaError_t resident_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, size_t smem_bytes,
                             bool one_sync, cudaStream_t s, const cudaAccessPolicyWindow& window);
+// GTG-preconditioned persistent kernel (pcg_gtg.cu): FP32 vectors, row-sum form, M^-1 = G^T G
+// with G and G^T in SELL form (FP32 values, int32 columns, chunk 2) over the matrix's ordering.
+cudaError_t gtg_grid(const KernelKey& k, int device, int n_slices, int* grid, int* tpb);
+cudaError_t gtg_launch(const KernelKey& k, const PcgArgs& a, int grid, int tpb, cudaStream_t s,
+                       const cudaAccessPolicyWindow& window);
+// val[q] = glow[map[q]] (0 where map[q] < 0): G values into a SELL image of G or G^T
+cudaError_t gtg_fill_values(const double* d_glow, const int* d_map, float* d_val, long long slots, cudaStream_t s);
 cudaError_t spmv_launch(const KernelKey& k, const SpmvArgs& a, const void* x, void* y,
                         cudaStream_t s);
 // dst[i] = (T) src[perm[i]] for i < n, 0 for n <= i < n_pad   (T per xt; f64 when xt==F64)

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "gnn.hpp"
 #include "pcg_kernels.cuh"
 
 struct xplus_pcg {
@@ -68,6 +69,17 @@ struct xplus_pcg {
     int debug_skip_block = -1;
     long long phase_ns[4] = {0, 0, 0, 0};
     std::vector<void*> allocations;
+    std::vector<int> perm;     // SELL row -> original row
+    // M^-1 = G^T G: G on A's lower pattern (original order), SELL images of G and G^T in the
+    // matrix's SELL order, and the map from each SELL slot to its entry of g_low
+    bool gtg = false;
+    int gtg_grid = 0;
+    int g_fallback_iters = 0;
+    int64_t n_glow = 0, g_slots = 0, gt_slots = 0;
+    long long *d_g_slice_ptr = nullptr, *d_gt_slice_ptr = nullptr;
+    int *d_g_col = nullptr, *d_gt_col = nullptr, *d_g_map = nullptr, *d_gt_map = nullptr;
+    float *d_g_val = nullptr, *d_gt_val = nullptr, *d_t = nullptr, *d_r2 = nullptr;
+    double* d_glow = nullptr;
 };
 
 namespace xplus {
@@ -191,6 +203,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         h->n_slices = S.n_slices;
         h->nnz = row_ptr[n];
         h->slots = S.slots;
+        h->perm = S.perm;
         cuda_check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaEventCreate(&h->ev0), "cudaEventCreate");
         cuda_check(cudaEventCreate(&h->ev1), "cudaEventCreate");
@@ -414,7 +427,18 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_out, 0, sizeof(PcgOut), st), "memset");
     cuda_check(cudaEventRecord(h->ev0, st), "event");
-    if (h->resident)
+    if (h->gtg) {
+        a.g_slice_ptr = h->d_g_slice_ptr;
+        a.g_col = h->d_g_col;
+        a.g_val = h->d_g_val;
+        a.gt_slice_ptr = h->d_gt_slice_ptr;
+        a.gt_col = h->d_gt_col;
+        a.gt_val = h->d_gt_val;
+        a.t = h->d_t;
+        a.r2 = h->d_r2;
+        a.g_fallback_iters = h->g_fallback_iters;
+        cuda_check(gtg_launch(h->key, a, h->gtg_grid, 512, st, h->window), "GTG PCG launch");
+    } else if (h->resident)
         cuda_check(resident_launch(h->key, a, h->grid, h->tpb, h->smem_bytes, h->one_sync, st, h->window),
                    "resident PCG launch");
     else
@@ -445,7 +469,8 @@ void collect(xplus_pcg* h, xplus_metrics* m) {
         L.kernel_ms = ms;
         L.reserved[0] = o.stagnated;
         L.reserved[1] = static_cast<double>(o.t_end_ns - o.t_start_ns) * 1e-6;
-        L.reserved[2] = h->resident ? (h->one_sync ? 2.0 : 1.0) : 0.0;
+        L.reserved[2] = h->gtg ? 3.0 : (h->resident ? (h->one_sync ? 2.0 : 1.0) : 0.0);
+        L.reserved[3] = h->gtg ? o.reserved : -1.0;
         h->phase_ns[0] = o.t_phase[0];
         h->phase_ns[1] = o.t_phase[1];
         h->phase_ns[2] = o.t_phase[2];
@@ -453,6 +478,107 @@ void collect(xplus_pcg* h, xplus_metrics* m) {
         h->pending = false;
     }
     if (m) *m = h->last;
+}
+
+// SELL image (C = 32, chunk 2) of a matrix given by rows in SELL order: rows[r] lists
+// (column in SELL order, source index into g_low).  Padding slots: own row, source -1.
+void gtg_sell(const std::vector<std::vector<std::pair<int, int>>>& rows, int n_pad, std::vector<long long>& sp,
+              std::vector<int>& col, std::vector<int>& map) {
+    const int ns = n_pad / 32;
+    sp.assign(static_cast<size_t>(ns) + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+        size_t w = 0;
+        for (int l = 0; l < 32; ++l) w = std::max(w, rows[static_cast<size_t>(s * 32 + l)].size());
+        w = (w + 1) / 2 * 2;
+        sp[static_cast<size_t>(s) + 1] = sp[static_cast<size_t>(s)] + static_cast<long long>(w) * 32;
+    }
+    col.assign(static_cast<size_t>(sp.back()), 0);
+    map.assign(static_cast<size_t>(sp.back()), -1);
+    for (int s = 0; s < ns; ++s) {
+        const size_t w = static_cast<size_t>((sp[static_cast<size_t>(s) + 1] - sp[static_cast<size_t>(s)]) / 32);
+        for (int l = 0; l < 32; ++l) {
+            const int r = s * 32 + l;
+            const auto& e = rows[static_cast<size_t>(r)];
+            for (size_t j = 0; j < w; ++j) {
+                const size_t pos = static_cast<size_t>(sp[static_cast<size_t>(s)]) + (j / 2) * 64 + static_cast<size_t>(l) * 2 + j % 2;
+                if (j < e.size()) {
+                    col[pos] = e[j].first;
+                    map[pos] = e[j].second;
+                } else {
+                    col[pos] = r;
+                }
+            }
+        }
+    }
+}
+
+// Builds the G / G^T SELL images for the pattern of the CSR given to xplus_pcg_create (once).
+void gtg_layout(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
+    require(h->opts.vector_type == XPLUS_F32 && h->key.diag && (h->opts.value_type == XPLUS_F32 || h->opts.value_type == XPLUS_F16),
+            XPLUS_ERR_ARG, "G^T G preconditioning needs FP32 vectors, FP32 or FP16 values and row_sum_form");
+    require(h->d_val64 != nullptr, XPLUS_ERR_ARG, "G^T G preconditioning needs keep_fp64");
+    if (h->d_g_slice_ptr) return;
+    const int n = h->n;
+    require(row_ptr && col_idx && row_ptr[0] == 0 && row_ptr[n] == h->nnz, XPLUS_ERR_ARG,
+            "pattern differs from the matrix of the handle");
+    std::vector<int> iperm(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) iperm[static_cast<size_t>(h->perm[static_cast<size_t>(i)])] = i;
+    std::vector<std::vector<std::pair<int, int>>> g(static_cast<size_t>(h->n_pad)), gt(static_cast<size_t>(h->n_pad));
+    int gl = 0;
+    for (int i = 0; i < n; ++i)
+        for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
+            const int j = col_idx[q];
+            require(j >= 0 && j < n, XPLUS_ERR_DATA, "column index out of range");
+            if (j > i) continue;
+            const int ri = iperm[static_cast<size_t>(i)], rj = iperm[static_cast<size_t>(j)];
+            g[static_cast<size_t>(ri)].push_back({rj, gl});
+            gt[static_cast<size_t>(rj)].push_back({ri, gl});
+            ++gl;
+        }
+    h->n_glow = gl;
+    std::vector<long long> sp, tsp;
+    std::vector<int> col, map, tcol, tmap;
+    gtg_sell(g, h->n_pad, sp, col, map);
+    gtg_sell(gt, h->n_pad, tsp, tcol, tmap);
+    h->g_slots = static_cast<int64_t>(col.size());
+    h->gt_slots = static_cast<int64_t>(tcol.size());
+    cudaStream_t st = h->stream;
+    h->d_g_slice_ptr = dalloc<long long>(h, sp.size());
+    h->d_gt_slice_ptr = dalloc<long long>(h, tsp.size());
+    h->d_g_col = dalloc<int>(h, col.size());
+    h->d_gt_col = dalloc<int>(h, tcol.size());
+    h->d_g_map = dalloc<int>(h, map.size());
+    h->d_gt_map = dalloc<int>(h, tmap.size());
+    h->d_g_val = dalloc<float>(h, col.size());
+    h->d_gt_val = dalloc<float>(h, tcol.size());
+    h->d_t = dalloc<float>(h, static_cast<size_t>(h->n_pad));
+    h->d_r2 = dalloc<float>(h, static_cast<size_t>(h->n_pad));
+    h->d_glow = dalloc<double>(h, static_cast<size_t>(gl));
+    cuda_check(cudaMemcpyAsync(h->d_g_slice_ptr, sp.data(), sp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemcpyAsync(h->d_gt_slice_ptr, tsp.data(), tsp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemcpyAsync(h->d_g_col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemcpyAsync(h->d_gt_col, tcol.data(), tcol.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemcpyAsync(h->d_g_map, map.data(), map.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemcpyAsync(h->d_gt_map, tmap.data(), tmap.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemsetAsync(h->d_r2, 0, static_cast<size_t>(h->n_pad) * sizeof(float), st), "memset");
+    cuda_check(cudaMemsetAsync(h->d_t, 0, static_cast<size_t>(h->n_pad) * sizeof(float), st), "memset");
+    int gtg_tpb = 0;
+    cuda_check(gtg_grid(h->key, h->device, h->n_slices, &h->gtg_grid, &gtg_tpb), "gtg grid");
+    if (h->gtg_grid > h->grid) {
+        // partial sums are sized by the grid
+        h->d_partial = dalloc<double>(h, static_cast<size_t>(16) * h->gtg_grid);
+    }
+    cuda_check(cudaStreamSynchronize(st), "sync");
+}
+
+// G values (device, g_low order) -> the two SELL images; switches the handle to G^T G
+void gtg_enable(xplus_pcg* h, int fallback_iters) {
+    cudaStream_t st = h->stream;
+    cuda_check(gtg_fill_values(h->d_glow, h->d_g_map, h->d_g_val, h->g_slots, st), "gtg fill");
+    cuda_check(gtg_fill_values(h->d_glow, h->d_gt_map, h->d_gt_val, h->gt_slots, st), "gtg fill");
+    cuda_check(cudaStreamSynchronize(st), "sync");
+    h->g_fallback_iters = fallback_iters;
+    h->gtg = true;
 }
 
 }  // namespace
@@ -702,6 +828,70 @@ int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double
         cuda_check(cudaMemcpyAsync(status, st_out, sizeof(st_out), cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(cudaMemcpyAsync(metrics, met, sizeof(met), cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(cudaStreamSynchronize(st), "sync");
+    });
+}
+
+int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* g_low,
+                      int fallback_iters) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        if (!g_low) {
+            h->gtg = false;
+            return;
+        }
+        require(fallback_iters >= 0, XPLUS_ERR_ARG, "fallback_iters must be >= 0");
+        gtg_layout(h, row_ptr, col_idx);
+        cuda_check(cudaMemcpyAsync(h->d_glow, g_low, static_cast<size_t>(h->n_glow) * sizeof(double),
+                                   cudaMemcpyHostToDevice, h->stream), "H2D");
+        gtg_enable(h, fallback_iters);
+    });
+}
+
+int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
+                      const float* params, int fallback_iters, double* infer_ms) {
+    return guarded([&] {
+        require(h && values && params, XPLUS_ERR_ARG, "null argument");
+        require(fallback_iters >= 0, XPLUS_ERR_ARG, "fallback_iters must be >= 0");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        gtg_layout(h, row_ptr, col_idx);
+        const auto t0 = std::chrono::steady_clock::now();
+        gnn::HostGraph hg;
+        hg.build(h->n, row_ptr, col_idx, values);
+        require(hg.n_glow == h->n_glow, XPLUS_ERR_DATA, "matrix pattern needs every diagonal entry");
+        gnn::Arena ar;
+        try {
+            cudaStream_t st = h->stream;
+            gnn::DevGraph dg;
+            dg.upload(hg, ar, st);
+            gnn::Work w;
+            w.alloc(ar, hg.n, std::max(1, hg.n_low), 1, false);
+            const int P = gnn::param_offsets().total;
+            float* master = ar.get<float>(static_cast<size_t>(P));
+            float* wr = ar.get<float>(static_cast<size_t>(P));
+            cuda_check(cudaMemcpyAsync(master, params, static_cast<size_t>(P) * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
+            gnn::round_params(master, wr, P, st);
+            gnn::forward(dg, wr, w, false, st);
+            gnn::g_to_low(dg, w, h->d_glow, st);
+            gtg_enable(h, fallback_iters);
+        } catch (...) {
+            cudaStreamSynchronize(h->stream);
+            ar.release();
+            throw;
+        }
+        cudaStreamSynchronize(h->stream);
+        ar.release();
+        if (infer_ms) *infer_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+int xplus_pcg_get_gtg(xplus_pcg* h, double* g_low, int64_t* n_glow) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        if (n_glow) *n_glow = h->n_glow;
+        if (!g_low) return;
+        require(h->d_glow != nullptr, XPLUS_ERR_ARG, "no G set on this handle");
+        cuda_check(cudaMemcpy(g_low, h->d_glow, static_cast<size_t>(h->n_glow) * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
     });
 }
 

@@ -37,7 +37,8 @@ class run_defaults:  # noqa: N801  (mirrors the reference namespace)
 
 
 kBreakdownEps = 1.0e-30
-KERNEL_NAMES = {0: "pcg_persistent_kernel", 1: "pcg_resident_kernel", 2: "pcg_resident1_kernel"}
+KERNEL_NAMES = {0: "pcg_persistent_kernel", 1: "pcg_resident_kernel", 2: "pcg_resident1_kernel",
+                3: "pcg_gtg_kernel"}
 kMaxN = 1024  # the reference multi-kernel cap; the GPU path has none
 
 
@@ -234,7 +235,32 @@ class PcgSolver:
             residual_rel=res_rel, iteration_trace=tr, replacements=m.replacements,
             kernel_ms=m.kernel_ms, setup_ms=m.setup_ms,
             metrics=dict(rz=m.rz, rr=m.rr, pap=m.pap, alpha=m.alpha, stagnated=bool(m.reserved[0]),
-                         device_ms=m.reserved[1], kernel=KERNEL_NAMES.get(int(m.reserved[2]), "unknown")))
+                         device_ms=m.reserved[1], kernel=KERNEL_NAMES.get(int(m.reserved[2]), "unknown"),
+                         jacobi_fallback_at=int(m.reserved[3]) if int(m.reserved[2]) == 3 else -1))
+
+    def set_gtg(self, g_low, fallback_iters: int = 0) -> None:
+        """M^-1 = G^T G with G given on A's lower pattern (g_low order); None: Jacobi again."""
+        g = None if g_low is None else np.ascontiguousarray(g_low, np.float64)
+        check(lib.xplus_pcg_set_gtg(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(g), int(fallback_iters)))
+
+    def set_gnn(self, params=None, fallback_iters: int = 0) -> float:
+        """M^-1 = G^T G with G predicted on the GPU by the learned network (default: the
+        shipped weights).  Returns the inference time in ms."""
+        from .learned import load_weights
+        if params is None:
+            params, _ = load_weights()
+        p = np.ascontiguousarray(params, np.float32)
+        ms = C.c_double()
+        check(lib.xplus_pcg_set_gnn(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), ptr(p),
+                                    int(fallback_iters), C.byref(ms)))
+        return ms.value
+
+    def get_gtg(self) -> np.ndarray:
+        n = C.c_int64()
+        check(lib.xplus_pcg_get_gtg(self._h, None, C.byref(n)))
+        g = np.empty(n.value, np.float64)
+        check(lib.xplus_pcg_get_gtg(self._h, ptr(g), C.byref(n)))
+        return g
 
     def spmv(self, x) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64)

@@ -1,0 +1,227 @@
+"""The learned G^T G preconditioner on the GPU: the network's forward pass, probe loss,
+gradients and Adam step against the FP64 oracle; training lowers the loss; the G^T G solve
+agrees with an FP64 PCG of the same preconditioner, falls back to Jacobi, and the trained
+network needs fewer iterations than Jacobi on a system it was not trained on."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import gnn_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems():
+    from project_xplus_b200 import generators as gen
+    return [gen.fem2d(20, sigma=2.0, seed=5, perm_seed=1, rcm=True)[0],
+            gen.fem3d(6, sigma=1.5, seed=2, perm_seed=3, rcm=True)[0],
+            gen.fem2d(13, sigma=0.7, seed=9)[0]]
+
+
+def _params(seed=3):
+    """Initial parameters with a non-zero output layer, so every path carries signal."""
+    from project_xplus_b200 import learned as L
+    p = L.init_params(seed).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    off = 0
+    for name, shape in L.layout():
+        k = int(np.prod(shape))
+        if name in ("w", "wd"):
+            p[off:off + k] = rng.uniform(-0.2, 0.2, k)
+        if name == "bw":
+            p[off] = -0.1
+        off += k
+    return p.astype(np.float32)
+
+
+def _glow_from_oracle(d, go, gd):
+    g = O.graph(d.row_ptr, d.col_idx, d.values)
+    G = O.g_matrix(g, go, gd).tocsr()
+    n = d.n
+    rows = np.repeat(np.arange(n), np.diff(d.row_ptr))
+    keep = d.col_idx <= rows
+    return np.asarray(G[rows[keep], d.col_idx[keep]]).ravel()
+
+
+@pytest.fixture(scope="module")
+def trainer(gpu):
+    from project_xplus_b200.learned import GnnTrainer
+    syss = _systems()
+    t = GnnTrainer([(d.row_ptr, d.col_idx, d.values) for d in syss], probes=4, params=_params())
+    yield t, syss
+    t.close()
+
+
+def test_forward_matches_oracle(trainer):
+    t, syss = trainer
+    theta = _params()
+    t.set_params(theta)
+    for k, d in enumerate(syss):
+        g = O.graph(d.row_ptr, d.col_idx, d.values)
+        go, gd, _ = O.forward(theta.astype(np.float64), g, round_bf16=True)
+        ref = _glow_from_oracle(d, go, gd)
+        got = t.predict(k)
+        assert got.shape == ref.shape
+        np.testing.assert_allclose(got, ref, rtol=2e-4, atol=2e-5 * np.abs(ref).max())
+
+
+def test_loss_and_gradient_match_oracle(trainer):
+    t, syss = trainer
+    theta = _params()
+    t.set_params(theta)
+    for k, d in enumerate(syss):
+        seed = 40 + k
+        loss, grad = t.loss_grad(k, seed)
+        g = O.graph(d.row_ptr, d.col_idx, d.values)
+        v = O.probes(d.n, t.probes, seed)
+        L_ref, g_ref = O.loss_and_grad(theta.astype(np.float64), g, v, round_bf16=True)
+        assert abs(loss - L_ref) <= 1e-4 * L_ref
+        # per parameter block: FP32 sums against FP64 (ReLU masks may differ at exact kinks)
+        from project_xplus_b200 import learned as L
+        off = 0
+        for name, shape in L.layout():
+            m = int(np.prod(shape))
+            a, b = grad[off:off + m].astype(np.float64), g_ref[off:off + m]
+            scale = max(np.abs(b).max(), 1e-12)
+            assert np.abs(a - b).max() <= 2e-3 * scale + 1e-9, (k, name, np.abs(a - b).max(), scale)
+            off += m
+        cos = float(grad @ g_ref / (np.linalg.norm(grad) * np.linalg.norm(g_ref)))
+        assert cos > 0.99999
+
+
+def test_adam_matches_oracle(trainer):
+    t, _ = trainer
+    theta = _params(7)
+    t.set_params(theta)
+    rng = np.random.default_rng(1)
+    th, m, v = theta.astype(np.float64), np.zeros(theta.size), np.zeros(theta.size)
+    for step in (1, 2, 3):
+        g = rng.normal(0, 1e-2, theta.size).astype(np.float32)
+        t.adam(g, 1e-3)
+        th, m, v = O.adam(th, m, v, g.astype(np.float64), step, 1e-3)
+    np.testing.assert_allclose(t.params(), th, rtol=1e-5, atol=1e-7)
+
+
+def test_training_lowers_the_loss(gpu):
+    from project_xplus_b200 import generators as gen
+    from project_xplus_b200.learned import GnnTrainer
+    rng = np.random.default_rng(0)
+    syss = []
+    for k in range(6):
+        side = int(rng.integers(20, 40))
+        syss.append(gen.fem2d(side, sigma=float(rng.uniform(0.5, 2.5)), seed=100 + k, perm_seed=k, rcm=True)[0])
+    t = GnnTrainer([(d.row_ptr, d.col_idx, d.values) for d in syss], probes=8)
+    losses = t.train(400, lr=3e-3, lr_final=3e-4, seed=5)
+    assert np.all(np.isfinite(losses))
+    assert losses[-40:].mean() < 0.6 * losses[:6].mean()
+    # deterministic: the same seed and start give the same losses
+    from project_xplus_b200.learned import init_params
+    t.set_params(init_params(0))
+    again = t.train(400, lr=3e-3, lr_final=3e-4, seed=5)
+    np.testing.assert_array_equal(losses, again)
+    t.close()
+
+
+def _pcg_iters_fp64(d, G, tol=1e-8, maxit=20000):
+    """FP64 PCG with M^-1 = G^T G (the oracle's arithmetic, unrounded)."""
+    A = sp.csr_matrix((d.values, d.col_idx, d.row_ptr), shape=(d.n, d.n))
+    b = d.b
+    x = np.zeros(d.n)
+    r = b.copy()
+    z = G.T @ (G @ r)
+    p = z.copy()
+    rz = r @ z
+    bn = np.linalg.norm(b)
+    for it in range(maxit):
+        Ap = A @ p
+        al = rz / (p @ Ap)
+        x += al * p
+        r -= al * Ap
+        if np.linalg.norm(r) <= tol * bn:
+            return it + 1
+        z = G.T @ (G @ r)
+        rz2 = r @ z
+        p = z + (rz2 / rz) * p
+        rz = rz2
+    return maxit
+
+
+def _gmat(d, glow):
+    n = d.n
+    rows = np.repeat(np.arange(n), np.diff(d.row_ptr))
+    keep = d.col_idx <= rows
+    return sp.csr_matrix((glow, (rows[keep], d.col_idx[keep])), shape=(n, n))
+
+
+@pytest.fixture(scope="module")
+def sys64():
+    from project_xplus_b200 import generators as gen
+    return gen.fem2d(64, sigma=2.0, seed=11, perm_seed=4, rcm=True)[0]
+
+
+def test_gtg_with_jacobi_g_matches_jacobi(gpu, sys64):
+    from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
+    from project_xplus_b200.learned import jacobi_g
+    d = sys64
+    s = PcgSolver(d.row_ptr, d.col_idx, d.values, resident=False)
+    base = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    s.set_gtg(jacobi_g(d.row_ptr, d.col_idx, d.values))
+    r = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    assert r.converged and base.converged and r.residual_rel <= 1e-8
+    assert r.metrics["kernel"] == "pcg_gtg_kernel" and r.metrics["jacobi_fallback_at"] == -1
+    assert abs(r.iterations - base.iterations) <= max(3, 0.03 * base.iterations)
+    s.close()
+
+
+def test_gtg_with_fsai_matches_fp64_pcg(gpu, sys64):
+    from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
+    from project_xplus_b200.learned import fsai_lower
+    d = sys64
+    g = fsai_lower(d.row_ptr, d.col_idx, d.values)
+    ref = _pcg_iters_fp64(d, _gmat(d, g))
+    s = PcgSolver(d.row_ptr, d.col_idx, d.values)
+    s.set_gtg(g)
+    r = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    assert r.converged and r.residual_rel <= 1e-8
+    assert abs(r.iterations - ref) <= max(3, 0.05 * ref), (r.iterations, ref)
+    np.testing.assert_allclose(s.get_gtg(), g.astype(np.float64))
+    # Jacobi takes over at the cap and still converges
+    s.set_gtg(g, fallback_iters=15)
+    r2 = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    assert r2.converged and r2.metrics["jacobi_fallback_at"] == 15 and r2.residual_rel <= 1e-8
+    # back to Jacobi
+    s.set_gtg(None)
+    r3 = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    assert r3.converged and r3.metrics["kernel"] != "pcg_gtg_kernel"
+    s.close()
+
+
+def test_solver_inference_matches_trainer(trainer):
+    from project_xplus_b200 import PcgSolver
+    t, syss = trainer
+    theta = _params(4)
+    t.set_params(theta)
+    d = syss[0]
+    s = PcgSolver(d.row_ptr, d.col_idx, d.values)
+    s.set_gnn(theta)
+    np.testing.assert_array_equal(s.get_gtg(), t.predict(0))
+    s.close()
+
+
+def test_trained_network_beats_jacobi(gpu):
+    """Held-out system (not in the training set): the shipped weights need fewer iterations
+    than Jacobi-PCG to the same FP64 true residual."""
+    from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
+    from project_xplus_b200 import generators as gen
+    from project_xplus_b200.learned import load_weights
+    params, meta = load_weights()
+    for d in (gen.fem2d(150, sigma=2.0, seed=77, perm_seed=77, rcm=True)[0],
+              gen.fem3d(24, sigma=1.5, seed=78, perm_seed=78, rcm=True)[0]):
+        s = PcgSolver(d.row_ptr, d.col_idx, d.values, resident=False)
+        jac = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+        s.set_gnn(params)
+        lrn = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+        assert jac.converged and lrn.converged and lrn.residual_rel <= 1e-8
+        assert lrn.metrics["jacobi_fallback_at"] == -1
+        assert lrn.iterations < 0.7 * jac.iterations, (lrn.iterations, jac.iterations)
+        s.close()

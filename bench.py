@@ -367,8 +367,32 @@ def run_b200(args):
             if name == "fp64":
                 fp64_iters = r2.iterations
             s2.close()
+        # M^-1 = G^T G: G from the learned network (shipped weights, inference on the GPU) and
+        # the exact FSAI of the same pattern (host), both with the in-kernel Jacobi fallback
+        from project_xplus_b200.learned import fsai_lower, load_weights
+        params, _ = load_weights()
+        for name in ("learned_gtg", "fsai_gtg"):
+            s3 = xp.PcgSolver.from_dataset(d, device=local)
+            t0 = time.perf_counter()
+            if name == "learned_gtg":
+                s3.set_gnn(params)
+            else:
+                s3.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))
+            setup_ms = (time.perf_counter() - t0) * 1e3
+            runs = []
+            for _ in range(2):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                runs.append(s3.solve(d.b, None, tau=args.tol, tau_mode=_lib.XPLUS_TAU_REL_TRUE, max_iters=40000))
+            r3 = runs[-1]
+            compare[name] = {"time_to_tol_ms": r3.kernel_ms, "iterations": r3.iterations, "status": r3.status,
+                             "true_rel_residual": r3.residual_rel, "setup_ms": setup_ms,
+                             "jacobi_fallback_at": r3.metrics["jacobi_fallback_at"]}
+            s3.close()
         compare["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / kern_mean
         compare["speedup_vs_fp64"] = compare["fp64"]["time_to_tol_ms"] / kern_mean
+        for name in ("learned_gtg", "fsai_gtg"):
+            compare[name]["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / compare[name]["time_to_tol_ms"]
 
     # CPU baseline: the reference's own golden on a bounded sample, rank 0 only, N=1 only
     cpu = None

@@ -34,32 +34,62 @@ using namespace dev;
 constexpr int kGtgSlices = 1024;  // slice table capacity per CTA
 constexpr int kGChunk = 2;        // G / G^T SELL chunk (FP32 values, int32 columns)
 
-// Row `32 s + lane` of G (or G^T) in SELL form times x.  With RECOMP the operand is
-// r'_j = fma(-alpha, Ap'_j, r_j), recomputed exactly as the owner of row j computes it.
-template <bool RECOMP>
-__device__ __forceinline__ float g_row(const long long* __restrict__ sp, const int* __restrict__ col,
-                                       const float* __restrict__ val, int s, int lane, const float* x,
-                                       const float* ap, float nal) {
-    const long long base = sp[s];
-    const int w = static_cast<int>((sp[s + 1] - base) >> 5);
-    const float* vp = val + base + lane * kGChunk;
-    const int* cp = col + base + lane * kGChunk;
-    float acc = 0.0f;
-    for (int c = 0; c < w; c += kGChunk) {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(vp));
-        const int2 cc = __ldg(reinterpret_cast<const int2*>(cp));
-        float x0 = x[cc.x], x1 = x[cc.y];
-        if (RECOMP) {
-            x0 = __fmaf_rn(nal, ap[cc.x], x0);
-            x1 = __fmaf_rn(nal, ap[cc.y], x1);
+// NB rows (32 sl[k] + lane) of G or G^T in SELL form times x (sl[k] < 0: no row).  With RECOMP
+// the operand is r'_j = fma(-alpha, Ap'_j, r_j), recomputed exactly as the owner of row j
+// computes it.  The slot loads of all
+// rows are issued first, then all the gathers, then the arithmetic, so a warp keeps
+// NB * 2 * kGChunk loads in flight instead of walking its slices one dependent chain at a time.
+template <int NB, bool RECOMP>
+__device__ __forceinline__ void g_rows(const long long* __restrict__ sp, const int* __restrict__ col,
+                                       const float* __restrict__ val, const int (&sl)[NB], int lane, const float* x,
+                                       const float* ap, float nal, float (&out)[NB]) {
+    long long base[NB];
+    int w[NB], wmax = 0;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        out[k] = 0.0f;
+        if (sl[k] >= 0) {
+            base[k] = sp[sl[k]];
+            w[k] = static_cast<int>((sp[sl[k] + 1] - base[k]) >> 5);
+        } else {
+            base[k] = 0;
+            w[k] = 0;
         }
-        acc = fmaf(v.x, x0, acc);
-        acc = fmaf(v.y, x1, acc);
-        vp += 32 * kGChunk;
-        cp += 32 * kGChunk;
+        wmax = max(wmax, w[k]);
     }
-    return acc;
+    for (int c = 0; c < wmax; c += kGChunk) {
+        float2 v[NB];
+        int2 cc[NB];
+#pragma unroll
+        for (int k = 0; k < NB; ++k) {
+            if (c < w[k]) {
+                const long long off = base[k] + static_cast<long long>(c) * 32 + lane * kGChunk;
+                v[k] = __ldg(reinterpret_cast<const float2*>(val + off));
+                cc[k] = __ldg(reinterpret_cast<const int2*>(col + off));
+            } else {
+                v[k] = make_float2(0.0f, 0.0f);
+                cc[k] = make_int2(-1, -1);
+            }
+        }
+        float x0[NB], x1[NB];
+#pragma unroll
+        for (int k = 0; k < NB; ++k) {
+            x0[k] = cc[k].x >= 0 ? x[cc[k].x] : 0.0f;
+            x1[k] = cc[k].y >= 0 ? x[cc[k].y] : 0.0f;
+            if (RECOMP) {
+                if (cc[k].x >= 0) x0[k] = __fmaf_rn(nal, ap[cc[k].x], x0[k]);
+                if (cc[k].y >= 0) x1[k] = __fmaf_rn(nal, ap[cc[k].y], x1[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NB; ++k) {
+            out[k] = fmaf(v[k].x, x0[k], out[k]);
+            out[k] = fmaf(v[k].y, x1[k], out[k]);
+        }
+    }
 }
+
+constexpr int kGRows = 4;  // G rows of one warp in flight
 
 template <typename VT, int CHUNK, typename IT>
 __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
@@ -130,11 +160,22 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     // z = G^T t into the record, partial r.z (r = r_cur)
     auto z_phase = [&]() {
         double acc[1] = {0.0};
-        for (int s = sb + warp; s < se; s += wpb) {
-            const int row = s * 32 + lane;
-            const float zv = g_row<false>(a.gt_slice_ptr, a.gt_col, gtval, s, lane, t, nullptr, 0.0f);
-            rec[row].z = zv;
-            acc[0] += static_cast<double>(r_cur[row]) * static_cast<double>(zv);
+        for (int s0 = sb + warp; s0 < se; s0 += kGRows * wpb) {
+            int sl[kGRows];
+            float zv[kGRows], rv[kGRows];
+#pragma unroll
+            for (int k = 0; k < kGRows; ++k) {
+                const int s = s0 + k * wpb;
+                sl[k] = s < se ? s : -1;
+                rv[k] = s < se ? r_cur[s * 32 + lane] : 0.0f;
+            }
+            g_rows<kGRows, false>(a.gt_slice_ptr, a.gt_col, gtval, sl, lane, t, nullptr, 0.0f, zv);
+#pragma unroll
+            for (int k = 0; k < kGRows; ++k) {
+                if (sl[k] < 0) continue;
+                rec[sl[k] * 32 + lane].z = zv[k];
+                acc[0] += static_cast<double>(rv[k]) * static_cast<double>(zv[k]);
+            }
         }
         cur_bank = next_bank();
         publish<1>(acc, s_red, cur_bank);
@@ -149,8 +190,16 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
         rr = s_tot[1];
         true_rr = s_tot[2];
         if (!jac) {
-            for (int s = sb + warp; s < se; s += wpb)
-                t[s * 32 + lane] = g_row<false>(a.g_slice_ptr, a.g_col, gval, s, lane, r_cur, nullptr, 0.0f);
+            for (int s0 = sb + warp; s0 < se; s0 += kGRows * wpb) {
+                int sl[kGRows];
+                float tv[kGRows];
+#pragma unroll
+                for (int k = 0; k < kGRows; ++k) sl[k] = s0 + k * wpb < se ? s0 + k * wpb : -1;
+                g_rows<kGRows, false>(a.g_slice_ptr, a.g_col, gval, sl, lane, r_cur, nullptr, 0.0f, tv);
+#pragma unroll
+                for (int k = 0; k < kGRows; ++k)
+                    if (sl[k] >= 0) t[sl[k] * 32 + lane] = tv[k];
+            }
             if (!bar.sync(&s_flag)) return false;
             z_phase();
             if (!bar.sync(&s_flag)) return false;
@@ -225,22 +274,45 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             {
                 double acc[2] = {0.0, 0.0};
                 const float nal = -static_cast<float>(alpha);
-                for (int s = sb + warp; s < se; s += wpb) {
-                    const int row = s * 32 + lane;
-                    const NodeRec<float> me = load_rec(rec + row);
-                    const float pv = node_pnew(me.z, be, me.p);
-                    a.x64[row] += alpha * static_cast<double>(pv);
-                    const float rn = __fmaf_rn(nal, ap[row], r_cur[row]);
-                    r_nxt[row] = rn;
-                    if (jac) {
-                        const float zv = minv[row] * rn;
-                        store_rec(rec + row, zv, pv);
-                        acc[0] += static_cast<double>(rn) * static_cast<double>(zv);
-                    } else {
-                        rec[row].p = pv;
-                        t[row] = g_row<true>(a.g_slice_ptr, a.g_col, gval, s, lane, r_cur, ap, nal);
+                for (int s0 = sb + warp; s0 < se; s0 += kGRows * wpb) {
+                    int sl[kGRows];
+                    NodeRec<float> me[kGRows];
+                    float apv[kGRows], rv[kGRows];
+                    double xv[kGRows];
+#pragma unroll
+                    for (int k = 0; k < kGRows; ++k) {
+                        const int s = s0 + k * wpb;
+                        sl[k] = s < se ? s : -1;
+                        const int row = (s < se ? s : s0) * 32 + lane;
+                        me[k] = load_rec(rec + row);
+                        apv[k] = ap[row];
+                        rv[k] = r_cur[row];
+                        xv[k] = a.x64[row];
                     }
-                    acc[1] += static_cast<double>(rn) * static_cast<double>(rn);
+#pragma unroll
+                    for (int k = 0; k < kGRows; ++k) {
+                        if (sl[k] < 0) continue;
+                        const int row = sl[k] * 32 + lane;
+                        const float pv = node_pnew(me[k].z, be, me[k].p);
+                        a.x64[row] = xv[k] + alpha * static_cast<double>(pv);
+                        const float rn = __fmaf_rn(nal, apv[k], rv[k]);
+                        r_nxt[row] = rn;
+                        if (jac) {
+                            const float zv = minv[row] * rn;
+                            store_rec(rec + row, zv, pv);
+                            acc[0] += static_cast<double>(rn) * static_cast<double>(zv);
+                        } else {
+                            rec[row].p = pv;
+                        }
+                        acc[1] += static_cast<double>(rn) * static_cast<double>(rn);
+                    }
+                    if (!jac) {
+                        float tv[kGRows];
+                        g_rows<kGRows, true>(a.g_slice_ptr, a.g_col, gval, sl, lane, r_cur, ap, nal, tv);
+#pragma unroll
+                        for (int k = 0; k < kGRows; ++k)
+                            if (sl[k] >= 0) t[sl[k] * 32 + lane] = tv[k];
+                    }
                 }
                 cur_bank = next_bank();
                 publish<2>(acc, s_red, cur_bank);

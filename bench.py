@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison solves")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched solve")
+    ap.add_argument("--no-spmv3d", action="store_true", help="skip the SpMV on the 128^3 3D system")
     return ap.parse_args()
 
 
@@ -290,39 +291,70 @@ def run_b200(args):
     kern_mean = statistics.mean(kern_ms)
     achieved = bytes_launch / (kern_mean / 1e3) / 1e9
 
-    # SpMV alone: cold (L2 flushed before every launch) and warm (back to back)
-    xs = C.c_void_p()
-    ys = C.c_void_p()
-    _lib.check(_lib.lib.xplus_pcg_scratch_vectors(solver.handle, C.byref(xs), C.byref(ys)))
-    spmv_bytes = info["spmv_bytes"]
+    # SpMV alone: cold (L2 flushed before every launch) and warm (back to back), for the product
+    # layout (row-sum form, FP32 off-diagonals, int16 offsets) and for the plain layout (FP32
+    # values with the diagonal, int32 columns, 128-bit value and column loads)
+    def measure_spmv(handle):
+        xs = C.c_void_p()
+        ys = C.c_void_p()
+        _lib.check(_lib.lib.xplus_pcg_scratch_vectors(handle, C.byref(xs), C.byref(ys)))
 
-    def spmv():
-        _lib.check(_lib.lib.xplus_pcg_spmv_device(solver.handle, xs, ys, sp))
+        def spmv():
+            _lib.check(_lib.lib.xplus_pcg_spmv_device(handle, xs, ys, sp))
 
-    cold = []
-    for k in range(23):
-        flush.fill_(1.0)
+        cold = []
+        for k in range(23):
+            flush.fill_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            spmv()
+            b.record(stream)
+            b.synchronize()
+            if k >= 3:
+                cold.append(a.elapsed_time(b))
+        for _ in range(5):
+            spmv()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        spmv()
+        for _ in range(100):
+            spmv()
         b.record(stream)
         b.synchronize()
-        if k >= 3:
-            cold.append(a.elapsed_time(b))
-    for _ in range(5):
-        spmv()
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(100):
-        spmv()
-    b.record(stream)
-    b.synchronize()
-    warm_ms = a.elapsed_time(b) / 100
-    cold_ms = statistics.median(cold)
+        return statistics.median(cold), a.elapsed_time(b) / 100
+
+    spmv_bytes = info["spmv_bytes"]
+    cold_ms, warm_ms = measure_spmv(solver.handle)
     spmv_cold_gbs = spmv_bytes / (cold_ms / 1e3) / 1e9
     spmv_warm_gbs = spmv_bytes / (warm_ms / 1e3) / 1e9
+    plain = xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=4, row_sum_form=False,
+                                      index16=False, keep_fp64=False, device=local)
+    plain_bytes = plain.info()["spmv_bytes"]
+    p_cold_ms, p_warm_ms = measure_spmv(plain.handle)
+    plain.close()
+    spmv_plain = {"cold_gbs": plain_bytes / (p_cold_ms / 1e3) / 1e9, "warm_gbs": plain_bytes / (p_warm_ms / 1e3) / 1e9,
+                  "cold_ms": p_cold_ms, "warm_ms": p_warm_ms, "bytes": plain_bytes,
+                  "frac_cold": plain_bytes / (p_cold_ms / 1e3) / 1e9 / hbm,
+                  "layout": "fp32 values incl. diagonal, int32 columns, chunk 4 (128-bit value and column loads)"}
+
+    # The same SpMV on the 128^3 3D system (n = 2.1M, ~15 nnz/row), whose matrix is larger than
+    # L2 (126 MB), so back-to-back launches stream it from HBM: the kernel's bandwidth without
+    # the fixed launch cost that dominates a single ~60 MB launch.
+    spmv_large = None
+    if not args.no_spmv3d:
+        d3, _ = g.system_3d(128)
+        spmv_large = {"workload": "3d-p1fem-128^3-sigma1.5", "n": d3.n, "nnz": d3.nnz}
+        for name, kw in (("rowsum_int16", dict(values_dtype="f32", chunk=4)),
+                         ("plain_int32", dict(values_dtype="f32", chunk=4, row_sum_form=False, index16=False))):
+            s3 = xp.PcgSolver.from_dataset(d3, vector_dtype="f32", keep_fp64=False, device=local, **kw)
+            b3 = s3.info()["spmv_bytes"]
+            c_ms, w_ms = measure_spmv(s3.handle)
+            spmv_large[name] = {"bytes": b3, "cold_ms": c_ms, "stream_ms": w_ms,
+                                "cold_gbs": b3 / (c_ms / 1e3) / 1e9, "stream_gbs": b3 / (w_ms / 1e3) / 1e9,
+                                "frac_stream": b3 / (w_ms / 1e3) / 1e9 / hbm}
+            s3.close()
+        del d3
 
     # end to end through the public host-array API (pinned host buffers)
     e2e = None
@@ -417,7 +449,9 @@ def run_b200(args):
             "time_to_tol_ms": ms_per_step,
             "iterations": it_mean, "replacements": rp_mean, "true_rel_residual": max(relres),
             "spmv": {"cold_gbs": spmv_cold_gbs, "warm_gbs": spmv_warm_gbs, "cold_ms": cold_ms, "warm_ms": warm_ms,
-                     "bytes": spmv_bytes, "frac_cold": spmv_cold_gbs / hbm, "peak_kind": hbm_kind},
+                     "bytes": spmv_bytes, "frac_cold": spmv_cold_gbs / hbm, "peak_kind": hbm_kind,
+                     "layout": "row-sum form: fp32 off-diagonals + row sums, int16 column offsets, chunk 4",
+                     "plain": spmv_plain, "large_3d": spmv_large},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm,
                          "traffic": (RESIDENT1_DRAM_BYTES_PER_ITER * it_mean

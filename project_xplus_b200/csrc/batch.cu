@@ -306,11 +306,11 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     status = XPLUS_BREAKDOWN;
                     break;
                 }
-                bool do_replace = false;
+                bool do_replace = false, drop_replace = false;
                 if (true_mode) {
-                    if (rr_new <= tau_true_rr) do_replace = true;
+                    if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                     if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
-                    if (a.replace_drop2 > 0.0 && rr_new <= a.replace_drop2 * rr_at_replace) do_replace = true;
+                    if (a.replace_drop2 > 0.0 && rr_new <= a.replace_drop2 * rr_at_replace) do_replace = drop_replace = true;
                 }
                 if (do_replace) {
                     double t4[4];
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     status = XPLUS_BREAKDOWN;
                     break;
                 }
-                beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
+                beta = (drop_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
                 if (bad(beta)) {
                     status = XPLUS_BREAKDOWN;
                     break;

@@ -51,7 +51,7 @@ struct PcgArgs {
     int max_iters;
     int replace_every;
     double replace_drop;    // rr ratio that triggers a replacement (0: off)
-    int restart_on_replace; // 1: beta = 0 after a replacement (search direction restarts)
+    int restart_on_replace; // 1: beta = 0 after a drop- or convergence-triggered replacement
     long long timeout_ns;
     int debug_skip_block;   // test-only fault injection: block that skips its first arrival
     // SM-resident kernel only: per-CTA shared window {first row, rows} of the search direction,

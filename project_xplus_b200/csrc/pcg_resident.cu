@@ -268,11 +268,11 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            bool do_replace = false;
+            bool do_replace = false, drop_replace = false;
             if (true_mode) {
-                if (rr_new <= a.tau_true_rr) do_replace = true;
+                if (rr_new <= a.tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
-                if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = true;
+                if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
             if (do_replace) {
                 flush_dx();
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
+            beta = (drop_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;
@@ -591,11 +591,11 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            bool do_replace = false;
+            bool do_replace = false, drop_replace = false;
             if (true_mode) {
-                if (rr_new <= a.tau_true_rr) do_replace = true;
+                if (rr_new <= a.tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
-                if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = true;
+                if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
             if (do_replace) {
                 apply_update(static_cast<float>(pend));
@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = (do_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
+            beta = (drop_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;

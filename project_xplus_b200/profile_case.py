@@ -24,9 +24,13 @@ def main() -> None:
     ap.add_argument("--values", default="f32")
     ap.add_argument("--vectors", default="f32")
     ap.add_argument("--chunk", type=int, default=4)
+    ap.add_argument("--dim3", type=int, default=0, help="use the 3D P1-FEM system with this grid side instead")
+    ap.add_argument("--plain", action="store_true",
+                    help="plain layout: values with the diagonal, int32 columns (no row-sum form)")
     a = ap.parse_args()
-    d, _ = g.system_2d_large(a.grid)
-    s = PcgSolver.from_dataset(d, values_dtype=a.values, vector_dtype=a.vectors, chunk=a.chunk)
+    d, _ = g.system_3d(a.dim3) if a.dim3 else g.system_2d_large(a.grid)
+    extra = dict(row_sum_form=False, index16=False) if a.plain else {}
+    s = PcgSolver.from_dataset(d, values_dtype=a.values, vector_dtype=a.vectors, chunk=a.chunk, **extra)
     for _ in range(2):
         r = s.solve(d.b, None, tau=1e-300, max_iters=a.iters)
     xs, ys = C.c_void_p(), C.c_void_p()

@@ -395,6 +395,16 @@ int xplus_sell_build(int n, const int* row_ptr, const int* col_idx, const double
                      int* perm, int64_t* slice_ptr, int* slice_width, int* col, double* val,
                      double* diag);
 
+/* The same SELL-C-sigma layout built on the GPU from device CSR arrays, bit-identical to
+ * xplus_sell_build (C = 32, sigma <= 4096).  Two-phase: NULL d_col, d_val and d_diag return
+ * only *n_slices and *slots (d_perm, d_slice_ptr, d_slice_width are filled when given).
+ * Outputs are device arrays of the sizes xplus_sell_build uses (d_diag: n).  Temporaries are
+ * allocated and freed inside; the call returns after the work on `stream` is done. */
+int xplus_sell_build_device(int n, const int* d_row_ptr, const int* d_col_idx, const double* d_values,
+                            int C, int sigma, int chunk, int diag_split, int* n_slices, int64_t* slots,
+                            int* d_perm, int64_t* d_slice_ptr, int* d_slice_width, int* d_col,
+                            double* d_val, double* d_diag, void* stream);
+
 /* Cuper packed-format import (host/cuper_control_matrix.hpp:73-83,130-207): decode the
  * 16 channel streams (channel_words words each) into COO triplets in the order they are
  * stored, skipping padding.  Returns the count in *nnz_out; rows/cols/vals may be NULL

@@ -87,6 +87,7 @@ _SIGS = {
     "xplus_rcm": (_i, [_i, _p, _p, _p]),
     "xplus_permute_symmetric": (_i, [_i, _p, _p, _p, _p, _p, _p, _p]),
     "xplus_sell_build": (_i, [_i, _p, _p, _p, _i, _i, _i, _i, _ip, C.POINTER(_i64), _p, _p, _p, _p, _p, _p]),
+    "xplus_sell_build_device": (_i, [_i, _p, _p, _p, _i, _i, _i, _i, _ip, C.POINTER(_i64), _p, _p, _p, _p, _p, _p, _p]),
     "xplus_cuper_unpack": (_i, [_i, _i, _p, _p, _i64, C.POINTER(_i64), _p, _p, _p]),
     "spmv_csr_kernel": (None, [_p, _p, _p, _p, _p, _i]),
     "spmv_blocked_kernel": (None, [_p, _p, _p, _p, _p, _i]),

@@ -104,6 +104,31 @@ def sell_build(row_ptr, col_idx, values, C_=32, sigma=256, chunk=1, diag_split=F
                 col=col, val=val, diag=diag)
 
 
+def sell_build_device(row_ptr, col_idx, values, C_=32, sigma=256, chunk=1, diag_split=False, device=0) -> dict:
+    """xplus_sell_build_device on torch CUDA tensors; returns the same fields as sell_build
+    (as torch tensors on the device)."""
+    import torch
+    dev = torch.device("cuda", device)
+    rp = torch.as_tensor(np.ascontiguousarray(row_ptr, np.int32), device=dev)
+    ci = torch.as_tensor(np.ascontiguousarray(col_idx, np.int32), device=dev)
+    v = torch.as_tensor(np.ascontiguousarray(values, np.float64), device=dev)
+    n = len(row_ptr) - 1
+    ns, slots = C.c_int(), C.c_int64()
+    torch.cuda.synchronize(dev)
+    args = (n, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), C_, sigma, chunk, int(diag_split))
+    check(lib.xplus_sell_build_device(*args, C.byref(ns), C.byref(slots), None, None, None, None, None, None, None))
+    perm = torch.empty(n, dtype=torch.int32, device=dev)
+    sp = torch.empty(ns.value + 1, dtype=torch.int64, device=dev)
+    sw = torch.empty(ns.value, dtype=torch.int32, device=dev)
+    col = torch.empty(slots.value, dtype=torch.int32, device=dev)
+    val = torch.empty(slots.value, dtype=torch.float64, device=dev)
+    diag = torch.empty(n, dtype=torch.float64, device=dev) if diag_split else None
+    check(lib.xplus_sell_build_device(*args, C.byref(ns), C.byref(slots), perm.data_ptr(), sp.data_ptr(), sw.data_ptr(),
+                                      col.data_ptr(), val.data_ptr(), None if diag is None else diag.data_ptr(), None))
+    return dict(n_slices=ns.value, slots=slots.value, perm=perm, slice_ptr=sp, slice_width=sw, col=col, val=val,
+                diag=diag)
+
+
 def cuper_unpack(n, batch_count, sp_element_list_ptr, words, channel_words):
     """Decodes the reference's packed 16-channel words into COO (row, col, fp32 value)."""
     ptr_a = np.ascontiguousarray(sp_element_list_ptr, np.int32)

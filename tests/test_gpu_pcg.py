@@ -294,3 +294,17 @@ def test_timeout_path_reports_status(gpu, sys0):
     assert _lib.lib.xplus_pcg_debug_skip_arrival(s.handle, -1) == 0
     r = s.solve(d.b, None, tau=1e-10)
     assert r.status == "converged"
+
+
+@pytest.mark.parametrize("sigma,chunk,split", [(1, 1, False), (32, 2, True), (256, 4, True), (256, 4, False),
+                                               (1024, 2, False), (4096, 8, True)])
+def test_gpu_sell_builder_is_bit_exact(gpu, sigma, chunk, split):
+    """The GPU builder against the host builder: every output array identical."""
+    for d in (g.fem2d(70, sigma=2.0, perm_seed=3, rcm=True)[0], g.fem3d(13, sigma=1.5)[0], g.fem2d(5)[0]):
+        h = g.sell_build(d.row_ptr, d.col_idx, d.values, 32, sigma, chunk, split)
+        dv = g.sell_build_device(d.row_ptr, d.col_idx, d.values, 32, sigma, chunk, split)
+        assert dv["n_slices"] == h["n_slices"] and dv["slots"] == h["slots"]
+        for k in ("perm", "slice_ptr", "slice_width", "col", "val"):
+            np.testing.assert_array_equal(dv[k].cpu().numpy(), h[k], err_msg=k)
+        if split:
+            np.testing.assert_array_equal(dv["diag"].cpu().numpy(), h["diag"])

@@ -354,6 +354,28 @@ def run_b200(args):
                                 "cold_gbs": b3 / (c_ms / 1e3) / 1e9, "stream_gbs": b3 / (w_ms / 1e3) / 1e9,
                                 "frac_stream": b3 / (w_ms / 1e3) / 1e9 / hbm}
             s3.close()
+    # The 3D system as a mixed-precision workload: values in FP32, BF16 or FP16 (power-of-two
+    # scale), FP32 inner PCG, FP64 residual replacement every 50 iterations or at a 1e-4 drop
+    # of the recurrence residual, to 1e-10 FP64 true relative residual; FP64 for comparison.
+    mixed_3d = None
+    if not args.no_spmv3d and not args.no_compare:
+        mixed_3d = {"workload": "3d-p1fem-128^3-sigma1.5, tol 1e-10 rel. FP64 true residual", "n": d3.n}
+        for name, kw in (("f32_values", dict(values_dtype="f32", vector_dtype="f32")),
+                         ("bf16_values", dict(values_dtype="bf16", vector_dtype="f32")),
+                         ("f16_values", dict(values_dtype="f16", vector_dtype="f32")),
+                         ("fp64", dict(values_dtype="f64", vector_dtype="f64", chunk=2))):
+            s3 = xp.PcgSolver.from_dataset(d3, replace_every=50, replace_drop=1e-4, device=local, **kw)
+            runs = []
+            for _ in range(2):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                runs.append(s3.solve(d3.b, None, tau=1e-10, tau_mode=_lib.XPLUS_TAU_REL_TRUE, max_iters=20000))
+            r3 = runs[-1]
+            mixed_3d[name] = {"time_to_tol_ms": r3.kernel_ms, "iterations": r3.iterations, "status": r3.status,
+                              "replacements": r3.replacements, "true_rel_residual": r3.residual_rel,
+                              "kernel": r3.metrics["kernel"]}
+            s3.close()
+    if not args.no_spmv3d:
         del d3
 
     # end to end through the public host-array API (pinned host buffers)
@@ -452,6 +474,7 @@ def run_b200(args):
                      "bytes": spmv_bytes, "frac_cold": spmv_cold_gbs / hbm, "peak_kind": hbm_kind,
                      "layout": "row-sum form: fp32 off-diagonals + row sums, int16 column offsets, chunk 4",
                      "plain": spmv_plain, "large_3d": spmv_large},
+            "mixed_3d": mixed_3d,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm,
                          "traffic": (RESIDENT1_DRAM_BYTES_PER_ITER * it_mean
@@ -475,6 +498,41 @@ def run_b200(args):
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+def _golden_solve(payload):
+    """One system solved by the reference's run_jacobi_pcg (oracle/_ref when built, else the
+    port), tolerance on ||r|| relative to ||b||; returns (seconds, iterations)."""
+    rp, ci, v, b, tol = payload
+    from oracle import oracle as O
+    from project_xplus_b200.solver import CsrDataset
+    d = CsrDataset(rp, ci, v, b, np.zeros(len(b)))
+    tau_rr = (tol * float(np.linalg.norm(b))) ** 2
+    t0 = time.perf_counter()
+    r = O.golden(d, tau_rr, 0, use_ref=O.reflib() is not None)
+    return time.perf_counter() - t0, int(r["iterations"])
+
+
+def batch_cpu_baseline(systems, works, tol, sample=24):
+    """The reference's CPU solver on the batch, as independent single-thread processes on all
+    host cores: a bounded sample of systems spread over the work range is solved in full and
+    the total is extrapolated by the work estimate nnz * sqrt(n) of every system."""
+    import multiprocessing as mp
+    order = np.argsort(works)
+    pick = [int(order[int(i)]) for i in np.linspace(0, len(order) - 1, min(sample, len(order)))]
+    cores = os.cpu_count() or 1
+    payloads = [(systems[k].row_ptr, systems[k].col_idx, systems[k].values, systems[k].b, tol) for k in pick]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(min(cores, len(payloads))) as pool:
+        res = pool.map(_golden_solve, payloads)
+    wall = time.perf_counter() - t0
+    per_work = sum(t for t, _ in res) / sum(works[k] for k in pick)
+    total_cpu_s = per_work * sum(works)
+    est_wall = total_cpu_s / cores
+    return {"value": len(systems) / est_wall, "unit": "systems/s", "cores": cores, "kind": "reference",
+            "sample": f"{len(pick)} of {len(systems)} systems (spread over the work range) solved by the reference "
+                      f"run_jacobi_pcg, one process per core; total CPU time {total_cpu_s:.1f} s extrapolated by "
+                      f"nnz*sqrt(n), divided over {cores} cores (sample wall {wall:.1f} s)"}
 
 
 def run_batch(args, world, rank, pg, dev, stream, flush):
@@ -519,11 +577,16 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
         raise SystemExit(f"batch: {int((r['status'] != 0).sum())} systems did not converge")
     tot = max_over_ranks(pg, sum(ms), dev)
     s.close()
-    return {"workload": "512 x 2d-p1fem, side log-uniform [45,256], sigma log-uniform [0.5,2.5], fp32, tol 1e-8",
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = batch_cpu_baseline(systems, [works[k] for k in mine], args.tol)
+    return {"cpu_baseline": cpu, "workload": "512 x 2d-p1fem, side log-uniform [45,256], sigma log-uniform [0.5,2.5], fp32, tol 1e-8",
             "systems": len(sides), "sum_n": int(sum(int(sd) ** 2 for sd in sides)),
             "value": len(sides) * args.steps / (tot / 1e3), "unit": "systems/s", "ms_per_step": tot / args.steps,
             "scaling": "strong (systems split over ranks)", "iterations_total": int(r["iterations"].sum()),
             "iterations_max": int(r["iterations"].max()), "max_true_rel_residual": float(r["true_rel"].max()),
+            "system_ms": {"max": float(r["system_ms"].max()), "median": float(np.median(r["system_ms"])),
+                          "sum": float(r["system_ms"].sum())},
             "launch": {"cluster": info["cluster"], "block_threads": info["block_threads"], "grid": info["grid"],
                        "autotune_ms": tune["ms"]},
             "graph": True}

@@ -96,16 +96,24 @@ typedef struct xplus_opts {
     int resident;          /* FP32 vectors, row-sum form: use the SM-resident kernel (state and
                               the search direction's band + halo in shared memory) when one CTA
                               per SM holds it (default 1) */
-    int restart_on_replace; /* after an FP64 residual replacement triggered by the convergence check
-                              or by a replace_drop fall of ||r||: 1 restarts the search direction
-                              (p = z), 0 keeps it; -1 (default) restarts only for 16-bit values,
-                              whose inexact operator breaks the conjugacy a kept p relies on.
-                              Periodic replacements (replace_every) always keep the direction:
-                              restarting every k iterations turns the solve into restarted CG(k),
-                              which stalls (measured on a 150^2 sigma=2 system with BF16 values) */
+    int restart_on_replace; /* search direction after an FP64 residual replacement: 0 keeps it,
+                              1 restarts it (p = z) after every replacement, 2 restarts it only
+                              after replacements triggered by a replace_drop fall of ||r|| or by
+                              the convergence check (periodic ones, replace_every, keep it),
+                              3 adaptive: starts as 2 and switches to 1 for the rest of the solve
+                              when ||b - A x|| grows past twice its best or stagnation_window
+                              replacements bring no progress.  -1 (default): 3 for 16-bit values,
+                              whose inexact operator can break the conjugacy a kept p relies on,
+                              0 otherwise.  Measured with FP16 values, replacement every 50
+                              iterations or at a 1e-4 drop: 2D 150^2 sigma=2 needs 2 (1154
+                              iterations; 1 takes 4890), 3D 128^3 needs 1 (1735; 2 stalls) */
     int barriers_per_iter; /* SM-resident kernel: 1 (default) folds both dot products into one
                               reduction by expanding r_{k+1}.z_{k+1} and r_{k+1}.r_{k+1} in alpha;
                               2 reduces them after the update as the reference does */
+    double stagnation_gain; /* TAU_REL_TRUE: an FP64 replacement counts as progress when it lowers
+                              the best ||b - A x|| by this fraction (default 0.05) ... */
+    int stagnation_window; /* ... and this many replacements in a row without progress stop the
+                              solve (status XPLUS_MAX_ITER, metrics.reserved[0] = 1; default 8) */
 } xplus_opts;
 
 typedef struct xplus_metrics {

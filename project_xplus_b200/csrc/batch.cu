@@ -59,7 +59,9 @@ struct BatchArgs {
     int max_iters;            // <= 0: max(4n, 1000) per system
     int replace_every;
     double replace_drop2;     // squared ||r|| drop that triggers a replacement (0: off)
-    int restart_on_replace;
+    int restart_on_replace;   // 1: beta = 0 after every replacement, 2: after drop/convergence ones
+    double stag_factor;
+    int stag_window;
     int* out_status;
     int* out_iters;
     int* out_repl;
@@ -188,6 +190,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
         double rr_at_replace = rr, best_true = true_rr;
         double pap = 0.0, alpha = 0.0, beta = 0.0;
         int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0;
+        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
         bool stagnated = false;
         const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau);
 
@@ -320,11 +323,17 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     true_rr = t4[2];
                     ++replacements;
                     rr_at_replace = rr_new;
-                    if (true_rr < 0.9 * best_true) {
+                    if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
+                    if (true_rr < a.stag_factor * best_true) {
                         best_true = true_rr;
                         stagnant = 0;
-                    } else if (++stagnant >= 8) {
-                        stagnated = true;
+                    } else if (++stagnant >= a.stag_window) {
+                        if (a.restart_on_replace == 3 && restart_mode == 2) {
+                            restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
+                            stagnant = 0;
+                        } else {
+                            stagnated = true;
+                        }
                     }
                 }
                 rz = rz_new;
@@ -338,7 +347,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     status = XPLUS_BREAKDOWN;
                     break;
                 }
-                beta = (drop_replace && a.restart_on_replace) ? 0.0 : rz / rz_old;
+                beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace)) ? 0.0 : rz / rz_old;
                 if (bad(beta)) {
                     status = XPLUS_BREAKDOWN;
                     break;
@@ -774,7 +783,8 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     a.replace_every = h->opts.replace_every;
     a.replace_drop2 = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
     const bool low = h->opts.value_type != XPLUS_F32;
-    a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 1 : 0) : h->opts.restart_on_replace;
+    a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 3 : 0) : h->opts.restart_on_replace;
+    stagnation_args(h->opts, &a.stag_factor, &a.stag_window);
     a.out_status = h->d_status;
     a.out_iters = h->d_iters;
     a.out_repl = h->d_repl;

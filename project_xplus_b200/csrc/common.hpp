@@ -63,6 +63,15 @@ struct SellHost {
     std::vector<double> diag;     // only with diag_split (new order)
 };
 
+// Stagnation test of the FP64 replacement loop from the options: a replacement is progress when
+// ||b - A x||^2 falls below factor x best (factor = (1 - gain)^2); `window` replacements in a
+// row without progress stop the solve.
+inline void stagnation_args(const xplus_opts& o, double* factor, int* window) {
+    const double g = o.stagnation_gain > 0.0 && o.stagnation_gain < 1.0 ? o.stagnation_gain : 0.05;
+    *factor = (1.0 - g) * (1.0 - g);
+    *window = o.stagnation_window > 0 ? o.stagnation_window : 8;
+}
+
 // SELL-C-sigma builder (the single implementation behind xplus_sell_build).
 void sell_build(int n, const int* row_ptr, const int* col_idx, const double* values, int C,
                 int sigma, int chunk, int diag_split, SellHost& out);

@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     double rr_at_replace = rr, best_true = true_rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
+        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
     const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
 
     if (converged_now) {
@@ -361,13 +362,19 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 rr_new = rr;
                 ++replacements;
                 rr_at_replace = rr_new;
+                if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
                 if (restart) {
                     best_true = true_rr;
-                } else if (true_rr < 0.9 * best_true) {
+                } else if (true_rr < a.stag_factor * best_true) {
                     best_true = true_rr;
                     stagnant = 0;
-                } else if (++stagnant >= 8) {
-                    stagnated = 1;
+                } else if (++stagnant >= a.stag_window) {
+                    if (a.restart_on_replace == 3 && restart_mode == 2) {
+                        restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
+                        stagnant = 0;
+                    } else {
+                        stagnated = 1;
+                    }
                 }
             }
             if (lead && a.trace && it < a.trace_cap) {
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = ((drop_replace && a.restart_on_replace) || restart) ? 0.0 : rz / rz_old;
+            beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace) || restart) ? 0.0 : rz / rz_old;
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;

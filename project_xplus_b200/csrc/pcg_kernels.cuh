@@ -51,7 +51,9 @@ struct PcgArgs {
     int max_iters;
     int replace_every;
     double replace_drop;    // rr ratio that triggers a replacement (0: off)
-    int restart_on_replace; // 1: beta = 0 after a drop- or convergence-triggered replacement
+    int restart_on_replace; // after a replacement beta = 0: 1 always, 2 only when drop- or convergence-triggered
+    double stag_factor;     // a replacement counts as progress when ||b-Ax||^2 < stag_factor * best
+    int stag_window;        // replacements without progress that stop the solve
     long long timeout_ns;
     int debug_skip_block;   // test-only fault injection: block that skips its first arrival
     // SM-resident kernel only: per-CTA shared window {first row, rows} of the search direction,

@@ -175,6 +175,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     require(o.slice_height == 32, XPLUS_ERR_ARG, "slice_height must be 32");
     require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
     require(o.sigma >= 1, XPLUS_ERR_ARG, "sigma must be >= 1");
+    require(o.restart_on_replace >= -1 && o.restart_on_replace <= 3, XPLUS_ERR_ARG, "restart_on_replace must be -1..3");
     validate_csr(n, row_ptr, col_idx, row_ptr[n]);
     std::vector<double> diag(static_cast<size_t>(n));
     jacobi_diag(n, row_ptr, col_idx, values, diag.data());
@@ -411,6 +412,7 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     a.block_clk = h->d_block_clk;
     a.flush_every = 16;
     a.timeout_ns = static_cast<long long>((h->opts.barrier_timeout_s > 0 ? h->opts.barrier_timeout_s : 2.0) * 1e9);
+    stagnation_args(h->opts, &a.stag_factor, &a.stag_window);
     if (tau_mode == XPLUS_TAU_ABS_RR) {
         a.tau_rr = tau;
         a.tau_true_rr = -1.0;
@@ -421,7 +423,7 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
         a.replace_every = h->opts.replace_every;
         a.replace_drop = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
         const bool low = h->opts.value_type == XPLUS_BF16 || h->opts.value_type == XPLUS_F16;
-        a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 1 : 0) : h->opts.restart_on_replace;
+        a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 3 : 0) : h->opts.restart_on_replace;
     }
     cuda_check(cudaMemsetAsync(h->d_bar, 0, sizeof(unsigned), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
@@ -611,6 +613,8 @@ void xplus_opts_default(xplus_opts* o) {
     o->resident = 1;
     o->barriers_per_iter = 1;
     o->restart_on_replace = -1;
+    o->stagnation_gain = 0.05;
+    o->stagnation_window = 8;
 }
 
 int xplus_device_count(void) {

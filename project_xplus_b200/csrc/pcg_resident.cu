@@ -514,7 +514,29 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 const float4* za4 = reinterpret_cast<const float4*>(rec_za(gen) + w0);
                 const float4* p4 = reinterpret_cast<const float4*>(rec_p(gen) + w0);
                 float4* pw4 = reinterpret_cast<float4*>(pw);
-                for (int t = threadIdx.x; t < (wn >> 2); t += blockDim.x) {
+                // four float4 groups per thread in flight: all twelve loads before any store
+                constexpr int U = 4;
+                const int nq = wn >> 2, bd = static_cast<int>(blockDim.x);
+                int t = threadIdx.x;
+                for (; t + (U - 1) * bd < nq; t += U * bd) {
+                    float4 z[U], q[U], p[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        z[u] = zr4[t + u * bd];
+                        q[u] = za4[t + u * bd];
+                        p[u] = p4[t + u * bd];
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        float4 o;
+                        o.x = __fmaf_rn(be, p[u].x, __fmaf_rn(-al_prev, q[u].x, z[u].x));
+                        o.y = __fmaf_rn(be, p[u].y, __fmaf_rn(-al_prev, q[u].y, z[u].y));
+                        o.z = __fmaf_rn(be, p[u].z, __fmaf_rn(-al_prev, q[u].z, z[u].z));
+                        o.w = __fmaf_rn(be, p[u].w, __fmaf_rn(-al_prev, q[u].w, z[u].w));
+                        pw4[t + u * bd] = o;
+                    }
+                }
+                for (; t < nq; t += bd) {
                     const float4 z = zr4[t], q = za4[t], p = p4[t];
                     float4 o;
                     o.x = __fmaf_rn(be, p.x, __fmaf_rn(-al_prev, q.x, z.x));
@@ -525,6 +547,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 }
                 __syncthreads();
             }
+            clock(2);
             // ---- Ap' from shared memory ----
             for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
                 int2 sl[NS];
@@ -547,6 +570,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 }
             }
             __syncthreads();
+            clock(3);
             // ---- records of the next generation and the seven sums ----
             {
                 double acc[kPartials1] = {0, 0, 0, 0, 0, 0, 0};

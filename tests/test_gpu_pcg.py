@@ -312,3 +312,48 @@ def test_gpu_sell_builder_is_bit_exact(gpu, sigma, chunk, split):
             np.testing.assert_array_equal(dv[k].cpu().numpy(), h[k], err_msg=k)
         if split:
             np.testing.assert_array_equal(dv["diag"].cpu().numpy(), h["diag"])
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 33, 65])
+def test_ragged_and_tiny_systems_match_golden(gpu, oracle, n):
+    """Sizes that leave a partial last slice (or a single row): FP64 path against the golden."""
+    rng = np.random.default_rng(n)
+    # tridiagonal SPD system with a random positive diagonal excess
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j in (i - 1, i, i + 1):
+            if 0 <= j < n:
+                rows.append(i); cols.append(j)
+                vals.append(2.0 + rng.uniform(0.1, 1.0) if i == j else -1.0)
+    import scipy.sparse as sps
+    A = sps.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    b = rng.uniform(-1, 1, n)
+    d = xp.CsrDataset(A.indptr, A.indices, A.data, b, np.zeros(n))
+    gr = oracle.golden(d, 1e-24, 0)
+    for vdt, xdt in (("f64", "f64"), ("f32", "f32")):
+        s = xp.PcgSolver.from_dataset(d, values_dtype=vdt, vector_dtype=xdt)
+        r = s.solve(d.b, None, tau=1e-12 if xdt == "f64" else 1e-10, tau_mode=xp.XPLUS_TAU_REL_TRUE, max_iters=4 * n + 10)
+        assert r.converged, (vdt, r.status)
+        np.testing.assert_allclose(r.solution, gr["x"], rtol=0, atol=1e-6 * np.abs(gr["x"]).max())
+        if xdt == "f64":
+            assert abs(r.iterations - gr["iterations"]) <= 2
+        s.close()
+
+
+def test_diagonal_matrix_converges_in_one_iteration(gpu):
+    n = 1000
+    diag = np.linspace(1.0, 50.0, n)
+    d = xp.CsrDataset(np.arange(n + 1), np.arange(n), diag, np.ones(n), np.zeros(n))
+    s = xp.PcgSolver.from_dataset(d, values_dtype="f64", vector_dtype="f64")
+    r = s.solve(d.b, tau=1e-24)
+    assert r.converged and r.iterations == 1
+    np.testing.assert_allclose(r.solution, 1.0 / diag, rtol=1e-14)
+
+
+def test_max_iters_one_and_exact_start(gpu, sys0):
+    d, xt = sys0
+    s = xp.PcgSolver.from_dataset(d)
+    r = s.solve(d.b, tau=1e-30, max_iters=1)
+    assert r.status == "max_iter" and r.iterations == 1
+    r0 = s.solve(d.b, xt, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE)
+    assert r0.converged and r0.iterations == 0

@@ -286,17 +286,36 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                 {
                     double acc[2] = {0.0, 0.0};
                     const float al = static_cast<float>(alpha);
-                    for (int s = sb + warp; s < se; s += wpb) {
-                        const int row = s * 32 + lane;
-                        const NodeRec<float> me = ldcg_rec(a.rec + row);
-                        const float pv = node_pnew(me.z, be, me.p);
-                        a.x64[row] += alpha * static_cast<double>(pv);
-                        const float rv = a.r[row] - al * a.ap[row];
-                        const float zv = a.minv[row] * rv;
-                        a.r[row] = rv;
-                        store_rec(a.rec + row, zv, pv);
-                        acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
-                        acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
+                    // four slices of the warp at once: every load before any arithmetic
+                    constexpr int NB = 4;
+                    for (int s0 = sb + warp; s0 < se; s0 += NB * wpb) {
+                        NodeRec<float> me[NB];
+                        double xv[NB];
+                        float r0[NB], apv[NB], mv[NB];
+                        int row[NB];
+#pragma unroll
+                        for (int k = 0; k < NB; ++k) {
+                            const int s = s0 + k * wpb;
+                            row[k] = s < se ? s * 32 + lane : -1;
+                            const int rr_ = row[k] >= 0 ? row[k] : s0 * 32 + lane;
+                            me[k] = ldcg_rec(a.rec + rr_);
+                            xv[k] = a.x64[rr_];
+                            r0[k] = a.r[rr_];
+                            apv[k] = a.ap[rr_];
+                            mv[k] = a.minv[rr_];
+                        }
+#pragma unroll
+                        for (int k = 0; k < NB; ++k) {
+                            if (row[k] < 0) continue;
+                            const float pv = node_pnew(me[k].z, be, me[k].p);
+                            a.x64[row[k]] = xv[k] + alpha * static_cast<double>(pv);
+                            const float rv = r0[k] - al * apv[k];
+                            const float zv = mv[k] * rv;
+                            a.r[row[k]] = rv;
+                            store_rec(a.rec + row[k], zv, pv);
+                            acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
+                            acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
+                        }
                     }
                     cluster_sum<2>(cl, acc, s_red, s_part, s_tot, pbank);
                     rz_new = acc[0];

@@ -183,18 +183,19 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            // ---- phase B: x, r, z and the two dots; the record becomes {z_new, p'}; two
-            //      slices per step so the loads of both are in flight together ----
+            // ---- phase B: x, r, z and the two dots; the record becomes {z_new, p'}; four
+            //      slices per step so the loads of all are in flight together ----
             {
                 double acc[2] = {0.0, 0.0};
                 const XT al = static_cast<XT>(alpha);
-                for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
-                    int row[NS];
-                    NodeRec<XT> me[NS];
-                    XT apv[NS], rv0[NS], mv[NS];
-                    double xv[NS];
+                constexpr int NB = 4;  // slices of one warp whose loads are in flight together
+                for (int s0 = sb + warp; s0 < se; s0 += NB * wpb) {
+                    int row[NB];
+                    NodeRec<XT> me[NB];
+                    XT apv[NB], rv0[NB], mv[NB];
+                    double xv[NB];
 #pragma unroll
-                    for (int k = 0; k < NS; ++k) {
+                    for (int k = 0; k < NB; ++k) {
                         const int s = s0 + k * wpb;
                         row[k] = s < se ? s * 32 + lane : -1;
                         const int rr_ = row[k] >= 0 ? row[k] : s0 * 32 + lane;
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
                         xv[k] = a.x64[rr_];
                     }
 #pragma unroll
-                    for (int k = 0; k < NS; ++k) {
+                    for (int k = 0; k < NB; ++k) {
                         if (row[k] < 0) continue;
                         const XT pv = node_pnew(me[k].z, be, me[k].p);
                         a.x64[row[k]] = xv[k] + alpha * static_cast<double>(pv);

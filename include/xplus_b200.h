@@ -92,7 +92,9 @@ typedef struct xplus_opts {
     int index16;           /* store columns as int16 offsets from the row when every |col - row|
                               < 32768 after ordering (lossless; default 1) */
     int l2_persist;        /* mark the matrix stream as persisting in L2 for the solve launch
-                              (default 1; sets this process's persisting-L2 limit) */
+                              (default 1).  Raises this process's persisting-L2 limit while the
+                              handle exists; destroying the handle releases its persisting lines
+                              and the last such handle restores the previous limit */
     int resident;          /* FP32 vectors, row-sum form: use the SM-resident kernel (state and
                               the search direction's band + halo in shared memory) when one CTA
                               per SM holds it (default 1) */
@@ -290,9 +292,10 @@ int xplus_batch_destroy(xplus_batch* h);
  * clusters as the device holds at once.  XPLUS_ERR_CUDA when the shape cannot launch. */
 int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads);
 /* The launch-shape autotuner: times every cluster x block_threads shape that launches and keeps
- * the fastest, on b = 1, x0 = 0 for every system.  iters > 0: that many PCG iterations per
- * system; iters <= 0: every system solved to FP64 true relative residual tau (0 < tau < 1),
- * so the queue's makespan is what is timed.  Returns the shape and its time (min of 2 runs). */
+ * the fastest, with x0 = 0 for every system.  iters > 0: that many PCG iterations per system on
+ * b = 1; iters <= 0: every system solved to FP64 true relative residual tau (0 < tau < 1) on the
+ * right-hand side of the last solve (b = 1 before any solve), so the queue's makespan on the
+ * caller's workload is what is timed.  Returns the shape and its time (min of 2 runs). */
 int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, int* block_threads,
                          double* best_ms);
 /* Blocking solve with host vectors of length sum(ns) (x0 NULL: zeros).  tau / tau_mode /

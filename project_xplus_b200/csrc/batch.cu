@@ -486,6 +486,7 @@ struct xplus_batch {
     double g_tau = 0.0;
     int g_mode = -1, g_iters = 0, g_cluster = 0, g_tpb = 0;
     bool pending = false;
+    bool have_b = false;   // d_b64 holds the (gathered) right-hand side of a solve
     double last_ms = 0.0;
     std::vector<void*> allocations;
 };
@@ -889,6 +890,7 @@ int xplus_batch_solve(xplus_batch* h, const double* b, const double* x0, double 
         else bcheck(cudaMemsetAsync(h->d_xio, 0, nb, st), "memset");
         bcheck(cudaEventRecord(h->ev0, st), "event");
         enqueue_solve(h, h->d_bio, h->d_xio, tau, tau_mode, max_iters, st);
+        h->have_b = true;
         bcheck(cudaEventRecord(h->ev1, st), "event");
         h->pending = true;
         bcheck(cudaMemcpyAsync(x_out, h->d_xio, nb, cudaMemcpyDeviceToHost, st), "D2H");
@@ -936,6 +938,7 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
         }
         bcheck(cudaEventRecord(h->ev0, st), "event");
         bcheck(cudaGraphLaunch(h->gexec, st), "graph launch");
+        h->have_b = true;
         bcheck(cudaEventRecord(h->ev1, st), "event");
         h->pending = true;
     });
@@ -967,14 +970,21 @@ int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, in
         require(h && (iters > 0 || (tau > 0.0 && tau < 1.0)), XPLUS_ERR_ARG, "bad argument");
         bcheck(cudaSetDevice(h->device), "cudaSetDevice");
         cudaStream_t st = h->stream;
-        // b = 1, x = 0 for every system; either a fixed number of iterations per system (an
+        // x = 0 for every system; either a fixed number of iterations per system on b = 1 (an
         // absolute tolerance no system reaches, so every shape does the same work), or every
-        // system solved to the FP64 true relative residual tau (the makespan that matters)
+        // system solved to the FP64 true relative residual tau (the makespan that matters), on
+        // the right-hand side of the last solve when there was one (b = 1 otherwise): how fast
+        // each system converges depends on b, and so does the best shape
         const bool fixed = iters > 0;
-        std::vector<double> ones(static_cast<size_t>(h->rows), 0.0);
+        const bool last_b = !fixed && h->have_b;
+        std::vector<double> ones(static_cast<size_t>(h->rows), 0.0), saved;
         std::vector<int> map(static_cast<size_t>(h->rows));
         bcheck(cudaMemcpy(map.data(), h->d_map, map.size() * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
         for (size_t i = 0; i < map.size(); ++i) ones[i] = map[i] >= 0 ? 1.0 : 0.0;
+        if (last_b) {
+            bcheck(cudaStreamSynchronize(st), "sync");
+            bcheck(cudaMemcpy(ones.data(), h->d_b64, ones.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        }
         double best = 1e300;
         int bc = h->cluster, bt = h->tpb;
         const int clusters[4] = {1, 2, 4, 8};

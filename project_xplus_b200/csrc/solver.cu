@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <vector>
 
 #include "common.hpp"
@@ -70,6 +71,7 @@ struct xplus_pcg {
     long long phase_ns[4] = {0, 0, 0, 0};
     std::vector<void*> allocations;
     std::vector<int> perm;     // SELL row -> original row
+    bool l2_user = false;      // raised the persisting-L2 limit (restored when the last such handle goes)
     // M^-1 = G^T G: G on A's lower pattern (original order), SELL images of G and G^T in the
     // matrix's SELL order, and the map from each SELL slot to its entry of g_low
     bool gtg = false;
@@ -149,10 +151,22 @@ double f16_scale(const std::vector<double>& v) {
     return std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(m))) - 15);
 }
 
+// Handles that raised the process's persisting-L2 limit, and the limit before the first did:
+// the last one to go restores it.
+std::mutex g_l2_mutex;
+int g_l2_users = 0;
+size_t g_l2_limit_before = 0;
+
 void destroy(xplus_pcg* h) {
     if (!h) return;
     if (h->device >= 0) cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->l2_user) {
+        // the matrix's lines stay persisting in L2 until reset: hand the cache back
+        cudaCtxResetPersistingL2Cache();
+        std::lock_guard<std::mutex> lk(g_l2_mutex);
+        if (--g_l2_users == 0) cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_limit_before);
+    }
     for (void* p : h->allocations) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -243,9 +257,15 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
             cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, o.device), "attr");
             const size_t bytes = std::min(col_bytes + val_bytes, static_cast<size_t>(max_window));
             size_t limit = 0;
-            cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
             const size_t want = std::min(bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
-            if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
+            {
+                std::lock_guard<std::mutex> lk(g_l2_mutex);
+                cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+                if (g_l2_users == 0) g_l2_limit_before = limit;
+                if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
+                ++g_l2_users;
+                h->l2_user = true;
+            }
             cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
             if (bytes > 0 && limit > 0) {
                 h->window.base_ptr = mat;

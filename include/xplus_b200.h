@@ -170,7 +170,8 @@ int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);
 /* Phase clock of the last solve, read from block 0's %globaltimer (ms, summed over the
  * iterations): {phase A work, grid-barrier wait after A, phase B work, wait after B}; for the
  * one-barrier SM-resident kernel {records + dot-product partials, barrier wait and totals,
- * pending update + search-direction window refill, A p' from shared memory}. */
+ * pending update + search-direction window refill, A p' from shared memory}; for the G^T G
+ * kernel {A p', all grid-barrier waits, x/r update + t = G r', z = G^T t}. */
 int xplus_pcg_last_phase_times(xplus_pcg* h, double* ms4);
 /* The same phase clock for every CTA of the last solve: ms[4*b + k], k as above; *blocks is
  * the grid size (pass ms = NULL to query it). */

@@ -34,27 +34,23 @@ using namespace dev;
 constexpr int kGtgSlices = 1024;  // slice table capacity per CTA
 constexpr int kGChunk = 2;        // G / G^T SELL chunk (FP32 values, int32 columns)
 
-// NB rows (32 sl[k] + lane) of G or G^T in SELL form times x (sl[k] < 0: no row).  With RECOMP
-// the operand is r'_j = fma(-alpha, Ap'_j, r_j), recomputed exactly as the owner of row j
+// NB rows (32 sl[k] + lane) of G or G^T in SELL form times x (sl[k] < 0: no row); st is the
+// CTA's shared slice table {first slot, width} starting at slice s_first.  With RECOMP the
+// operand is r'_j = fma(-alpha, Ap'_j, r_j), recomputed exactly as the owner of row j
 // computes it.  The slot loads of all
 // rows are issued first, then all the gathers, then the arithmetic, so a warp keeps
 // NB * 2 * kGChunk loads in flight instead of walking its slices one dependent chain at a time.
 template <int NB, bool RECOMP>
-__device__ __forceinline__ void g_rows(const long long* __restrict__ sp, const int* __restrict__ col,
+__device__ __forceinline__ void g_rows(const int2* __restrict__ st, int s_first, const int* __restrict__ col,
                                        const float* __restrict__ val, const int (&sl)[NB], int lane, const float* x,
                                        const float* ap, float nal, float (&out)[NB]) {
-    long long base[NB];
-    int w[NB], wmax = 0;
+    int base[NB], w[NB], wmax = 0;
 #pragma unroll
     for (int k = 0; k < NB; ++k) {
         out[k] = 0.0f;
-        if (sl[k] >= 0) {
-            base[k] = sp[sl[k]];
-            w[k] = static_cast<int>((sp[sl[k] + 1] - base[k]) >> 5);
-        } else {
-            base[k] = 0;
-            w[k] = 0;
-        }
+        const int2 e = sl[k] >= 0 ? st[sl[k] - s_first] : make_int2(0, 0);
+        base[k] = e.x;
+        w[k] = e.y;
         wmax = max(wmax, w[k]);
     }
     for (int c = 0; c < wmax; c += kGChunk) {
@@ -63,7 +59,7 @@ __device__ __forceinline__ void g_rows(const long long* __restrict__ sp, const i
 #pragma unroll
         for (int k = 0; k < NB; ++k) {
             if (c < w[k]) {
-                const long long off = base[k] + static_cast<long long>(c) * 32 + lane * kGChunk;
+                const int off = base[k] + c * 32 + lane * kGChunk;
                 v[k] = __ldg(reinterpret_cast<const float2*>(val + off));
                 cc[k] = __ldg(reinterpret_cast<const int2*>(col + off));
             } else {
@@ -98,6 +94,9 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     __shared__ double s_tot[4];
     __shared__ int s_flag;
     __shared__ int2 s_slice[kGtgSlices];
+    __shared__ int2 s_gslice[kGtgSlices];   // G and G^T slice tables {first slot, width}
+    __shared__ int2 s_gtslice[kGtgSlices];
+    __shared__ long long s_clk[6];
     GridBarrier bar{a.bar, a.err, a.timeout_ns, 0u, a.debug_skip_block};
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -120,9 +119,25 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     for (int k = threadIdx.x; k < se - sb; k += blockDim.x) {
         const long long b0 = a.slice_ptr[sb + k];
         s_slice[k] = make_int2(static_cast<int>(b0), static_cast<int>((a.slice_ptr[sb + k + 1] - b0) >> 5));
+        const long long g0 = a.g_slice_ptr[sb + k];
+        s_gslice[k] = make_int2(static_cast<int>(g0), static_cast<int>((a.g_slice_ptr[sb + k + 1] - g0) >> 5));
+        const long long t0 = a.gt_slice_ptr[sb + k];
+        s_gtslice[k] = make_int2(static_cast<int>(t0), static_cast<int>((a.gt_slice_ptr[sb + k + 1] - t0) >> 5));
     }
-    if (lead) a.out->t_start_ns = globaltimer_ns();
+    // phase clock (per CTA, thread 0): {A work, grid-barrier waits, BC work, D work}
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 5; ++k) s_clk[k] = 0;
+        s_clk[5] = globaltimer_ns();
+        if (lead) a.out->t_start_ns = s_clk[5];
+    }
     __syncthreads();
+    auto clock = [&](int slot) {
+        if (threadIdx.x == 0) {
+            const long long t = globaltimer_ns();
+            s_clk[slot] += t - s_clk[5];
+            s_clk[5] = t;
+        }
+    };
     int bank = 0;
     auto next_bank = [&]() {
         double* b = a.partial + static_cast<size_t>(bank) * 4 * gridDim.x;
@@ -169,7 +184,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 sl[k] = s < se ? s : -1;
                 rv[k] = s < se ? r_cur[s * 32 + lane] : 0.0f;
             }
-            g_rows<kGRows, false>(a.gt_slice_ptr, a.gt_col, gtval, sl, lane, t, nullptr, 0.0f, zv);
+            g_rows<kGRows, false>(s_gtslice, sb, a.gt_col, gtval, sl, lane, t, nullptr, 0.0f, zv);
 #pragma unroll
             for (int k = 0; k < kGRows; ++k) {
                 if (sl[k] < 0) continue;
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 float tv[kGRows];
 #pragma unroll
                 for (int k = 0; k < kGRows; ++k) sl[k] = s0 + k * wpb < se ? s0 + k * wpb : -1;
-                g_rows<kGRows, false>(a.g_slice_ptr, a.g_col, gval, sl, lane, r_cur, nullptr, 0.0f, tv);
+                g_rows<kGRows, false>(s_gslice, sb, a.g_col, gval, sl, lane, r_cur, nullptr, 0.0f, tv);
 #pragma unroll
                 for (int k = 0; k < kGRows; ++k)
                     if (sl[k] >= 0) t[sl[k] * 32 + lane] = tv[k];
@@ -257,7 +272,9 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 cur_bank = next_bank();
                 publish<1>(acc, s_red, cur_bank);
             }
+            clock(0);
             if (!bar.sync(&s_flag)) return;
+            clock(1);
             grid_totals(cur_bank, 1, s_tot);
             pap = s_tot[0];
             if (bad(pap) || fabs(pap) <= kBreakdownEps) {
@@ -309,7 +326,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                     }
                     if (!jac) {
                         float tv[kGRows];
-                        g_rows<kGRows, true>(a.g_slice_ptr, a.g_col, gval, sl, lane, r_cur, ap, nal, tv);
+                        g_rows<kGRows, true>(s_gslice, sb, a.g_col, gval, sl, lane, r_cur, ap, nal, tv);
 #pragma unroll
                         for (int k = 0; k < kGRows; ++k)
                             if (sl[k] >= 0) t[sl[k] * 32 + lane] = tv[k];
@@ -318,7 +335,9 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 cur_bank = next_bank();
                 publish<2>(acc, s_red, cur_bank);
             }
+            clock(2);
             if (!bar.sync(&s_flag)) return;
+            clock(1);
             grid_totals(cur_bank, 2, s_tot);
             rz_new = s_tot[0];
             rr_new = s_tot[1];
@@ -330,7 +349,9 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             if (!jac) {
                 // ---- D: z = G^T t, r'.z ----
                 z_phase();
+                clock(3);
                 if (!bar.sync(&s_flag)) return;
+                clock(1);
                 grid_totals(cur_bank, 1, s_tot);
                 rz_new = s_tot[0];
             }
@@ -417,6 +438,8 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
         cur_bank = next_bank();
         publish<1>(acc, s_red, cur_bank);
     }
+    if (threadIdx.x == 0 && a.block_clk)
+        for (int k = 0; k < 4; ++k) a.block_clk[4 * static_cast<size_t>(blockIdx.x) + k] = s_clk[k];
     if (!bar.sync(&s_flag)) return;
     if (blockIdx.x == 0) {
         grid_totals(cur_bank, 1, s_tot);
@@ -433,6 +456,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             o->true_rr = s_tot[0];
             o->reserved = static_cast<double>(fell_back);
             o->t_end_ns = globaltimer_ns();
+            for (int k = 0; k < 4; ++k) o->t_phase[k] = s_clk[k];
         }
     }
 }

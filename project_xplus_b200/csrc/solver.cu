@@ -562,6 +562,7 @@ void gtg_layout(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
     std::vector<int> col, map, tcol, tmap;
     gtg_sell(g, h->n_pad, sp, col, map);
     gtg_sell(gt, h->n_pad, tsp, tcol, tmap);
+    require(col.size() < (1ULL << 31) && tcol.size() < (1ULL << 31), XPLUS_ERR_ARG, "G too large (2^31 slots)");
     h->g_slots = static_cast<int64_t>(col.size());
     h->gt_slots = static_cast<int64_t>(tcol.size());
     cudaStream_t st = h->stream;
@@ -587,8 +588,9 @@ void gtg_layout(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
     int gtg_tpb = 0;
     cuda_check(gtg_grid(h->key, h->device, h->n_slices, &h->gtg_grid, &gtg_tpb), "gtg grid");
     if (h->gtg_grid > h->grid) {
-        // partial sums are sized by the grid
+        // partial sums and the per-CTA clock are sized by the grid
         h->d_partial = dalloc<double>(h, static_cast<size_t>(16) * h->gtg_grid);
+        h->d_block_clk = dalloc<long long>(h, static_cast<size_t>(4) * h->gtg_grid);
     }
     cuda_check(cudaStreamSynchronize(st), "sync");
 }
@@ -744,10 +746,11 @@ int xplus_pcg_last_block_times(xplus_pcg* h, double* ms, int max_blocks, int* bl
     return guarded([&] {
         require(h && blocks, XPLUS_ERR_ARG, "null argument");
         collect(h, nullptr);
-        *blocks = h->grid;
+        const int grid = h->gtg ? h->gtg_grid : h->grid;
+        *blocks = grid;
         if (!ms) return;
-        const int nb = std::min(max_blocks, h->grid);
-        std::vector<long long> t(static_cast<size_t>(4) * h->grid);
+        const int nb = std::min(max_blocks, grid);
+        std::vector<long long> t(static_cast<size_t>(4) * grid);
         cuda_check(cudaMemcpy(t.data(), h->d_block_clk, t.size() * sizeof(long long), cudaMemcpyDeviceToHost), "D2H");
         for (int k = 0; k < 4 * nb; ++k) ms[k] = static_cast<double>(t[static_cast<size_t>(k)]) * 1e-6;
     });

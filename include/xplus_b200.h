@@ -116,6 +116,9 @@ typedef struct xplus_opts {
                               the best ||b - A x|| by this fraction (default 0.05) ... */
     int stagnation_window; /* ... and this many replacements in a row without progress stop the
                               solve (status XPLUS_MAX_ITER, metrics.reserved[0] = 1; default 8) */
+    int build_on_gpu;      /* xplus_pcg_create builds the SELL-C-sigma layout on the GPU (the
+                              same arrays as the host builder, bit for bit; default 1, sigma <=
+                              4096); 0 builds it on the host */
 } xplus_opts;
 
 typedef struct xplus_metrics {

@@ -75,5 +75,8 @@ inline void stagnation_args(const xplus_opts& o, double* factor, int* window) {
 // SELL-C-sigma builder (the single implementation behind xplus_sell_build).
 void sell_build(int n, const int* row_ptr, const int* col_idx, const double* values, int C,
                 int sigma, int chunk, int diag_split, SellHost& out);
+// The same layout built on the current GPU (sell_gpu.cu, bit-identical) and copied back.
+void sell_build_via_gpu(int n, const int* row_ptr, const int* col_idx, const double* values, int C,
+                        int sigma, int chunk, int diag_split, SellHost& out);
 
 }  // namespace xplus

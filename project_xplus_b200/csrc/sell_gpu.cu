@@ -35,6 +35,22 @@ __global__ void k_lengths(const int* __restrict__ rp, const int* __restrict__ ci
     len[i] = l;
 }
 
+// CSR structure checks before anything is indexed: row_ptr[0] == 0, non-decreasing, and every
+// column in [0, n).  Sets *bad (the caller zeroes it) instead of reading out of bounds.
+__global__ void k_check_rows(const int* __restrict__ rp, int n, int* __restrict__ bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && rp[0] != 0) atomicOr(bad, 1);
+    if (i < n && rp[i + 1] < rp[i]) atomicOr(bad, 1);
+}
+
+__global__ void k_check_cols(const int* __restrict__ ci, long long nnz, int n, int* __restrict__ bad) {
+    const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < nnz) {
+        const int c = ci[k];
+        if (c < 0 || c >= n) atomicOr(bad, 2);
+    }
+}
+
 // one CTA per window of sigma rows
 __global__ void k_sigma_rank(const int* __restrict__ len, int n, int sigma, int* __restrict__ perm) {
     __shared__ int s_len[kMaxSigmaGpu];
@@ -174,6 +190,24 @@ void sell_build_device(int n, const int* d_rp, const int* d_ci, const double* d_
     int* width = d_slice_width ? d_slice_width : tmp.get<int>(static_cast<size_t>(ns));
     long long* ptr = d_slice_ptr ? reinterpret_cast<long long*>(d_slice_ptr) : tmp.get<long long>(static_cast<size_t>(ns) + 1);
     const int tb = 256;
+    {
+        int* bad = tmp.get<int>(1);
+        int h_bad = 0, h_nnz = 0;
+        ck(cudaMemsetAsync(bad, 0, sizeof(int), st), "memset");
+        k_check_rows<<<(n + tb - 1) / tb, tb, 0, st>>>(d_rp, n, bad);
+        ck(cudaGetLastError(), "sell check");
+        ck(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(&h_nnz, d_rp + n, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaStreamSynchronize(st), "sync");
+        require(h_bad == 0, XPLUS_ERR_DATA, "row_ptr must start at 0 and be non-decreasing");
+        if (h_nnz > 0) {
+            k_check_cols<<<static_cast<unsigned>((static_cast<long long>(h_nnz) + tb - 1) / tb), tb, 0, st>>>(d_ci, h_nnz, n, bad);
+            ck(cudaGetLastError(), "sell check");
+            ck(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+            ck(cudaStreamSynchronize(st), "sync");
+            require(h_bad == 0, XPLUS_ERR_DATA, "column index out of range");
+        }
+    }
     k_lengths<<<(n + tb - 1) / tb, tb, 0, st>>>(d_rp, d_ci, n, diag_split ? 1 : 0, len);
     ck(cudaGetLastError(), "sell lengths");
     if (sigma > 1)
@@ -207,6 +241,63 @@ void sell_build_device(int n, const int* d_rp, const int* d_ci, const double* d_
 }
 
 }  // namespace
+
+void sell_build_via_gpu(int n, const int* row_ptr, const int* col_idx, const double* values, int C, int sigma,
+                        int chunk, int diag_split, SellHost& S) {
+    const int64_t nnz = row_ptr[n];
+    cudaStream_t st = nullptr;
+    ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+    try {
+        DevTmp tmp;
+        int* rp = tmp.get<int>(static_cast<size_t>(n) + 1);
+        int* ci = tmp.get<int>(static_cast<size_t>(nnz));
+        double* v = tmp.get<double>(static_cast<size_t>(nnz));
+        ck(cudaMemcpyAsync(rp, row_ptr, (static_cast<size_t>(n) + 1) * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+        ck(cudaMemcpyAsync(ci, col_idx, static_cast<size_t>(nnz) * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+        ck(cudaMemcpyAsync(v, values, static_cast<size_t>(nnz) * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+        int ns = 0;
+        int64_t slots = 0;
+        sell_build_device(n, rp, ci, v, C, sigma, chunk, diag_split, &ns, &slots, nullptr, nullptr, nullptr, nullptr,
+                          nullptr, nullptr, st);
+        int* perm = tmp.get<int>(static_cast<size_t>(n));
+        int64_t* sp = tmp.get<int64_t>(static_cast<size_t>(ns) + 1);
+        int* sw = tmp.get<int>(static_cast<size_t>(ns));
+        int* col = tmp.get<int>(static_cast<size_t>(slots));
+        double* val = tmp.get<double>(static_cast<size_t>(slots));
+        double* dg = diag_split ? tmp.get<double>(static_cast<size_t>(n)) : nullptr;
+        sell_build_device(n, rp, ci, v, C, sigma, chunk, diag_split, &ns, &slots, perm, sp, sw, col, val, dg, st);
+        S.n = n;
+        S.C = C;
+        S.sigma = sigma;
+        S.chunk = chunk;
+        S.diag_split = diag_split;
+        S.n_slices = ns;
+        S.n_pad = ns * C;
+        S.slots = slots;
+        S.perm.resize(static_cast<size_t>(n));
+        S.slice_ptr.resize(static_cast<size_t>(ns) + 1);
+        S.slice_width.resize(static_cast<size_t>(ns));
+        S.col.resize(static_cast<size_t>(slots));
+        S.val.resize(static_cast<size_t>(slots));
+        ck(cudaMemcpyAsync(S.perm.data(), perm, S.perm.size() * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(S.slice_ptr.data(), sp, S.slice_ptr.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(S.slice_width.data(), sw, S.slice_width.size() * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(S.col.data(), col, S.col.size() * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(S.val.data(), val, S.val.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        if (diag_split) {
+            S.diag.assign(static_cast<size_t>(S.n_pad), 0.0);
+            ck(cudaMemcpyAsync(S.diag.data(), dg, static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        }
+        ck(cudaStreamSynchronize(st), "sync");
+        S.iperm.resize(static_cast<size_t>(n));
+        for (int i = 0; i < n; ++i) S.iperm[static_cast<size_t>(S.perm[static_cast<size_t>(i)])] = i;
+    } catch (...) {
+        cudaStreamDestroy(st);
+        throw;
+    }
+    cudaStreamDestroy(st);
+}
+
 }  // namespace xplus
 
 extern "C" int xplus_sell_build_device(int n, const int* d_row_ptr, const int* d_col_idx, const double* d_values,

@@ -206,7 +206,10 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     require((o.value_type != XPLUS_BF16 && o.value_type != XPLUS_F16) || split, XPLUS_ERR_ARG,
             "16-bit values need row_sum_form");
     SellHost S;
-    sell_build(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+    if (o.build_on_gpu && o.sigma <= 4096)
+        sell_build_via_gpu(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+    else
+        sell_build(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
 
     auto* h = new xplus_pcg();
     h->device = o.device;
@@ -637,6 +640,7 @@ void xplus_opts_default(xplus_opts* o) {
     o->restart_on_replace = -1;
     o->stagnation_gain = 0.05;
     o->stagnation_window = 8;
+    o->build_on_gpu = 1;
 }
 
 int xplus_device_count(void) {

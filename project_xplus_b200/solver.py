@@ -167,7 +167,8 @@ class PcgSolver:
                  sigma=256, chunk=4, keep_fp64=True, replace_every=0, replace_drop=1e-2,
                  block_threads=0, blocks_per_sm=0, barrier_timeout_s=2.0, device=0,
                  row_sum_form=True, index16=True, l2_persist=True, resident=True,
-                 barriers_per_iter=1, restart_on_replace=-1, stagnation_gain=0.05, stagnation_window=8):
+                 barriers_per_iter=1, restart_on_replace=-1, stagnation_gain=0.05, stagnation_window=8,
+                 build_on_gpu=True):
         self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
         self.col_idx = np.ascontiguousarray(col_idx, np.int32)
         self.values = np.ascontiguousarray(values, np.float64)
@@ -179,7 +180,7 @@ class PcgSolver:
             barrier_timeout_s=barrier_timeout_s, device=device, row_sum_form=int(row_sum_form), index16=int(index16),
             l2_persist=int(l2_persist), resident=int(resident), barriers_per_iter=int(barriers_per_iter),
             restart_on_replace=int(restart_on_replace), stagnation_gain=float(stagnation_gain),
-            stagnation_window=int(stagnation_window))
+            stagnation_window=int(stagnation_window), build_on_gpu=int(build_on_gpu))
         h = C.c_void_p()
         check(lib.xplus_pcg_create(ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), self.n,
                                    C.byref(self.opts), C.byref(h)))

@@ -357,3 +357,38 @@ def test_max_iters_one_and_exact_start(gpu, sys0):
     assert r.status == "max_iter" and r.iterations == 1
     r0 = s.solve(d.b, xt, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE)
     assert r0.converged and r0.iterations == 0
+
+
+def test_create_with_gpu_and_host_builders_agree(gpu):
+    """xplus_pcg_create builds the layout on the GPU by default; the host builder gives the
+    same handle: identical solves, bit for bit."""
+    d, _ = g.fem2d(90, sigma=2.0, perm_seed=2, rcm=True)
+    out = []
+    for gpu_build in (True, False):
+        s = xp.PcgSolver.from_dataset(d, build_on_gpu=gpu_build)
+        r = s.solve(d.b, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE, trace=True)
+        out.append((r.iterations, r.solution.copy(), [t.residual for t in r.iteration_trace]))
+        s.close()
+    assert out[0][0] == out[1][0]
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+def test_gpu_builder_rejects_bad_csr(gpu):
+    """Invalid device CSR is refused with XPLUS_ERR_DATA before any indexing."""
+    import torch
+    n = 4
+    rp = torch.tensor([0, 2, 1, 3, 4], dtype=torch.int32, device="cuda")   # decreasing
+    ci = torch.tensor([0, 1, 2, 3], dtype=torch.int32, device="cuda")
+    v = torch.ones(4, dtype=torch.float64, device="cuda")
+    import ctypes as C
+    from project_xplus_b200 import _lib
+    ns, slots = C.c_int(), C.c_int64()
+    rc = _lib.lib.xplus_sell_build_device(n, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), 32, 1, 1, 0,
+                                          C.byref(ns), C.byref(slots), None, None, None, None, None, None, None)
+    assert rc == _lib.XPLUS_ERR_DATA
+    rp2 = torch.tensor([0, 1, 2, 3, 4], dtype=torch.int32, device="cuda")
+    ci2 = torch.tensor([0, 1, 7, 3], dtype=torch.int32, device="cuda")    # column out of range
+    rc = _lib.lib.xplus_sell_build_device(n, rp2.data_ptr(), ci2.data_ptr(), v.data_ptr(), 32, 1, 1, 0,
+                                          C.byref(ns), C.byref(slots), None, None, None, None, None, None, None)
+    assert rc == _lib.XPLUS_ERR_DATA

@@ -1,10 +1,12 @@
 // common.hpp -- error reporting and small helpers shared by the host and CUDA sources.
 #pragma once
+#include <algorithm>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/xplus_b200.h"
@@ -42,6 +44,14 @@ int guarded(F&& f) {
 inline void require(bool cond, int code, const std::string& msg) {
     if (!cond) throw Error(code, msg);
 }
+// The same for a literal message: no string is built unless the check fails (hot host loops).
+inline void require(bool cond, int code, const char* msg) {
+    if (!cond) throw Error(code, std::string(msg));
+}
+
+// Runs f(begin, end) over [0, count) in contiguous chunks on the host's threads (at most 32).
+template <typename F>
+void parallel_for(int64_t count, F&& f);
 
 // CSR structure checks of src/CsrDataset.hpp:29-52, same messages.
 void validate_csr(int n, const int* row_ptr, const int* col_idx, int64_t nnz_expected);
@@ -78,5 +88,21 @@ void sell_build(int n, const int* row_ptr, const int* col_idx, const double* val
 // The same layout built on the current GPU (sell_gpu.cu, bit-identical) and copied back.
 void sell_build_via_gpu(int n, const int* row_ptr, const int* col_idx, const double* values, int C,
                         int sigma, int chunk, int diag_split, SellHost& out);
+
+template <typename F>
+void parallel_for(int64_t count, F&& f) {
+    const int nt = static_cast<int>(std::max<unsigned>(1u, std::min(32u, std::thread::hardware_concurrency())));
+    if (count < 65536 || nt == 1) {
+        f(int64_t{0}, count);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const int64_t per = (count + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+        const int64_t b = t * per, e = std::min(count, b + per);
+        if (b < e) pool.emplace_back([&f, b, e] { f(b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
 
 }  // namespace xplus

@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "common.hpp"
@@ -480,77 +481,124 @@ ParamOffsets param_offsets() {
 // ---------------------------------------------------------------------------------------
 // Host: graph construction (the single builder for training and for the solver's inference)
 // ---------------------------------------------------------------------------------------
+// Runs f(begin, end) over [0, count) split into contiguous chunks on the host's threads.
+template <typename F>
+static void parallel_rows(int count, F&& f) {
+    const int nt = std::max(1, std::min(32, static_cast<int>(std::thread::hardware_concurrency())));
+    if (count < 4096 || nt == 1) {
+        f(0, count);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const int per = (count + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+        const int b = t * per, e = std::min(count, b + per);
+        if (b < e) pool.emplace_back([&f, b, e] { f(b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
+
 void HostGraph::build(int n_, const int* row_ptr, const int* col_idx, const double* values) {
     n = n_;
-    std::vector<double> d(static_cast<size_t>(n), 0.0), rowabs(static_cast<size_t>(n), 0.0);
-    for (int i = 0; i < n; ++i)
-        for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
-            rowabs[static_cast<size_t>(i)] += std::fabs(values[q]);
-            if (col_idx[q] == i) d[static_cast<size_t>(i)] += values[q];
+    const size_t N = static_cast<size_t>(n);
+    std::vector<double> d(N, 0.0), rowabs(N, 0.0), logd(N, 0.0);
+    std::vector<int> adj_cnt(N, 0), low_cnt(N, 0), glow_cnt(N, 0);
+    std::vector<unsigned char> dup(N, 0);
+    // pass 1 (rows in parallel): diagonal, row abs-sum, how many entries each output takes
+    parallel_rows(n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            int diag_seen = 0;
+            for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
+                const int j = col_idx[q];
+                rowabs[static_cast<size_t>(i)] += std::fabs(values[q]);
+                if (j == i) {
+                    d[static_cast<size_t>(i)] += values[q];
+                    ++diag_seen;
+                } else {
+                    ++adj_cnt[static_cast<size_t>(i)];
+                    if (j < i) ++low_cnt[static_cast<size_t>(i)];
+                }
+                if (j <= i) ++glow_cnt[static_cast<size_t>(i)];
+            }
+            dup[static_cast<size_t>(i)] = diag_seen > 1;
+            logd[static_cast<size_t>(i)] = d[static_cast<size_t>(i)] > 0.0 ? std::log(d[static_cast<size_t>(i)]) : 0.0;
         }
-    for (int i = 0; i < n; ++i)
+    });
+    for (int i = 0; i < n; ++i) {
         require(d[static_cast<size_t>(i)] > 0.0, XPLUS_ERR_DATA, "learned preconditioner needs a positive diagonal");
+        require(!dup[static_cast<size_t>(i)], XPLUS_ERR_DATA, "duplicate diagonal entry");
+    }
     double mean_ld = 0.0;
-    for (double v : d) mean_ld += std::log(v);
+    for (double v : logd) mean_ld += v;
     mean_ld /= n;
-    x.resize(static_cast<size_t>(n) * 2);
-    isq.resize(static_cast<size_t>(n));
+    adj_ptr.assign(N + 1, 0);
+    low_ptr.assign(N + 1, 0);
+    std::vector<int> glow_ptr(N + 1, 0);
     for (int i = 0; i < n; ++i) {
-        x[2 * static_cast<size_t>(i)] = static_cast<float>(std::log(d[static_cast<size_t>(i)]) - mean_ld);
-        x[2 * static_cast<size_t>(i) + 1] = static_cast<float>(rowabs[static_cast<size_t>(i)] / d[static_cast<size_t>(i)] - 1.0);
-        isq[static_cast<size_t>(i)] = static_cast<float>(1.0 / std::sqrt(d[static_cast<size_t>(i)]));
+        adj_ptr[static_cast<size_t>(i) + 1] = adj_ptr[static_cast<size_t>(i)] + adj_cnt[static_cast<size_t>(i)];
+        low_ptr[static_cast<size_t>(i) + 1] = low_ptr[static_cast<size_t>(i)] + low_cnt[static_cast<size_t>(i)];
+        glow_ptr[static_cast<size_t>(i) + 1] = glow_ptr[static_cast<size_t>(i)] + glow_cnt[static_cast<size_t>(i)];
     }
-    adj_ptr.assign(static_cast<size_t>(n) + 1, 0);
-    low_ptr.assign(static_cast<size_t>(n) + 1, 0);
+    n_adj = adj_ptr[N];
+    n_low = low_ptr[N];
+    n_glow = glow_ptr[N];
+    const int64_t nnz = row_ptr[n];
+    x.resize(N * 2);
+    isq.resize(N);
+    adj_col.resize(static_cast<size_t>(n_adj));
+    adj_e.resize(static_cast<size_t>(n_adj));
+    low_col.resize(static_cast<size_t>(n_low));
+    low_row.resize(static_cast<size_t>(n_low));
+    low_e.resize(static_cast<size_t>(n_low));
+    pos_low.assign(static_cast<size_t>(n_low), -1);
+    pos_diag.assign(N, -1);
     a_ptr.assign(row_ptr, row_ptr + n + 1);
-    a_col.assign(col_idx, col_idx + row_ptr[n]);
-    a_val.resize(static_cast<size_t>(row_ptr[n]));
-    for (int q = 0; q < row_ptr[n]; ++q) a_val[static_cast<size_t>(q)] = static_cast<float>(values[q]);
-    adj_col.clear(); adj_e.clear(); low_col.clear(); low_row.clear(); low_e.clear(); pos_low.clear();
-    pos_diag.assign(static_cast<size_t>(n), -1);
-    n_glow = 0;
-    for (int i = 0; i < n; ++i) {
-        // columns of row i in ascending order (stable for equal columns); kq[q - row_ptr[i]] is
-        // the lower-edge index of CSR entry q (-1 for the diagonal and the upper entries)
-        const int len = row_ptr[i + 1] - row_ptr[i];
-        std::vector<int> idx(static_cast<size_t>(len)), kq(static_cast<size_t>(len), -1);
-        std::iota(idx.begin(), idx.end(), row_ptr[i]);
-        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return col_idx[a] < col_idx[b]; });
-        for (int q : idx) {
-            const int j = col_idx[q];
-            if (j == i) continue;
-            const float e = static_cast<float>(values[q] / std::sqrt(d[static_cast<size_t>(i)] * d[static_cast<size_t>(j)]));
-            adj_col.push_back(j);
-            adj_e.push_back(e);
-            if (j < i) {
-                kq[static_cast<size_t>(q - row_ptr[i])] = static_cast<int>(low_col.size());
-                low_col.push_back(j);
-                low_row.push_back(i);
-                low_e.push_back(e);
+    a_col.assign(col_idx, col_idx + nnz);
+    a_val.resize(static_cast<size_t>(nnz));
+    // pass 2 (rows in parallel): every row writes its own ranges of the outputs
+    parallel_rows(n, [&](int b, int e) {
+        std::vector<int> idx, kq;
+        for (int i = b; i < e; ++i) {
+            const size_t I = static_cast<size_t>(i);
+            x[2 * I] = static_cast<float>(logd[I] - mean_ld);
+            x[2 * I + 1] = static_cast<float>(rowabs[I] / d[I] - 1.0);
+            isq[I] = static_cast<float>(1.0 / std::sqrt(d[I]));
+            for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) a_val[static_cast<size_t>(q)] = static_cast<float>(values[q]);
+            // columns of row i in ascending order (stable for equal columns); kq[q - row_ptr[i]]
+            // is the lower-edge index of CSR entry q (-1 for the diagonal and the upper entries)
+            const int len = row_ptr[i + 1] - row_ptr[i];
+            idx.resize(static_cast<size_t>(len));
+            kq.assign(static_cast<size_t>(len), -1);
+            std::iota(idx.begin(), idx.end(), row_ptr[i]);
+            std::stable_sort(idx.begin(), idx.end(), [&](int a2, int b2) { return col_idx[a2] < col_idx[b2]; });
+            int wa = adj_ptr[I], wl = low_ptr[I];
+            for (int q : idx) {
+                const int j = col_idx[q];
+                if (j == i) continue;
+                const float ev = static_cast<float>(values[q] / std::sqrt(d[I] * d[static_cast<size_t>(j)]));
+                adj_col[static_cast<size_t>(wa)] = j;
+                adj_e[static_cast<size_t>(wa)] = ev;
+                ++wa;
+                if (j < i) {
+                    kq[static_cast<size_t>(q - row_ptr[i])] = wl;
+                    low_col[static_cast<size_t>(wl)] = j;
+                    low_row[static_cast<size_t>(wl)] = i;
+                    low_e[static_cast<size_t>(wl)] = ev;
+                    ++wl;
+                }
+            }
+            // positions of this row's G entries in A's CSR order of the entries with col <= row
+            int g = glow_ptr[I];
+            for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
+                const int j = col_idx[q];
+                if (j > i) continue;
+                if (j == i) pos_diag[I] = g++;
+                else pos_low[static_cast<size_t>(kq[static_cast<size_t>(q - row_ptr[i])])] = g++;
             }
         }
-        adj_ptr[static_cast<size_t>(i) + 1] = static_cast<int>(adj_col.size());
-        low_ptr[static_cast<size_t>(i) + 1] = static_cast<int>(low_col.size());
-        pos_low.resize(low_col.size(), -1);
-        // positions of this row's G entries in A's CSR order of the entries with col <= row
-        bool diag_seen = false;
-        for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
-            const int j = col_idx[q];
-            if (j > i) continue;
-            if (j == i) {
-                require(!diag_seen, XPLUS_ERR_DATA, "duplicate diagonal entry");
-                diag_seen = true;
-                pos_diag[static_cast<size_t>(i)] = n_glow++;
-            } else {
-                pos_low[static_cast<size_t>(kq[static_cast<size_t>(q - row_ptr[i])])] = n_glow++;
-            }
-        }
-    }
-    pos_low.resize(low_col.size(), -1);
-    n_low = static_cast<int>(low_col.size());
-    n_adj = static_cast<int>(adj_col.size());
+    });
     // lower edges grouped by column: up(j) = {k : low_col[k] == j}, by increasing row
-    up_ptr.assign(static_cast<size_t>(n) + 1, 0);
+    up_ptr.assign(N + 1, 0);
     for (int k = 0; k < n_low; ++k) ++up_ptr[static_cast<size_t>(low_col[static_cast<size_t>(k)]) + 1];
     for (int i = 0; i < n; ++i) up_ptr[static_cast<size_t>(i) + 1] += up_ptr[static_cast<size_t>(i)];
     up_k.assign(static_cast<size_t>(n_low), 0);

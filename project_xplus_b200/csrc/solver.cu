@@ -233,18 +233,27 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         std::vector<short> col16;
         if (idx16) {
             col16.resize(static_cast<size_t>(S.slots));
-            for (int sl = 0; sl < S.n_slices && idx16; ++sl) {
-                const int64_t base = S.slice_ptr[static_cast<size_t>(sl)], end = S.slice_ptr[static_cast<size_t>(sl) + 1];
-                for (int64_t pos = base; pos < end; ++pos) {
-                    const int lane = static_cast<int>(((pos - base) % (32 * o.chunk)) / o.chunk);
-                    const int d = S.col[static_cast<size_t>(pos)] - (sl * 32 + lane);
-                    if (d < -32768 || d > 32767) {
-                        idx16 = false;
-                        break;
-                    }
-                    col16[static_cast<size_t>(pos)] = static_cast<short>(d);
+            // slot (j/chunk) 32 chunk + lane chunk + j%chunk of slice sl belongs to row 32 sl + lane
+            std::vector<unsigned char> far(static_cast<size_t>(S.n_slices), 0);
+            const int ch = o.chunk;
+            parallel_for(S.n_slices, [&](int64_t b, int64_t e) {
+                for (int64_t sl = b; sl < e; ++sl) {
+                    const int64_t base = S.slice_ptr[static_cast<size_t>(sl)];
+                    const int64_t groups = (S.slice_ptr[static_cast<size_t>(sl) + 1] - base) / (32 * ch);
+                    for (int64_t jg = 0; jg < groups; ++jg)
+                        for (int lane = 0; lane < 32; ++lane) {
+                            const int row = static_cast<int>(sl) * 32 + lane;
+                            const int64_t p0 = base + jg * 32 * ch + lane * ch;
+                            for (int q = 0; q < ch; ++q) {
+                                const int d = S.col[static_cast<size_t>(p0 + q)] - row;
+                                if (d < -32768 || d > 32767) far[static_cast<size_t>(sl)] = 1;
+                                col16[static_cast<size_t>(p0 + q)] = static_cast<short>(d);
+                            }
+                        }
                 }
-            }
+            });
+            for (unsigned char f : far)
+                if (f) idx16 = false;
         }
         h->key.idx16 = idx16 ? 1 : 0;
         // columns and values in one allocation, so one L2 access-policy window covers both
@@ -320,12 +329,14 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         }
         if (split) {
             std::vector<double> rs(np, 0.0);
-            for (int i = 0; i < n; ++i) {
-                const int old = S.perm[static_cast<size_t>(i)];
-                double acc = 0.0;
-                for (int k = row_ptr[old]; k < row_ptr[old + 1]; ++k) acc += values[k];
-                rs[static_cast<size_t>(i)] = acc;
-            }
+            parallel_for(n, [&](int64_t b, int64_t e) {
+                for (int64_t i = b; i < e; ++i) {
+                    const int old = S.perm[static_cast<size_t>(i)];
+                    double acc = 0.0;
+                    for (int k = row_ptr[old]; k < row_ptr[old + 1]; ++k) acc += values[k];
+                    rs[static_cast<size_t>(i)] = acc;
+                }
+            });
             std::vector<unsigned char> rb = convert(rs, o.vector_type);
             h->d_rowsum = dalloc<unsigned char>(h, np * xs);
             cuda_check(cudaMemcpyAsync(h->d_rowsum, rb.data(), rb.size(), cudaMemcpyHostToDevice, st), "H2D");

@@ -392,3 +392,49 @@ def test_gpu_builder_rejects_bad_csr(gpu):
     rc = _lib.lib.xplus_sell_build_device(n, rp2.data_ptr(), ci2.data_ptr(), v.data_ptr(), 32, 1, 1, 0,
                                           C.byref(ns), C.byref(slots), None, None, None, None, None, None, None)
     assert rc == _lib.XPLUS_ERR_DATA
+
+
+def test_control_kernel_abi_matches_golden(gpu, oracle, sys0):
+    """xplus_pcg_control, the device-pointer form of cuper_pcg_control_kernel
+    (kernels/cuper_pcg_control_kernel.cpp:972-1001): status[2] = {code, iterations} and
+    metrics[4] = {rz, rr, pAp, alpha} written on the device, x updated in place; tolerance is the
+    reference's absolute rr <= tau.  Invalid parameters give status {2, 0} and zero metrics
+    (:1078-1087)."""
+    import ctypes as C
+
+    import torch
+
+    from project_xplus_b200 import _lib
+    d, _ = sys0
+    n = d.n
+    s = xp.PcgSolver.from_dataset(d, values_dtype="f64", vector_dtype="f64")
+    dev = torch.device("cuda")
+    b = torch.from_numpy(d.b).to(dev)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    work = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(5)]  # m_inv, r, z, p, ap (unused)
+    metrics = torch.zeros(4, dtype=torch.float64, device=dev)
+    status = torch.zeros(2, dtype=torch.int32, device=dev)
+    tau = 1e-10 ** 2  # rr <= tau, the reference's test
+    torch.cuda.synchronize()
+    rc = _lib.lib.xplus_pcg_control(s.handle, b.data_ptr(), work[0].data_ptr(), x.data_ptr(), work[1].data_ptr(),
+                                    work[2].data_ptr(), work[3].data_ptr(), work[4].data_ptr(), metrics.data_ptr(),
+                                    status.data_ptr(), tau, 2000, n, None)
+    assert rc == _lib.XPLUS_OK, _lib.last_error()
+    torch.cuda.synchronize()
+    ref = oracle.golden(d, tau, 2000)
+    st = status.cpu().numpy()
+    assert st[0] == 0 and abs(int(st[1]) - ref["iterations"]) <= 1
+    met = metrics.cpu().numpy()
+    assert met[1] <= tau and met[2] > 0 and met[3] > 0      # rr converged, pAp and alpha positive
+    np.testing.assert_allclose(x.cpu().numpy(), ref["x"], rtol=0, atol=1e-8 * np.abs(ref["x"]).max())
+    # invalid n: status {2, 0}, metrics zeroed, x untouched
+    x2 = torch.zeros(n, dtype=torch.float64, device=dev)
+    metrics.fill_(7.0)
+    rc = _lib.lib.xplus_pcg_control(s.handle, b.data_ptr(), work[0].data_ptr(), x2.data_ptr(), work[1].data_ptr(),
+                                    work[2].data_ptr(), work[3].data_ptr(), work[4].data_ptr(), metrics.data_ptr(),
+                                    status.data_ptr(), tau, 2000, n + 1, None)
+    assert rc == _lib.XPLUS_OK
+    torch.cuda.synchronize()
+    assert status.cpu().tolist() == [2, 0] and metrics.cpu().tolist() == [0.0, 0.0, 0.0, 0.0]
+    assert float(x2.abs().max()) == 0.0
+    s.close()

@@ -562,6 +562,19 @@ void set_launch(xplus_batch* h, int cluster, int tpb) {
     h->grid = num * cluster;
 }
 
+// f(k) for every system k, on the host's threads (system k on thread k mod T, which balances
+// systems of mixed size); every call writes only system k's own output ranges.
+template <typename F>
+void for_each_system(int count, F&& f) {
+    const int nt = std::max(1, std::min(count, std::min(32, static_cast<int>(std::thread::hardware_concurrency()))));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&f, t, nt, count] {
+            for (int k = t; k < count; k += nt) f(k);
+        });
+    for (auto& th : pool) th.join();
+}
+
 void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_idxs,
                   const double* const* values, const int* ns, const xplus_opts* opts_in, xplus_batch** out) {
     require(nsys > 0 && row_ptrs && col_idxs && values && ns && out, XPLUS_ERR_ARG, "null argument or nsys <= 0");
@@ -645,17 +658,28 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
         require(slots < (1LL << 31) && h->total_n < (1LL << 31), XPLUS_ERR_ARG, "batch too large (2^31 slots)");
         // int16 offsets when every system's ordered bandwidth allows
         bool idx16 = o.index16 != 0;
-        for (int k = 0; k < nsys && idx16; ++k) {
-            const SellHost& s = S[static_cast<size_t>(k)];
-            for (int sl = 0; sl < s.n_slices && idx16; ++sl)
-                for (int64_t pos = s.slice_ptr[static_cast<size_t>(sl)]; pos < s.slice_ptr[static_cast<size_t>(sl) + 1]; ++pos) {
-                    const int lane = static_cast<int>(((pos - s.slice_ptr[static_cast<size_t>(sl)]) % (32 * o.chunk)) / o.chunk);
+        const int ch = o.chunk;
+        // slot (j/chunk) 32 chunk + lane chunk + j%chunk of slice sl belongs to row 32 sl + lane
+        auto for_each_slot = [ch](const SellHost& s, auto&& g) {
+            for (int sl = 0; sl < s.n_slices; ++sl) {
+                const int64_t b0 = s.slice_ptr[static_cast<size_t>(sl)];
+                const int64_t groups = (s.slice_ptr[static_cast<size_t>(sl) + 1] - b0) / (32 * ch);
+                for (int64_t jg = 0; jg < groups; ++jg)
+                    for (int lane = 0; lane < 32; ++lane)
+                        for (int q = 0; q < ch; ++q) g(sl, lane, b0 + jg * 32 * ch + lane * ch + q);
+            }
+        };
+        if (idx16) {
+            std::vector<unsigned char> far(static_cast<size_t>(nsys), 0);
+            for_each_system(nsys, [&](int k) {
+                const SellHost& s = S[static_cast<size_t>(k)];
+                for_each_slot(s, [&](int sl, int lane, int64_t pos) {
                     const int d = s.col[static_cast<size_t>(pos)] - (sl * 32 + lane);
-                    if (d < -32768 || d > 32767) {
-                        idx16 = false;
-                        break;
-                    }
-                }
+                    if (d < -32768 || d > 32767) far[static_cast<size_t>(k)] = 1;
+                });
+            });
+            for (unsigned char f : far)
+                if (f) idx16 = false;
         }
         h->idx16 = idx16;
         h->kernel = pick_kernel(o.value_type, o.chunk, idx16);
@@ -673,32 +697,32 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
         std::vector<int> map(R, -1);
         std::vector<float> scale(static_cast<size_t>(nsys), 1.0f);
         std::vector<unsigned char> vbytes(static_cast<size_t>(slots) * (o.value_type == XPLUS_F32 ? 4 : 2));
-        int64_t base = 0;
-        for (int k = 0; k < nsys; ++k) {
+        std::vector<int64_t> sys_base(static_cast<size_t>(nsys) + 1, 0);
+        for (int k = 0; k < nsys; ++k) sys_base[static_cast<size_t>(k) + 1] = sys_base[static_cast<size_t>(k)] + S[static_cast<size_t>(k)].slots;
+        const int64_t base = sys_base[static_cast<size_t>(nsys)];
+        for_each_system(nsys, [&](int k) {
             const size_t K = static_cast<size_t>(k);
             const SellHost& s = S[K];
+            const int64_t b0 = sys_base[K];
             const int r0 = slice0[K] * 32;
             for (int sl = 0; sl < s.n_slices; ++sl)
-                sp[static_cast<size_t>(slice0[K] + sl)] = base + s.slice_ptr[static_cast<size_t>(sl)];
+                sp[static_cast<size_t>(slice0[K] + sl)] = b0 + s.slice_ptr[static_cast<size_t>(sl)];
             double vmax = 0.0;
             for (double x : s.val) vmax = std::max(vmax, std::fabs(x));
             const double sc = (o.value_type == XPLUS_F16 && vmax > 0.0)
                                   ? std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(vmax))) - 15) : 1.0;
             scale[K] = static_cast<float>(sc);
-            for (int sl = 0; sl < s.n_slices; ++sl)
-                for (int64_t pos = s.slice_ptr[static_cast<size_t>(sl)]; pos < s.slice_ptr[static_cast<size_t>(sl) + 1]; ++pos) {
-                    const size_t g = static_cast<size_t>(base + pos);
-                    const int lane = static_cast<int>(((pos - s.slice_ptr[static_cast<size_t>(sl)]) % (32 * o.chunk)) / o.chunk);
-                    const int c = s.col[static_cast<size_t>(pos)];
-                    if (idx16) col16[g] = static_cast<short>(c - (sl * 32 + lane));
-                    else col32[g] = r0 + c;
-                    const double v = s.val[static_cast<size_t>(pos)];
-                    v64[g] = v;
-                    if (o.value_type == XPLUS_F32) reinterpret_cast<float*>(vbytes.data())[g] = static_cast<float>(v);
-                    else if (o.value_type == XPLUS_F16) reinterpret_cast<__half*>(vbytes.data())[g] = __double2half(v / sc);
-                    else reinterpret_cast<__nv_bfloat16*>(vbytes.data())[g] = __double2bfloat16(v);
-                }
-            base += s.slots;
+            for_each_slot(s, [&](int sl, int lane, int64_t pos) {
+                const size_t gpos = static_cast<size_t>(b0 + pos);
+                const int c = s.col[static_cast<size_t>(pos)];
+                if (idx16) col16[gpos] = static_cast<short>(c - (sl * 32 + lane));
+                else col32[gpos] = r0 + c;
+                const double v = s.val[static_cast<size_t>(pos)];
+                v64[gpos] = v;
+                if (o.value_type == XPLUS_F32) reinterpret_cast<float*>(vbytes.data())[gpos] = static_cast<float>(v);
+                else if (o.value_type == XPLUS_F16) reinterpret_cast<__half*>(vbytes.data())[gpos] = __double2half(v / sc);
+                else reinterpret_cast<__nv_bfloat16*>(vbytes.data())[gpos] = __double2bfloat16(v);
+            });
             for (int i = 0; i < s.n; ++i) {
                 const int old = s.perm[static_cast<size_t>(i)];
                 const size_t gi = static_cast<size_t>(r0 + i);
@@ -710,7 +734,7 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
                 rs[gi] = acc;
                 map[gi] = static_cast<int>(h->sys_off[K] + old);
             }
-        }
+        });
         sp[static_cast<size_t>(h->n_slices)] = base;
         // queue: largest first by nnz * sqrt(n) (PCG iterations grow like sqrt(n) on these grids)
         std::vector<int> order(static_cast<size_t>(nsys));

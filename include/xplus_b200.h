@@ -165,8 +165,10 @@ int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau,
                     int hist_len, xplus_metrics* metrics);
 
 /* Asynchronous solve on device-resident FP64 b and x (original row order), enqueued on
- * `stream` (a cudaStream_t, NULL = the handle's stream).  d_x holds x0 on entry and x on
- * exit.  Fetch the outcome with xplus_pcg_last_metrics() after synchronising. */
+ * `stream` (a cudaStream_t, NULL = the handle's stream) without waiting for the device: the
+ * relative tolerance is scaled by ||b||^2 summed inside the kernel, so b may be produced by
+ * earlier work on the same stream.  d_x holds x0 on entry and x on exit.  Fetch the outcome
+ * with xplus_pcg_last_metrics() (which waits for the solve). */
 int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double tau,
                            int tau_mode, int max_iters, void* stream);
 int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);

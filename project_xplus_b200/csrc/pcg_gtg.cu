@@ -90,7 +90,7 @@ constexpr int kGRows = 4;  // G rows of one warp in flight
 template <typename VT, int CHUNK, typename IT>
 __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     constexpr int NS = 2;
-    __shared__ double s_red[32 * 3];
+    __shared__ double s_red[32 * 4];
     __shared__ double s_tot[4];
     __shared__ int s_flag;
     __shared__ int2 s_slice[kGtgSlices];
@@ -149,13 +149,15 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     int fell_back = -1;
 
     // r = b - A x in FP64 (stored rounded); with Jacobi also z = M^-1 r into the record.
-    // Partials: r.z (Jacobi only), r.r, ||b - A x||^2.
+    // Partials: r.z (Jacobi only), r.r, ||b - A x||^2, and in the first pass ||b||^2.
     auto residual_phase = [&](bool init) {
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = sb + warp; s < se; s += wpb) {
             const int row = s * 32 + lane;
             const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
-            const double rt = a.b64[row] - y;
+            const double bv = a.b64[row];
+            const double rt = bv - y;
+            if (init) acc[3] += bv * bv;
             const float rv = static_cast<float>(rt);
             r_cur[row] = rv;
             if (jac) {
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             acc[2] += rt * rt;
         }
         cur_bank = next_bank();
-        publish<3>(acc, s_red, cur_bank);
+        publish<4>(acc, s_red, cur_bank);
     };
     // z = G^T t into the record, partial r.z (r = r_cur)
     auto z_phase = [&]() {
@@ -195,15 +197,17 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
         cur_bank = next_bank();
         publish<1>(acc, s_red, cur_bank);
     };
-    double rz = 0.0, rr = 0.0, true_rr = 0.0;
-    // FP64 residual and its preconditioning; false when a barrier gave up
+    double rz = 0.0, rr = 0.0, true_rr = 0.0, bb = 0.0;
+    // FP64 residual and its preconditioning (the first one also sums ||b||^2); false when
+    // a barrier gave up
     auto refresh = [&](bool init) -> bool {
         residual_phase(init);
         if (!bar.sync(&s_flag)) return false;
-        grid_totals(cur_bank, 3, s_tot);
+        grid_totals(cur_bank, 4, s_tot);
         rz = s_tot[0];
         rr = s_tot[1];
         true_rr = s_tot[2];
+        if (init) bb = s_tot[3];
         if (!jac) {
             for (int s0 = sb + warp; s0 < se; s0 += kGRows * wpb) {
                 int sl[kGRows];
@@ -225,11 +229,13 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     };
 
     if (!refresh(true)) return;
+    const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * bb : a.tau_true_rr;
+    if (lead) a.out->bb = bb;
     double rr_at_replace = rr, best_true = true_rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
         int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
-    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
 
     if (converged_now) {
         status = XPLUS_CONVERGED;
@@ -364,7 +370,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             }
             bool do_replace = false, drop_replace = false, restart = false;
             if (true_mode) {
-                if (rr_new <= a.tau_true_rr) do_replace = drop_replace = true;
+                if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
                 if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
@@ -408,7 +414,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             }
             rz = rz_new;
             rr = rr_new;
-            if (true_mode ? (do_replace && true_rr <= a.tau_true_rr) : (rr <= a.tau_rr)) {
+            if (true_mode ? (do_replace && true_rr <= tau_true_rr) : (rr <= a.tau_rr)) {
                 status = XPLUS_CONVERGED;
                 break;
             }

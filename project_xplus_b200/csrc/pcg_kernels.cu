@@ -45,7 +45,7 @@ constexpr int kSlicesInFlight = 2;
 template <typename VT, typename XT, int CHUNK, bool DIFF, typename IT>
 __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
     constexpr int NS = kSlicesInFlight;
-    __shared__ double s_red[32 * 3];
+    __shared__ double s_red[32 * 4];
     __shared__ double s_tot[4];
     __shared__ int s_flag;
     __shared__ int2 s_slice[kMaxSlicesPerBlock];  // {first slot, width} of the block's slices
@@ -98,11 +98,13 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
     // ---- residual phase: r = b - A x in FP64, stored rounded, z = M^-1 r into the record
     //      (init also clears p); partials r.z, r.r, true r.r ----
     auto residual_phase = [&](bool init) {
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = sb + warp; s < se; s += wpb) {
             const int row = s * 32 + lane;
             const double y = row_fp64<VT, XT, CHUNK, DIFF, IT>(a, s, lane, row);
-            const double rt = a.b64[row] - y;
+            const double bv = a.b64[row];
+            const double rt = bv - y;
+            if (init) acc[3] += bv * bv;
             const XT rv = static_cast<XT>(rt);
             const XT zv = minv[row] * rv;
             r[row] = rv;
@@ -113,18 +115,20 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
             acc[2] += rt * rt;
         }
         cur_bank = next_bank();
-        publish<3>(acc, s_red, cur_bank);
+        publish<4>(acc, s_red, cur_bank);
     };
 
     residual_phase(true);
     if (!bar.sync(&s_flag)) return;
-    grid_totals(cur_bank, 3, s_tot);
+    grid_totals(cur_bank, 4, s_tot);
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
+    const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
+    if (lead) a.out->bb = s_tot[3];
     double rr_at_replace = rr, best_true = true_rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
         int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
-    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
     clock(4);
 
     if (converged_now) {
@@ -235,7 +239,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
             }
             bool do_replace = false, drop_replace = false;
             if (true_mode) {
-                if (rr_new <= a.tau_true_rr) do_replace = drop_replace = true;
+                if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
                 if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
@@ -272,7 +276,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
             }
             rz = rz_new;
             rr = rr_new;
-            if (true_mode ? (do_replace && true_rr <= a.tau_true_rr) : (rr <= a.tau_rr)) {
+            if (true_mode ? (do_replace && true_rr <= tau_true_rr) : (rr <= a.tau_rr)) {
                 status = XPLUS_CONVERGED;
                 break;
             }

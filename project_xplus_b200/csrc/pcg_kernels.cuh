@@ -14,6 +14,7 @@ struct PcgOut {
     double rz, rr, pap, alpha;
     double true_rr;    // ||b - A x||^2 in FP64 at exit
     double reserved;   // GTG kernel: iteration at which it fell back to Jacobi (-1: never)
+    double bb;         // ||b||^2 in FP64, summed by the kernel in its first residual pass
     long long t_start_ns, t_end_ns;
     long long t_phase[4];  // block 0: phase A work, barrier wait, phase B work, barrier wait (ns)
 };
@@ -48,6 +49,8 @@ struct PcgArgs {
     int trace_cap;
     double tau_rr;          // stop when recurrence rr <= tau_rr (abs mode)
     double tau_true_rr;     // >= 0: FP64 true-residual mode, stop when ||b-Ax||^2 <= this
+    double tau2_rel;        // > 0: relative true-residual mode; the kernel replaces tau_true_rr
+                            // by tau2_rel * ||b||^2, ||b||^2 summed with the first residual
     int max_iters;
     int replace_every;
     double replace_drop;    // rr ratio that triggers a replacement (0: off)

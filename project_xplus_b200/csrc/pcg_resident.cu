@@ -76,7 +76,7 @@ template <typename VT, int CHUNK, typename IT>
 __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
     constexpr int NS = kResNS;
     extern __shared__ float smem[];
-    __shared__ double s_red[32 * 3];
+    __shared__ double s_red[32 * 4];
     __shared__ double s_tot[4];
     __shared__ int s_flag;
     __shared__ int2 s_slice[kResSlices];
@@ -146,11 +146,13 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
     // ---- residual phase: r = b - A x in FP64 (x of neighbours from global memory), rounded
     //      into shared r; z = M^-1 r into the record (init also clears p) ----
     auto residual_phase = [&](bool init) {
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = sb + warp; s < se; s += wpb) {
             const int row = s * 32 + lane;
             const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
-            const double rt = a.b64[row] - y;
+            const double bv = a.b64[row];
+            const double rt = bv - y;
+            if (init) acc[3] += bv * bv;
             const float r_ = static_cast<float>(rt);
             const float z_ = mi[row - r0] * r_;
             rv[row - r0] = r_;
@@ -161,18 +163,20 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
             acc[2] += rt * rt;
         }
         cur_bank = next_bank();
-        publish<3>(acc, s_red, cur_bank);
+        publish<4>(acc, s_red, cur_bank);
     };
 
     residual_phase(true);
     if (!bar.sync(&s_flag)) return;
-    grid_totals(cur_bank, 3, s_tot);
+    grid_totals(cur_bank, 4, s_tot);
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
+    const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
+    if (lead) a.out->bb = s_tot[3];
     double rr_at_replace = rr, best_true = true_rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
         int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
-    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
     const int flush_every = a.flush_every > 0 ? a.flush_every : 16;
     clock(4);
 
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
             }
             bool do_replace = false, drop_replace = false;
             if (true_mode) {
-                if (rr_new <= a.tau_true_rr) do_replace = drop_replace = true;
+                if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
                 if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
             }
             rz = rz_new;
             rr = rr_new;
-            if (true_mode ? (do_replace && true_rr <= a.tau_true_rr) : (rr <= a.tau_rr)) {
+            if (true_mode ? (do_replace && true_rr <= tau_true_rr) : (rr <= a.tau_rr)) {
                 status = XPLUS_CONVERGED;
                 break;
             }
@@ -451,11 +455,13 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
     };
     // r = b - A x in FP64 into shared r; records of generation g get {m r, 0, p (kept, or 0)}
     auto residual_phase = [&](bool init, int g) {
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = sb + warp; s < se; s += wpb) {
             const int row = s * 32 + lane;
             const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
-            const double rt = a.b64[row] - y;
+            const double bv = a.b64[row];
+            const double rt = bv - y;
+            if (init) acc[3] += bv * bv;
             const float r_ = static_cast<float>(rt);
             const float z_ = mi[row - r0] * r_;
             rv[row - r0] = r_;
@@ -467,7 +473,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             acc[2] += rt * rt;
         }
         cur_bank = next_bank();
-        publish<3>(acc, s_red, cur_bank);
+        publish<4>(acc, s_red, cur_bank);
     };
     // the pending update of the previous iteration: dx += alpha p', r -= alpha Ap'
     auto apply_update = [&](float al) {
@@ -481,14 +487,16 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
     int gen = 0;
     residual_phase(true, gen);
     if (!bar.sync(&s_flag)) return;
-    grid_totals(cur_bank, 3, s_tot);
+    grid_totals(cur_bank, 4, s_tot);
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
+    const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
+    if (lead) a.out->bb = s_tot[3];
     double rr_at_replace = rr, best_true = true_rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     double pend = 0.0;  // alpha of the update not yet applied to x and r (0: none)
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
         int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
-    const bool converged_now = true_mode ? (true_rr <= a.tau_true_rr) : (rr <= a.tau_rr);
+    const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
     const int flush_every = a.flush_every > 0 ? a.flush_every : 16;
     clock(4);
 
@@ -625,7 +633,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             }
             bool do_replace = false, drop_replace = false;
             if (true_mode) {
-                if (rr_new <= a.tau_true_rr) do_replace = drop_replace = true;
+                if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
                 if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
@@ -667,7 +675,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             }
             rz = rz_new;
             rr = rr_new;
-            if (true_mode ? (do_replace && true_rr <= a.tau_true_rr) : (rr <= a.tau_rr)) {
+            if (true_mode ? (do_replace && true_rr <= tau_true_rr) : (rr <= a.tau_rr)) {
                 status = XPLUS_CONVERGED;
                 break;
             }

@@ -65,7 +65,6 @@ struct xplus_pcg {
     long long* d_block_clk = nullptr;  // per-CTA phase clock [grid][4]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     xplus_metrics last{};
-    double last_bnorm2 = 0.0;
     bool pending = false;
     int debug_skip_block = -1;
     long long phase_ns[4] = {0, 0, 0, 0};
@@ -412,8 +411,7 @@ void ensure_trace(xplus_pcg* h, int cap) {
 }
 
 // Enqueue one solve on stream st: b64/x64 already in SELL order on the device.
-void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, double bnorm2,
-                   int trace_rows, cudaStream_t st) {
+void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, int trace_rows, cudaStream_t st) {
     require(tau > 0.0 && tau == tau, XPLUS_ERR_ARG, "tau must be positive");
     require(tau_mode == XPLUS_TAU_ABS_RR || tau_mode == XPLUS_TAU_REL_TRUE, XPLUS_ERR_ARG, "bad tau_mode");
     const int max_iters = max_iters_in > 0 ? max_iters_in : std::max(4 * h->n, 1000);
@@ -452,8 +450,9 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
         a.tau_true_rr = -1.0;
     } else {
         require(h->d_val64 != nullptr, XPLUS_ERR_ARG, "TAU_REL_TRUE needs keep_fp64 (the FP64 matrix copy)");
-        a.tau_true_rr = tau * tau * bnorm2;
-        a.tau_rr = a.tau_true_rr;
+        a.tau_true_rr = 0.0;
+        a.tau2_rel = tau * tau;  // the kernel scales it by ||b||^2 of the b on the device
+        a.tau_rr = 0.0;
         a.replace_every = h->opts.replace_every;
         a.replace_drop = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
         const bool low = h->opts.value_type == XPLUS_BF16 || h->opts.value_type == XPLUS_F16;
@@ -480,7 +479,6 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, dou
     else
         cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st, h->window), "persistent PCG launch");
     cuda_check(cudaEventRecord(h->ev1, st), "event");
-    h->last_bnorm2 = bnorm2;
     h->pending = true;
 }
 
@@ -501,7 +499,7 @@ void collect(xplus_pcg* h, xplus_metrics* m) {
         L.rr = o.rr;
         L.pap = o.pap;
         L.alpha = o.alpha;
-        L.true_rel_residual = h->last_bnorm2 > 0 ? std::sqrt(o.true_rr / h->last_bnorm2) : std::sqrt(o.true_rr);
+        L.true_rel_residual = o.bb > 0 ? std::sqrt(o.true_rr / o.bb) : std::sqrt(o.true_rr);
         L.kernel_ms = ms;
         L.reserved[0] = o.stagnated;
         L.reserved[1] = static_cast<double>(o.t_end_ns - o.t_start_ns) * 1e-6;
@@ -686,8 +684,6 @@ int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau,
         cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
         cudaStream_t st = h->stream;
         const size_t nb = sizeof(double) * static_cast<size_t>(h->n);
-        double bnorm2 = 0.0;
-        for (int i = 0; i < h->n; ++i) bnorm2 += b[i] * b[i];
         cuda_check(cudaMemcpyAsync(h->d_bio, b, nb, cudaMemcpyHostToDevice, st), "H2D");
         if (x0) cuda_check(cudaMemcpyAsync(h->d_xio, x0, nb, cudaMemcpyHostToDevice, st), "H2D");
         else cuda_check(cudaMemsetAsync(h->d_xio, 0, nb, st), "memset");
@@ -695,7 +691,7 @@ int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau,
         cuda_check(gather_to_sell(XPLUS_F64, h->d_xio, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");
         const int rows = resid_hist && hist_len > 0 ? hist_len : 0;
         if (rows > 0) ensure_trace(h, rows);
-        enqueue_solve(h, tau, tau_mode, max_iters, bnorm2, rows, st);
+        enqueue_solve(h, tau, tau_mode, max_iters, rows, st);
         cuda_check(scatter_from_sell(h->d_x64, h->d_xio, h->d_perm, h->n, st), "scatter");
         cuda_check(cudaMemcpyAsync(x_out, h->d_xio, nb, cudaMemcpyDeviceToHost, st), "D2H");
         std::vector<double> tr;
@@ -728,16 +724,9 @@ int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double 
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
         cuda_check(gather_to_sell(XPLUS_F64, d_b, h->d_b64, h->d_perm, h->n, h->n_pad, st), "gather");
         cuda_check(gather_to_sell(XPLUS_F64, d_x, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");
-        // ||b||^2 is needed for the relative test; it is taken by the kernel's exit
-        // residual only in absolute form, so the host supplies it from the last device b.
-        double bnorm2 = 0.0;
-        if (tau_mode == XPLUS_TAU_REL_TRUE) {
-            std::vector<double> hb(static_cast<size_t>(h->n));
-            cuda_check(cudaMemcpyAsync(hb.data(), d_b, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
-            cuda_check(cudaStreamSynchronize(st), "sync");
-            for (double v : hb) bnorm2 += v * v;
-        }
-        enqueue_solve(h, tau, tau_mode, max_iters, bnorm2, 0, st);
+        // stream-ordered: the kernel sums ||b||^2 for the relative test itself, so nothing
+        // here waits for the device
+        enqueue_solve(h, tau, tau_mode, max_iters, 0, st);
         cuda_check(scatter_from_sell(h->d_x64, d_x, h->d_perm, h->n, st), "scatter");
     });
 }
@@ -861,7 +850,7 @@ int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double
         }
         cuda_check(gather_to_sell(XPLUS_F64, b, h->d_b64, h->d_perm, h->n, h->n_pad, st), "gather");
         cuda_check(gather_to_sell(XPLUS_F64, x, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");
-        enqueue_solve(h, tau, XPLUS_TAU_ABS_RR, max_iters > 0 ? max_iters : std::max(4 * n, 1000), 0.0, 0, st);
+        enqueue_solve(h, tau, XPLUS_TAU_ABS_RR, max_iters > 0 ? max_iters : std::max(4 * n, 1000), 0, st);
         cuda_check(scatter_from_sell(h->d_x64, x, h->d_perm, h->n, st), "scatter");
         xplus_metrics m;
         collect(h, &m);

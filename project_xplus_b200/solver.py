@@ -160,6 +160,12 @@ def _type(t) -> int:
     return _TYPES[t] if isinstance(t, str) else int(t)
 
 
+def _metrics_dict(m) -> dict:
+    return dict(rz=m.rz, rr=m.rr, pap=m.pap, alpha=m.alpha, stagnated=bool(m.reserved[0]),
+                device_ms=m.reserved[1], kernel=KERNEL_NAMES.get(int(m.reserved[2]), "unknown"),
+                jacobi_fallback_at=int(m.reserved[3]) if int(m.reserved[2]) == 3 else -1)
+
+
 class PcgSolver:
     """One SPD system resident on the GPU (xplus_pcg handle)."""
 
@@ -229,16 +235,32 @@ class PcgSolver:
             t = t.reshape(rows, 5)
             tr = [IterationTrace(k, *map(float, t[k])) for k in range(rows)]
         bnorm = float(np.linalg.norm(b))
-        res_rel = m.true_rel_residual if bnorm > 0 else m.true_rel_residual
+        res_rel = m.true_rel_residual
         status = STATUS_NAMES.get(m.status, "unknown")
         return PcgResult(
             solution=x, iterations=m.iterations, effective_max_iters=eff, final_rr=m.rr,
             status=status, converged=(m.status == 0), residual_l2=res_rel * bnorm,
             residual_rel=res_rel, iteration_trace=tr, replacements=m.replacements,
-            kernel_ms=m.kernel_ms, setup_ms=m.setup_ms,
-            metrics=dict(rz=m.rz, rr=m.rr, pap=m.pap, alpha=m.alpha, stagnated=bool(m.reserved[0]),
-                         device_ms=m.reserved[1], kernel=KERNEL_NAMES.get(int(m.reserved[2]), "unknown"),
-                         jacobi_fallback_at=int(m.reserved[3]) if int(m.reserved[2]) == 3 else -1))
+            kernel_ms=m.kernel_ms, setup_ms=m.setup_ms, metrics=_metrics_dict(m))
+
+    def solve_device(self, d_b, d_x, *, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE, max_iters=0, stream=None) -> None:
+        """Enqueues one solve on device-resident FP64 vectors (original row order; d_x holds
+        x0 and receives x) on `stream` (a torch.cuda.Stream or raw handle; None: the
+        solver's own) and returns without waiting.  last_metrics() waits and reports."""
+        s = getattr(stream, "cuda_stream", stream)
+        check(lib.xplus_pcg_solve_device(self._h, ptr(d_b), ptr(d_x), float(tau), int(tau_mode),
+                                         int(max_iters), s))
+
+    def last_metrics(self) -> dict:
+        """Outcome of the last solve (waits for it): status, iterations, replacements,
+        true relative residual, kernel time and the kernel's own counters."""
+        m = _lib.XplusMetrics()
+        check(lib.xplus_pcg_last_metrics(self._h, C.byref(m)))
+        out = _metrics_dict(m)
+        out.update(status=STATUS_NAMES.get(m.status, "unknown"), converged=(m.status == 0),
+                   iterations=m.iterations, replacements=m.replacements,
+                   residual_rel=m.true_rel_residual, kernel_ms=m.kernel_ms)
+        return out
 
     def set_gtg(self, g_low, fallback_iters: int = 0) -> None:
         """M^-1 = G^T G with G given on A's lower pattern (g_low order); None: Jacobi again."""

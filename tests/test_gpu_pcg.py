@@ -274,6 +274,49 @@ def test_nonzero_x0_and_repeat_solves_are_deterministic(gpu):
     assert [t.rr for t in r1.iteration_trace] == [t.rr for t in r2.iteration_trace]
 
 
+@pytest.mark.parametrize("kernel,kw", [("pcg_persistent_kernel", dict(resident=False)),
+                                       ("pcg_resident_kernel", dict(barriers_per_iter=2)),
+                                       ("pcg_resident1_kernel", dict()),
+                                       ("pcg_gtg_kernel", dict())])
+def test_device_solve_is_stream_ordered(gpu, oracle, kernel, kw):
+    """xplus_pcg_solve_device returns without waiting for the device (the relative tolerance
+    is scaled by ||b||^2 summed inside the kernel): enqueued behind a sleeping kernel on the
+    same stream, the stream is still busy when the call returns; the outcome is bit-identical
+    to the host-buffer solve and reaches the FP64 relative tolerance, for every kernel."""
+    import torch
+    from project_xplus_b200.learned import fsai_lower
+    d, _ = g.fem2d(150, sigma=2.0, seed=3, perm_seed=2, rcm=True)
+    s = xp.PcgSolver.from_dataset(d, **kw)
+    if kernel == "pcg_gtg_kernel":
+        s.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))
+    host = s.solve(d.b, None, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE)
+    assert host.converged and host.metrics["kernel"] == kernel
+    st = torch.cuda.Stream()
+    d_b = torch.from_numpy(d.b).cuda()
+    d_x = torch.zeros_like(d_b)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(st):
+        torch.cuda._sleep(200_000_000)  # ~0.1 s of spinning ahead of the solve
+        d_b2 = d_b * 1.0                # b produced on the stream itself
+    s.solve_device(d_b2, d_x, tau=1e-8, stream=st)
+    assert not st.query()
+    m = s.last_metrics()
+    st.synchronize()
+    assert m["converged"] and m["kernel"] == kernel
+    assert m["iterations"] == host.iterations and m["residual_rel"] == host.residual_rel
+    x = d_x.cpu().numpy()
+    np.testing.assert_array_equal(x, host.solution)
+    assert oracle.residual_norm(d, x) / np.linalg.norm(d.b) <= 1e-8
+    # absolute mode reports the same relative residual measure as the host path
+    a_host = s.solve(d.b, None, tau=1e-6, max_iters=40)
+    d_x.zero_()
+    torch.cuda.synchronize()
+    s.solve_device(d_b, d_x, tau=1e-6, tau_mode=xp.XPLUS_TAU_ABS_RR, max_iters=40)
+    a_dev = s.last_metrics()
+    assert a_dev["iterations"] == a_host.iterations and a_dev["residual_rel"] == a_host.residual_rel
+    s.close()
+
+
 def test_cfg_scale_solve_property(gpu, oracle):
     """The 1108x1108 system (n = 1,227,664): FP32 plain kernel with FP64 residual replacement
     reaches 1e-8 FP64 true relative residual; checked on the host in FP64."""

@@ -359,6 +359,8 @@ def run_b200(args):
     # The 3D system as a mixed-precision workload: values in FP32, BF16 or FP16 (power-of-two
     # scale), FP32 inner PCG, FP64 residual replacement every 50 iterations or at a 1e-4 drop
     # of the recurrence residual, to 1e-10 FP64 true relative residual; FP64 for comparison.
+    # 16-bit values run with the library defaults: two-term entries in cancelling rows and
+    # flexible re-conjugation of the search direction at replacements.
     mixed_3d = None
     if not args.no_spmv3d and not args.no_compare:
         mixed_3d = {"workload": "3d-p1fem-128^3-sigma1.5, tol 1e-10 rel. FP64 true residual", "n": d3.n}
@@ -375,7 +377,8 @@ def run_b200(args):
             r3 = runs[-1]
             mixed_3d[name] = {"time_to_tol_ms": r3.kernel_ms, "iterations": r3.iterations, "status": r3.status,
                               "replacements": r3.replacements, "true_rel_residual": r3.residual_rel,
-                              "kernel": r3.metrics["kernel"]}
+                              "stagnated": r3.metrics["stagnated"], "kernel": r3.metrics["kernel"],
+                              "slots": s3.info()["slots"]}
             s3.close()
     if not args.no_spmv3d:
         del d3

@@ -104,11 +104,13 @@ typedef struct xplus_opts {
                               the convergence check (periodic ones, replace_every, keep it),
                               3 adaptive: starts as 2 and switches to 1 for the rest of the solve
                               when ||b - A x|| grows past twice its best or stagnation_window
-                              replacements bring no progress.  -1 (default): 3 for 16-bit values,
-                              whose inexact operator can break the conjugacy a kept p relies on,
-                              0 otherwise.  Measured with FP16 values, replacement every 50
-                              iterations or at a 1e-4 drop: 2D 150^2 sigma=2 needs 2 (1154
-                              iterations; 1 takes 4890), 3D 128^3 needs 1 (1735; 2 stalls) */
+                              replacements bring no progress, 4 flexible: at every replacement
+                              p is re-conjugated to the replaced residual with the flexible-CG
+                              coefficient beta = -(z.Ap)/(p.Ap), switching to 1 for the rest of
+                              the solve on the same two signals as 3.
+                              -1 (default): 4 for 16-bit values, whose inexact operator opens a
+                              gap between the recurrence and the true residual that a kept p
+                              does not survive, 0 otherwise */
     int barriers_per_iter; /* SM-resident kernel: 1 (default) folds both dot products into one
                               reduction by expanding r_{k+1}.z_{k+1} and r_{k+1}.r_{k+1} in alpha;
                               2 reduces them after the update as the reference does */
@@ -119,6 +121,18 @@ typedef struct xplus_opts {
     int build_on_gpu;      /* xplus_pcg_create builds the SELL-C-sigma layout on the GPU (the
                               same arrays as the host builder, bit for bit; default 1, sigma <=
                               4096); 0 builds it on the host */
+    double split_ratio;    /* 16-bit values, xplus_pcg_create: an off-diagonal entry a_ij of a
+                              row i or j whose sum_k |a_ik| / a_ii exceeds this, with |a_ij|
+                              above half of min(a_ii, a_jj), is stored as two 16-bit terms, the
+                              rounded value and its rounding remainder, in two slots of the row
+                              (the FP64 copy holds both terms, summing to a_ij exactly).  Such
+                              rows carry large weights of both signs that cancel in A but whose
+                              16-bit rounding errors do not; left rounded they can make the
+                              stored operator indefinite.  0: off; -1 (default): 1.5 for BF16,
+                              2 for FP16 values.  Measured on the 128^3 P1-tetrahedra system
+                              (1e-10, replacement every 50 iterations or at a 1e-4 drop): BF16
+                              826 iterations in 102 ms with 1.6% more slots (singly rounded BF16
+                              diverges), FP16 836 in 91 ms, FP32 values 807 in 90 ms */
 } xplus_opts;
 
 typedef struct xplus_metrics {

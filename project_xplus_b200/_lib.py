@@ -29,6 +29,7 @@ class XplusOpts(C.Structure):
         ("row_sum_form", C.c_int), ("index16", C.c_int), ("l2_persist", C.c_int),
         ("resident", C.c_int), ("restart_on_replace", C.c_int), ("barriers_per_iter", C.c_int),
         ("stagnation_gain", C.c_double), ("stagnation_window", C.c_int), ("build_on_gpu", C.c_int),
+        ("split_ratio", C.c_double),
     ]
 
 

@@ -59,7 +59,7 @@ struct BatchArgs {
     int max_iters;            // <= 0: max(4n, 1000) per system
     int replace_every;
     double replace_drop2;     // squared ||r|| drop that triggers a replacement (0: off)
-    int restart_on_replace;   // 1: beta = 0 after every replacement, 2: after drop/convergence ones
+    int restart_on_replace;   // ReplacePolicy: 0 keep p, 1 / 2 restart, 3 / 4 adaptive
     double stag_factor;
     int stag_window;
     int* out_status;
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
         const bool true_mode = a.tau_mode == XPLUS_TAU_REL_TRUE;
 
         // residual phase: r = b - A x in FP64 rounded to FP32, z = M^-1 r into the record
-        // (init also clears p); totals r.z, r.r, ||b - A x||^2, ||b||^2
+        // (init also clears p); totals r.z, r.r, ||b - A x||^2, and ||b||^2 (init) or z.Ap'
         auto residual_phase = [&](bool init, double (&acc)[4]) {
             acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
             for (int s = sb + warp; s < se; s += wpb) {
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                 acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
                 acc[1] += static_cast<double>(rv) * static_cast<double>(rv);
                 acc[2] += rt * rt;
-                acc[3] += bv * bv;
+                acc[3] += init ? bv * bv : static_cast<double>(zv) * static_cast<double>(a.ap[row]);
             }
             cluster_sum<4>(cl, acc, s_red, s_part, s_tot, pbank);
         };
@@ -187,10 +187,10 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
         double rz = tot[0], rr = tot[1], true_rr = tot[2];
         const double bb = tot[3];
         const double tau_true_rr = a.tau * a.tau * bb;
-        double rr_at_replace = rr, best_true = true_rr;
+        double rr_at_replace = rr, zap = 0.0;
         double pap = 0.0, alpha = 0.0, beta = 0.0;
-        int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0;
-        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
+        int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0;
+        ReplacePolicy pol(a.restart_on_replace, true_rr);
         bool stagnated = false;
         const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau);
 
@@ -340,20 +340,10 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     rz_new = t4[0];
                     rr_new = t4[1];
                     true_rr = t4[2];
+                    zap = t4[3];
                     ++replacements;
                     rr_at_replace = rr_new;
-                    if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
-                    if (true_rr < a.stag_factor * best_true) {
-                        best_true = true_rr;
-                        stagnant = 0;
-                    } else if (++stagnant >= a.stag_window) {
-                        if (a.restart_on_replace == 3 && restart_mode == 2) {
-                            restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
-                            stagnant = 0;
-                        } else {
-                            stagnated = true;
-                        }
-                    }
+                    if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = true;
                 }
                 rz = rz_new;
                 rr = rr_new;
@@ -366,7 +356,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     status = XPLUS_BREAKDOWN;
                     break;
                 }
-                beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace)) ? 0.0 : rz / rz_old;
+                beta = pol.beta(do_replace, drop_replace, rz, rz_old, zap, pap);
                 if (bad(beta)) {
                     status = XPLUS_BREAKDOWN;
                     break;
@@ -587,6 +577,7 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
     require(o.slice_height == 32, XPLUS_ERR_ARG, "slice_height must be 32");
     require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
     require(o.sigma >= 1, XPLUS_ERR_ARG, "sigma must be >= 1");
+    require(o.restart_on_replace >= -1 && o.restart_on_replace <= 4, XPLUS_ERR_ARG, "restart_on_replace must be -1..4");
     for (int k = 0; k < nsys; ++k) {
         require(row_ptrs[k] && col_idxs[k] && values[k] && ns[k] > 0, XPLUS_ERR_ARG, "bad system " + std::to_string(k));
         validate_csr(ns[k], row_ptrs[k], col_idxs[k], row_ptrs[k][ns[k]]);
@@ -827,7 +818,7 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     a.replace_every = h->opts.replace_every;
     a.replace_drop2 = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
     const bool low = h->opts.value_type != XPLUS_F32;
-    a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 3 : 0) : h->opts.restart_on_replace;
+    a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 4 : 0) : h->opts.restart_on_replace;
     stagnation_args(h->opts, &a.stag_factor, &a.stag_window);
     a.out_status = h->d_status;
     a.out_iters = h->d_iters;

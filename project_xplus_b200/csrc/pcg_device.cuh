@@ -13,6 +13,47 @@ namespace dev {
 
 constexpr double kBreakdownEps = 1.0e-30;  // include/cg_common.hpp:13
 
+// Search direction after an FP64 residual replacement (xplus_opts.restart_on_replace), and
+// the stagnation test, for one solve.  Modes: 0 keeps p (beta = rz_new / rz_old); 1 restarts
+// it (beta = 0) at every replacement; 2 restarts it only at drop- or convergence-triggered
+// replacements; 4 re-conjugates it to the replaced residual with the flexible-CG coefficient
+// beta = -(z_new . Ap') / (p' . Ap') (Notay's FCG(1); equal to rz_new / rz_old when the
+// replaced residual is the recurrence one), which survives the gap an inexact low-precision
+// operator opens between the two residuals.  Policy 3 starts in mode 2 and policy 4 in mode 4;
+// both drop to mode 1 for the rest of the solve when a replacement finds ||b - A x|| above
+// twice its best (CG's residual is not monotone, so a smaller rise is no signal) or the
+// stagnation window runs out.
+struct ReplacePolicy {
+    int policy, mode, stagnant;
+    double best;
+    __device__ ReplacePolicy(int restart_on_replace, double true_rr)
+        : policy(restart_on_replace), mode(restart_on_replace == 3 ? 2 : restart_on_replace), stagnant(0),
+          best(true_rr) {}
+    // After a replacement that measured true_rr = ||b - A x||^2: true when the solve stagnated.
+    __device__ bool after(double true_rr, double stag_factor, int stag_window) {
+        if (((policy == 3 && mode == 2) || mode == 4) && true_rr > 4.0 * best) mode = 1;
+        if (true_rr < stag_factor * best) {
+            best = true_rr;
+            stagnant = 0;
+        } else if (++stagnant >= stag_window) {
+            if ((policy == 3 && mode == 2) || mode == 4) {
+                mode = 1;  // no progress keeping p: restart it at every replacement from now on
+                stagnant = 0;
+            } else {
+                return true;
+            }
+        }
+        return false;
+    }
+    // zap = z_new . Ap' (taken by the replacement), pap = p' . Ap' of the iteration
+    __device__ double beta(bool replaced, bool drop_replaced, double rz, double rz_old, double zap,
+                           double pap) const {
+        if (replaced && mode == 4) return -zap / pap;
+        if ((mode == 1 && replaced) || (mode == 2 && drop_replaced)) return 0.0;
+        return rz / rz_old;
+    }
+};
+
 // Row `32*s + lane` of the SELL matrix times x, accumulated in AT.  With DIFF the slots hold
 // the off-diagonal weights w_ij only and the row computes sum_j w_ij (x_j - x_i); the caller
 // adds s_i x_i with the row sum s_i = sum_j a_ij.  That form is exact algebra, and it keeps

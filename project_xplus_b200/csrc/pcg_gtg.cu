@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     int fell_back = -1;
 
     // r = b - A x in FP64 (stored rounded); with Jacobi also z = M^-1 r into the record.
-    // Partials: r.z (Jacobi only), r.r, ||b - A x||^2, and in the first pass ||b||^2.
+    // Partials: r.z (Jacobi only), r.r, ||b - A x||^2, and ||b||^2 in the first pass or
+    // z_new . Ap' at a replacement (Jacobi only).
     auto residual_phase = [&](bool init) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = sb + warp; s < se; s += wpb) {
@@ -162,8 +163,12 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             r_cur[row] = rv;
             if (jac) {
                 const float zv = minv[row] * rv;
-                if (init) store_rec(rec + row, zv, 0.0f);
-                else rec[row].z = zv;
+                if (init) {
+                    store_rec(rec + row, zv, 0.0f);
+                } else {
+                    rec[row].z = zv;
+                    acc[3] += static_cast<double>(zv) * static_cast<double>(ap[row]);
+                }
                 acc[0] += static_cast<double>(rv) * static_cast<double>(zv);
             } else if (init) {
                 store_rec(rec + row, 0.0f, 0.0f);
@@ -174,9 +179,9 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
         cur_bank = next_bank();
         publish<4>(acc, s_red, cur_bank);
     };
-    // z = G^T t into the record, partial r.z (r = r_cur)
-    auto z_phase = [&]() {
-        double acc[1] = {0.0};
+    // z = G^T t into the record, partials r.z (r = r_cur) and, with zap_too (a replacement), z.Ap'
+    auto z_phase = [&](bool zap_too) {
+        double acc[2] = {0.0, 0.0};
         for (int s0 = sb + warp; s0 < se; s0 += kGRows * wpb) {
             int sl[kGRows];
             float zv[kGRows], rv[kGRows];
@@ -192,12 +197,13 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 if (sl[k] < 0) continue;
                 rec[sl[k] * 32 + lane].z = zv[k];
                 acc[0] += static_cast<double>(rv[k]) * static_cast<double>(zv[k]);
+                if (zap_too) acc[1] += static_cast<double>(zv[k]) * static_cast<double>(ap[sl[k] * 32 + lane]);
             }
         }
         cur_bank = next_bank();
-        publish<1>(acc, s_red, cur_bank);
+        publish<2>(acc, s_red, cur_bank);
     };
-    double rz = 0.0, rr = 0.0, true_rr = 0.0, bb = 0.0;
+    double rz = 0.0, rr = 0.0, true_rr = 0.0, bb = 0.0, zap = 0.0;
     // FP64 residual and its preconditioning (the first one also sums ||b||^2); false when
     // a barrier gave up
     auto refresh = [&](bool init) -> bool {
@@ -208,6 +214,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
         rr = s_tot[1];
         true_rr = s_tot[2];
         if (init) bb = s_tot[3];
+        else zap = s_tot[3];
         if (!jac) {
             for (int s0 = sb + warp; s0 < se; s0 += kGRows * wpb) {
                 int sl[kGRows];
@@ -220,10 +227,11 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                     if (sl[k] >= 0) t[sl[k] * 32 + lane] = tv[k];
             }
             if (!bar.sync(&s_flag)) return false;
-            z_phase();
+            z_phase(!init);
             if (!bar.sync(&s_flag)) return false;
-            grid_totals(cur_bank, 1, s_tot);
+            grid_totals(cur_bank, 2, s_tot);
             rz = s_tot[0];
+            if (!init) zap = s_tot[1];
         }
         return true;
     };
@@ -231,10 +239,10 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
     if (!refresh(true)) return;
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * bb : a.tau_true_rr;
     if (lead) a.out->bb = bb;
-    double rr_at_replace = rr, best_true = true_rr;
+    double rr_at_replace = rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
-    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
-        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
+    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
+    ReplacePolicy pol(a.restart_on_replace, true_rr);
     const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
 
     if (converged_now) {
@@ -354,7 +362,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
             }
             if (!jac) {
                 // ---- D: z = G^T t, r'.z ----
-                z_phase();
+                z_phase(false);
                 clock(3);
                 if (!bar.sync(&s_flag)) return;
                 clock(1);
@@ -379,7 +387,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 jac = true;
                 fell_back = iterations;
                 stagnated = 0;
-                stagnant = 0;
+                pol.stagnant = 0;
                 do_replace = true;
                 restart = true;
             }
@@ -389,19 +397,12 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 rr_new = rr;
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
                 if (restart) {
-                    best_true = true_rr;
-                } else if (true_rr < a.stag_factor * best_true) {
-                    best_true = true_rr;
-                    stagnant = 0;
-                } else if (++stagnant >= a.stag_window) {
-                    if (a.restart_on_replace == 3 && restart_mode == 2) {
-                        restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
-                        stagnant = 0;
-                    } else {
-                        stagnated = 1;
-                    }
+                    // the switch to Jacobi: the refreshed residual is the new reference
+                    if (pol.policy == 3 && pol.mode == 2 && true_rr > 4.0 * pol.best) pol.mode = 1;
+                    pol.best = true_rr;
+                } else if (pol.after(true_rr, a.stag_factor, a.stag_window)) {
+                    stagnated = 1;
                 }
             }
             if (lead && a.trace && it < a.trace_cap) {
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace) || restart) ? 0.0 : rz / rz_old;
+            beta = restart ? 0.0 : pol.beta(do_replace, drop_replace, rz, rz_old, zap, pap);
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
     double* cur_bank = nullptr;
 
     // ---- residual phase: r = b - A x in FP64, stored rounded, z = M^-1 r into the record
-    //      (init also clears p); partials r.z, r.r, true r.r ----
+    //      (init also clears p); partials r.z, r.r, true r.r, and ||b||^2 (init) or z.Ap' ----
     auto residual_phase = [&](bool init) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = sb + warp; s < se; s += wpb) {
@@ -104,9 +104,10 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
             const double y = row_fp64<VT, XT, CHUNK, DIFF, IT>(a, s, lane, row);
             const double bv = a.b64[row];
             const double rt = bv - y;
-            if (init) acc[3] += bv * bv;
             const XT rv = static_cast<XT>(rt);
             const XT zv = minv[row] * rv;
+            // slot 3: ||b||^2 in the first pass, z_new . Ap' at a replacement
+            acc[3] += init ? bv * bv : static_cast<double>(zv) * static_cast<double>(ap[row]);
             r[row] = rv;
             if (init) store_rec(rec + row, zv, XT(0));
             else rec[row].z = zv;
@@ -124,10 +125,10 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
     if (lead) a.out->bb = s_tot[3];
-    double rr_at_replace = rr, best_true = true_rr;
+    double rr_at_replace = rr, zap = 0.0;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
-    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
-        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
+    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
+    ReplacePolicy pol(a.restart_on_replace, true_rr);
     const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
     clock(4);
 
@@ -246,25 +247,15 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
             if (do_replace) {
                 residual_phase(false);
                 if (!bar.sync(&s_flag)) return;
-                grid_totals(cur_bank, 3, s_tot);
+                grid_totals(cur_bank, 4, s_tot);
                 clock(4);
                 rz_new = s_tot[0];
                 rr_new = s_tot[1];
                 true_rr = s_tot[2];
+                zap = s_tot[3];
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
-                if (true_rr < a.stag_factor * best_true) {
-                    best_true = true_rr;
-                    stagnant = 0;
-                } else if (++stagnant >= a.stag_window) {
-                    if (a.restart_on_replace == 3 && restart_mode == 2) {
-                        restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
-                        stagnant = 0;
-                    } else {
-                        stagnated = 1;
-                    }
-                }
+                if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
             }
             if (lead && a.trace && it < a.trace_cap) {
                 double* t = a.trace + 5 * static_cast<size_t>(it);
@@ -285,7 +276,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace)) ? 0.0 : rz / rz_old;
+            beta = pol.beta(do_replace, drop_replace, rz, rz_old, zap, pap);
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;

@@ -152,9 +152,10 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
             const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
             const double bv = a.b64[row];
             const double rt = bv - y;
-            if (init) acc[3] += bv * bv;
             const float r_ = static_cast<float>(rt);
             const float z_ = mi[row - r0] * r_;
+            // slot 3: ||b||^2 in the first pass, z_new . Ap' at a replacement
+            acc[3] += init ? bv * bv : static_cast<double>(z_) * static_cast<double>(apv[row - r0]);
             rv[row - r0] = r_;
             if (init) store_rec(rec + row, z_, 0.0f);
             else rec[row].z = z_;
@@ -172,10 +173,10 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
     if (lead) a.out->bb = s_tot[3];
-    double rr_at_replace = rr, best_true = true_rr;
+    double rr_at_replace = rr, zap = 0.0;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
-    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
-        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
+    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
+    ReplacePolicy pol(a.restart_on_replace, true_rr);
     const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
     const int flush_every = a.flush_every > 0 ? a.flush_every : 16;
     clock(4);
@@ -284,25 +285,15 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 if (!bar.sync(&s_flag)) return;
                 residual_phase(false);
                 if (!bar.sync(&s_flag)) return;
-                grid_totals(cur_bank, 3, s_tot);
+                grid_totals(cur_bank, 4, s_tot);
                 clock(4);
                 rz_new = s_tot[0];
                 rr_new = s_tot[1];
                 true_rr = s_tot[2];
+                zap = s_tot[3];
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
-                if (true_rr < a.stag_factor * best_true) {
-                    best_true = true_rr;
-                    stagnant = 0;
-                } else if (++stagnant >= a.stag_window) {
-                    if (a.restart_on_replace == 3 && restart_mode == 2) {
-                        restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
-                        stagnant = 0;
-                    } else {
-                        stagnated = 1;
-                    }
-                }
+                if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
             }
             if (lead && a.trace && it < a.trace_cap) {
                 double* t = a.trace + 5 * static_cast<size_t>(it);
@@ -323,7 +314,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace)) ? 0.0 : rz / rz_old;
+            beta = pol.beta(do_replace, drop_replace, rz, rz_old, zap, pap);
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;
@@ -461,9 +452,10 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             const double y = row_fp64<VT, float, CHUNK, true, IT>(a, s, lane, row);
             const double bv = a.b64[row];
             const double rt = bv - y;
-            if (init) acc[3] += bv * bv;
             const float r_ = static_cast<float>(rt);
             const float z_ = mi[row - r0] * r_;
+            // slot 3: ||b||^2 in the first pass, z_new . Ap' at a replacement
+            acc[3] += init ? bv * bv : static_cast<double>(z_) * static_cast<double>(apv[row - r0]);
             rv[row - r0] = r_;
             rec_zr(g)[row] = z_;
             rec_za(g)[row] = 0.0f;
@@ -491,11 +483,11 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
     if (lead) a.out->bb = s_tot[3];
-    double rr_at_replace = rr, best_true = true_rr;
+    double rr_at_replace = rr, zap = 0.0;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     double pend = 0.0;  // alpha of the update not yet applied to x and r (0: none)
-    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnant = 0, stagnated = 0;
-        int restart_mode = a.restart_on_replace == 3 ? 2 : a.restart_on_replace;  // 3: adaptive, starts as 2
+    int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
+    ReplacePolicy pol(a.restart_on_replace, true_rr);
     const bool converged_now = true_mode ? (true_rr <= tau_true_rr) : (rr <= a.tau_rr);
     const int flush_every = a.flush_every > 0 ? a.flush_every : 16;
     clock(4);
@@ -645,25 +637,15 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 if (!bar.sync(&s_flag)) return;
                 residual_phase(false, gen);
                 if (!bar.sync(&s_flag)) return;
-                grid_totals(cur_bank, 3, s_tot);
+                grid_totals(cur_bank, 4, s_tot);
                 clock(4);
                 rz_new = s_tot[0];
                 rr_new = s_tot[1];
                 true_rr = s_tot[2];
+                zap = s_tot[3];
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (a.restart_on_replace == 3 && restart_mode == 2 && true_rr > 4.0 * best_true) restart_mode = 1;
-                if (true_rr < a.stag_factor * best_true) {
-                    best_true = true_rr;
-                    stagnant = 0;
-                } else if (++stagnant >= a.stag_window) {
-                    if (a.restart_on_replace == 3 && restart_mode == 2) {
-                        restart_mode = 1;  // no progress keeping p: restart it at every replacement from now on
-                        stagnant = 0;
-                    } else {
-                        stagnated = 1;
-                    }
-                }
+                if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
             }
             if (lead && a.trace && it < a.trace_cap) {
                 double* t = a.trace + 5 * static_cast<size_t>(it);
@@ -684,7 +666,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            beta = ((restart_mode == 1 && do_replace) || (restart_mode == 2 && drop_replace)) ? 0.0 : rz / rz_old;
+            beta = pol.beta(do_replace, drop_replace, rz, rz_old, zap, pap);
             if (bad(beta)) {
                 status = XPLUS_BREAKDOWN;
                 break;

@@ -141,13 +141,78 @@ std::vector<unsigned char> convert(const std::vector<double>& v, int type, doubl
     return out;
 }
 
-// Power-of-two scale that puts the largest |value| just below 2^15, inside FP16's range with
-// the smallest values of a ~1e9 dynamic range still normal.
-double f16_scale(const std::vector<double>& v) {
-    double m = 0.0;
-    for (double x : v) m = std::max(m, std::fabs(x));
-    if (!(m > 0.0)) return 1.0;
-    return std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(m))) - 15);
+// A CSR whose selected off-diagonal entries appear twice in a row: first the value rounded to
+// the 16-bit type, then the remainder a_ij - round(a_ij), exact in FP64, so the two terms sum
+// to a_ij exactly and the second, rounded in turn, carries the bits the first lost.  An entry
+// (i, j) is selected when row i or row j has sum_k |a_ik| / a_ii above `ratio` (a row whose
+// weights of both signs cancel in A, where independent rounding errors of the weights do not
+// cancel and can leave the stored operator indefinite) and |a_ij| is above half the smaller of
+// a_ii and a_jj (the weights whose errors matter there).  Empty when nothing is selected.
+struct TwoTermCsr {
+    std::vector<int> row_ptr, col_idx;
+    std::vector<double> values;
+};
+
+double round16(double v, int type, double scale) {
+    if (type == XPLUS_F16) return static_cast<double>(__half2float(__double2half(v / scale))) * scale;
+    return static_cast<double>(__bfloat162float(__double2bfloat16(v)));
+}
+
+void two_term_entries(int n, const int* row_ptr, const int* col_idx, const double* values, int type,
+                      double scale, double ratio, TwoTermCsr& out) {
+    std::vector<unsigned char> wide(static_cast<size_t>(n), 0);
+    std::vector<double> dabs(static_cast<size_t>(n), 0.0);
+    parallel_for(n, [&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            double off = 0.0, d = 0.0;
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+                if (col_idx[k] == i) d += values[k];
+                else off += std::fabs(values[k]);
+            }
+            dabs[static_cast<size_t>(i)] = std::fabs(d);
+            wide[static_cast<size_t>(i)] = off > ratio * std::fabs(d);
+        }
+    });
+    auto selected = [&](int64_t i, int k) {
+        const int j = col_idx[k];
+        return j != i && (wide[static_cast<size_t>(i)] || wide[static_cast<size_t>(j)]) &&
+               std::fabs(values[k]) > 0.5 * std::min(dabs[static_cast<size_t>(i)], dabs[static_cast<size_t>(j)]);
+    };
+    std::vector<int> extra(static_cast<size_t>(n) + 1, 0);
+    parallel_for(n, [&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            int c = 0;
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+                if (selected(i, k)) ++c;
+            extra[static_cast<size_t>(i) + 1] = c;
+        }
+    });
+    for (int i = 0; i < n; ++i) extra[static_cast<size_t>(i) + 1] += extra[static_cast<size_t>(i)];
+    if (extra[static_cast<size_t>(n)] == 0) return;
+    const int64_t total = static_cast<int64_t>(row_ptr[n]) + extra[static_cast<size_t>(n)];
+    require(total <= std::numeric_limits<int>::max(), XPLUS_ERR_ARG, "two-term entries overflow int32 row pointers");
+    out.row_ptr.resize(static_cast<size_t>(n) + 1);
+    for (int i = 0; i <= n; ++i) out.row_ptr[static_cast<size_t>(i)] = row_ptr[i] + extra[static_cast<size_t>(i)];
+    out.col_idx.resize(static_cast<size_t>(total));
+    out.values.resize(static_cast<size_t>(total));
+    parallel_for(n, [&](int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) {
+            int q = out.row_ptr[static_cast<size_t>(i)];
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+                const int j = col_idx[k];
+                if (selected(i, k)) {
+                    const double hi = round16(values[k], type, scale);
+                    out.col_idx[static_cast<size_t>(q)] = j;
+                    out.values[static_cast<size_t>(q++)] = hi;
+                    out.col_idx[static_cast<size_t>(q)] = j;
+                    out.values[static_cast<size_t>(q++)] = values[k] - hi;
+                } else {
+                    out.col_idx[static_cast<size_t>(q)] = j;
+                    out.values[static_cast<size_t>(q++)] = values[k];
+                }
+            }
+        }
+    });
 }
 
 // Handles that raised the process's persisting-L2 limit, and the limit before the first did:
@@ -188,7 +253,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     require(o.slice_height == 32, XPLUS_ERR_ARG, "slice_height must be 32");
     require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
     require(o.sigma >= 1, XPLUS_ERR_ARG, "sigma must be >= 1");
-    require(o.restart_on_replace >= -1 && o.restart_on_replace <= 3, XPLUS_ERR_ARG, "restart_on_replace must be -1..3");
+    require(o.restart_on_replace >= -1 && o.restart_on_replace <= 4, XPLUS_ERR_ARG, "restart_on_replace must be -1..4");
     validate_csr(n, row_ptr, col_idx, row_ptr[n]);
     std::vector<double> diag(static_cast<size_t>(n));
     jacobi_diag(n, row_ptr, col_idx, values, diag.data());
@@ -204,11 +269,29 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     const bool split = (o.value_type != XPLUS_F64) && o.row_sum_form;
     require((o.value_type != XPLUS_BF16 && o.value_type != XPLUS_F16) || split, XPLUS_ERR_ARG,
             "16-bit values need row_sum_form");
+    const bool low = o.value_type == XPLUS_BF16 || o.value_type == XPLUS_F16;
+    // FP16 stores a_ij / scale16: the power of two that puts the largest off-diagonal |a_ij|
+    // just below 2^15, inside FP16's range with a ~1e9 dynamic range still normal
+    double scale16 = 1.0;
+    if (o.value_type == XPLUS_F16) {
+        double m = 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+                if (col_idx[k] != i) m = std::max(m, std::fabs(values[k]));
+        scale16 = m > 0.0 ? std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(m))) - 15) : 1.0;
+    }
+    const double split_ratio = o.split_ratio >= 0.0 ? o.split_ratio : (o.value_type == XPLUS_BF16 ? 1.5 : 2.0);
+    TwoTermCsr two;
+    if (low && split_ratio > 0.0) two_term_entries(n, row_ptr, col_idx, values, o.value_type, scale16, split_ratio, two);
+    const bool use_two = !two.row_ptr.empty();
+    const int* rp_s = use_two ? two.row_ptr.data() : row_ptr;
+    const int* ci_s = use_two ? two.col_idx.data() : col_idx;
+    const double* va_s = use_two ? two.values.data() : values;
     SellHost S;
     if (o.build_on_gpu && o.sigma <= 4096)
-        sell_build_via_gpu(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+        sell_build_via_gpu(n, rp_s, ci_s, va_s, 32, o.sigma, o.chunk, split ? 1 : 0, S);
     else
-        sell_build(n, row_ptr, col_idx, values, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+        sell_build(n, rp_s, ci_s, va_s, 32, o.sigma, o.chunk, split ? 1 : 0, S);
 
     auto* h = new xplus_pcg();
     h->device = o.device;
@@ -309,7 +392,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         else
             cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
         cuda_check(cudaMemcpyAsync(h->d_perm, S.perm.data(), S.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
-        h->val_scale = o.value_type == XPLUS_F16 ? f16_scale(S.val) : 1.0;
+        h->val_scale = o.value_type == XPLUS_F16 ? scale16 : 1.0;
         std::vector<unsigned char> vbytes = convert(S.val, o.value_type, h->val_scale);
         cuda_check(cudaMemcpyAsync(h->d_val, vbytes.data(), vbytes.size(), cudaMemcpyHostToDevice, st), "H2D");
         const bool keep64 = o.keep_fp64 != 0 && o.value_type != XPLUS_F64;
@@ -456,7 +539,7 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, int
         a.replace_every = h->opts.replace_every;
         a.replace_drop = h->opts.replace_drop > 0.0 ? h->opts.replace_drop * h->opts.replace_drop : 0.0;
         const bool low = h->opts.value_type == XPLUS_BF16 || h->opts.value_type == XPLUS_F16;
-        a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 3 : 0) : h->opts.restart_on_replace;
+        a.restart_on_replace = h->opts.restart_on_replace < 0 ? (low ? 4 : 0) : h->opts.restart_on_replace;
     }
     cuda_check(cudaMemsetAsync(h->d_bar, 0, sizeof(unsigned), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_err, 0, sizeof(int), st), "memset");
@@ -650,6 +733,7 @@ void xplus_opts_default(xplus_opts* o) {
     o->stagnation_gain = 0.05;
     o->stagnation_window = 8;
     o->build_on_gpu = 1;
+    o->split_ratio = -1.0;
 }
 
 int xplus_device_count(void) {

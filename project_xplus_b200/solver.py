@@ -174,7 +174,7 @@ class PcgSolver:
                  block_threads=0, blocks_per_sm=0, barrier_timeout_s=2.0, device=0,
                  row_sum_form=True, index16=True, l2_persist=True, resident=True,
                  barriers_per_iter=1, restart_on_replace=-1, stagnation_gain=0.05, stagnation_window=8,
-                 build_on_gpu=True):
+                 build_on_gpu=True, split_ratio=-1.0):
         self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
         self.col_idx = np.ascontiguousarray(col_idx, np.int32)
         self.values = np.ascontiguousarray(values, np.float64)
@@ -186,7 +186,8 @@ class PcgSolver:
             barrier_timeout_s=barrier_timeout_s, device=device, row_sum_form=int(row_sum_form), index16=int(index16),
             l2_persist=int(l2_persist), resident=int(resident), barriers_per_iter=int(barriers_per_iter),
             restart_on_replace=int(restart_on_replace), stagnation_gain=float(stagnation_gain),
-            stagnation_window=int(stagnation_window), build_on_gpu=int(build_on_gpu))
+            stagnation_window=int(stagnation_window), build_on_gpu=int(build_on_gpu),
+            split_ratio=float(split_ratio))
         h = C.c_void_p()
         check(lib.xplus_pcg_create(ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), self.n,
                                    C.byref(self.opts), C.byref(h)))

@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
         double rz = tot[0], rr = tot[1], true_rr = tot[2];
         const double bb = tot[3];
         const double tau_true_rr = a.tau * a.tau * bb;
-        double rr_at_replace = rr, zap = 0.0;
+        double rr_at_replace = rr;
         double pap = 0.0, alpha = 0.0, beta = 0.0;
         int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0;
         ReplacePolicy pol(a.restart_on_replace, true_rr);
@@ -329,6 +329,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     break;
                 }
                 bool do_replace = false, drop_replace = false;
+                double zap = 0.0;  // z_new . Ap' of a replacement
                 if (true_mode) {
                     if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                     if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
                     zap = t4[3];
                     ++replacements;
                     rr_at_replace = rr_new;
-                    if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = true;
+                    if (pol.after(a.restart_on_replace, true_rr, a.stag_factor, a.stag_window)) stagnated = true;
                 }
                 rz = rz_new;
                 rr = rr_new;

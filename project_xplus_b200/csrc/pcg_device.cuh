@@ -23,14 +23,14 @@ constexpr double kBreakdownEps = 1.0e-30;  // include/cg_common.hpp:13
 // both drop to mode 1 for the rest of the solve when a replacement finds ||b - A x|| above
 // twice its best (CG's residual is not monotone, so a smaller rise is no signal) or the
 // stagnation window runs out.
+// The policy itself stays in the kernel arguments (read where needed, no register held).
 struct ReplacePolicy {
-    int policy, mode, stagnant;
+    int mode, stagnant;
     double best;
-    __device__ ReplacePolicy(int restart_on_replace, double true_rr)
-        : policy(restart_on_replace), mode(restart_on_replace == 3 ? 2 : restart_on_replace), stagnant(0),
-          best(true_rr) {}
+    __device__ ReplacePolicy(int policy, double true_rr)
+        : mode(policy == 3 ? 2 : policy), stagnant(0), best(true_rr) {}
     // After a replacement that measured true_rr = ||b - A x||^2: true when the solve stagnated.
-    __device__ bool after(double true_rr, double stag_factor, int stag_window) {
+    __device__ bool after(int policy, double true_rr, double stag_factor, int stag_window) {
         if (((policy == 3 && mode == 2) || mode == 4) && true_rr > 4.0 * best) mode = 1;
         if (true_rr < stag_factor * best) {
             best = true_rr;
@@ -46,11 +46,18 @@ struct ReplacePolicy {
         return false;
     }
     // zap = z_new . Ap' (taken by the replacement), pap = p' . Ap' of the iteration
+    // (one division site: a second one would cost the hot loop registers)
     __device__ double beta(bool replaced, bool drop_replaced, double rz, double rz_old, double zap,
                            double pap) const {
-        if (replaced && mode == 4) return -zap / pap;
-        if ((mode == 1 && replaced) || (mode == 2 && drop_replaced)) return 0.0;
-        return rz / rz_old;
+        double num = rz, den = rz_old;
+        if (replaced && mode == 4) {
+            num = -zap;
+            den = pap;
+        } else if ((mode == 1 && replaced) || (mode == 2 && drop_replaced)) {
+            num = 0.0;
+            den = 1.0;
+        }
+        return num / den;
     }
 };
 

@@ -399,9 +399,9 @@ __global__ void __launch_bounds__(512, 1) pcg_gtg_kernel(PcgArgs a) {
                 rr_at_replace = rr_new;
                 if (restart) {
                     // the switch to Jacobi: the refreshed residual is the new reference
-                    if (pol.policy == 3 && pol.mode == 2 && true_rr > 4.0 * pol.best) pol.mode = 1;
+                    if (a.restart_on_replace == 3 && pol.mode == 2 && true_rr > 4.0 * pol.best) pol.mode = 1;
                     pol.best = true_rr;
-                } else if (pol.after(true_rr, a.stag_factor, a.stag_window)) {
+                } else if (pol.after(a.restart_on_replace, true_rr, a.stag_factor, a.stag_window)) {
                     stagnated = 1;
                 }
             }

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
     if (lead) a.out->bb = s_tot[3];
-    double rr_at_replace = rr, zap = 0.0;
+    double rr_at_replace = rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
     ReplacePolicy pol(a.restart_on_replace, true_rr);
@@ -239,6 +239,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
                 break;
             }
             bool do_replace = false, drop_replace = false;
+            double zap = 0.0;  // z_new . Ap' of a replacement
             if (true_mode) {
                 if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
@@ -255,7 +256,7 @@ __global__ void __launch_bounds__(512, 1) pcg_persistent_kernel(PcgArgs a) {
                 zap = s_tot[3];
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
+                if (pol.after(a.restart_on_replace, true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
             }
             if (lead && a.trace && it < a.trace_cap) {
                 double* t = a.trace + 5 * static_cast<size_t>(it);

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
     if (lead) a.out->bb = s_tot[3];
-    double rr_at_replace = rr, zap = 0.0;
+    double rr_at_replace = rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
     ReplacePolicy pol(a.restart_on_replace, true_rr);
@@ -275,6 +275,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 break;
             }
             bool do_replace = false, drop_replace = false;
+            double zap = 0.0;  // z_new . Ap' of a replacement
             if (true_mode) {
                 if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
                 zap = s_tot[3];
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
+                if (pol.after(a.restart_on_replace, true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
             }
             if (lead && a.trace && it < a.trace_cap) {
                 double* t = a.trace + 5 * static_cast<size_t>(it);
@@ -454,8 +455,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             const double rt = bv - y;
             const float r_ = static_cast<float>(rt);
             const float z_ = mi[row - r0] * r_;
-            // slot 3: ||b||^2 in the first pass, z_new . Ap' at a replacement
-            acc[3] += init ? bv * bv : static_cast<double>(z_) * static_cast<double>(apv[row - r0]);
+            if (init) acc[3] += bv * bv;
             rv[row - r0] = r_;
             rec_zr(g)[row] = z_;
             rec_za(g)[row] = 0.0f;
@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
     if (lead) a.out->bb = s_tot[3];
-    double rr_at_replace = rr, zap = 0.0;
+    double rr_at_replace = rr;
     double pap = 0.0, alpha = 0.0, beta = 0.0;
     double pend = 0.0;  // alpha of the update not yet applied to x and r (0: none)
     int status = XPLUS_MAX_ITER, iterations = 0, replacements = 0, stagnated = 0;
@@ -624,6 +624,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 break;
             }
             bool do_replace = false, drop_replace = false;
+            double zap = 0.0;  // z_new . Ap' of a replacement
             if (true_mode) {
                 if (rr_new <= tau_true_rr) do_replace = drop_replace = true;
                 if (a.replace_every > 0 && iterations % a.replace_every == 0) do_replace = true;
@@ -637,15 +638,29 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 if (!bar.sync(&s_flag)) return;
                 residual_phase(false, gen);
                 if (!bar.sync(&s_flag)) return;
-                grid_totals(cur_bank, 4, s_tot);
+                grid_totals(cur_bank, 3, s_tot);
                 clock(4);
                 rz_new = s_tot[0];
                 rr_new = s_tot[1];
                 true_rr = s_tot[2];
-                zap = s_tot[3];
                 ++replacements;
                 rr_at_replace = rr_new;
-                if (pol.after(true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
+                if (pol.after(a.restart_on_replace, true_rr, a.stag_factor, a.stag_window)) stagnated = 1;
+                if (pol.mode == 4) {
+                    // z_new . Ap' for the flexible coefficient: a pass of its own, so the
+                    // residual phase (and the hot loop around it) stays as in the other modes;
+                    // every thread reads back only the records it wrote
+                    double acc[1] = {0.0};
+                    for (int s = sb + warp; s < se; s += wpb) {
+                        const int row = s * 32 + lane;
+                        acc[0] += static_cast<double>(rec_zr(gen)[row]) * static_cast<double>(apv[row - r0]);
+                    }
+                    cur_bank = next_bank();
+                    publish<1>(acc, s_red, cur_bank);
+                    if (!bar.sync(&s_flag)) return;
+                    grid_totals(cur_bank, 1, s_tot);
+                    zap = s_tot[0];
+                }
             }
             if (lead && a.trace && it < a.trace_cap) {
                 double* t = a.trace + 5 * static_cast<size_t>(it);

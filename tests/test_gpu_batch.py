@@ -33,7 +33,7 @@ def _b(batch_systems):
     return np.concatenate([d.b for d, _ in batch_systems])
 
 
-@pytest.mark.parametrize("vt", ["f32", "f16"])
+@pytest.mark.parametrize("vt", ["f32", "f16", "bf16"])
 def test_every_system_converges(gpu, batch_systems, vt):
     s = _make(batch_systems, values_dtype=vt)
     r = s.solve(_b(batch_systems), tau=1e-8)

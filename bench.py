@@ -589,6 +589,33 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
         raise SystemExit(f"batch: {int((r['status'] != 0).sum())} systems did not converge")
     tot = max_over_ranks(pg, sum(ms), dev)
     s.close()
+    # the same batch with BF16 values (the other value type of the batched workload), on the
+    # launch shape tuned for FP32
+    s16 = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems], values_dtype="bf16")
+    s16.set_launch(info["cluster"], info["block_threads"])
+    for _ in range(args.warmup):
+        x.zero_()
+        s16.solve_device(b, x, tau=args.tol, stream=stream)
+        stream.synchronize()
+    ms16 = []
+    clk = Clocks(dev.index, append=True).__enter__()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        x.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s16.solve_device(b, x, tau=args.tol, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms16.append(e0.elapsed_time(e1))
+    clk.__exit__(None, None, None)
+    r16 = s16.results()
+    tot16 = max_over_ranks(pg, sum(ms16), dev)
+    s16.close()
+    bf16 = {"value": len(sides) * args.steps / (tot16 / 1e3), "unit": "systems/s", "ms_per_step": tot16 / args.steps,
+            "converged": int((r16["status"] == 0).sum()), "iterations_total": int(r16["iterations"].sum()),
+            "max_true_rel_residual": float(r16["true_rel"].max())}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = batch_cpu_baseline(systems, [works[k] for k in mine], args.tol)
@@ -601,7 +628,7 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
                           "sum": float(r["system_ms"].sum())},
             "launch": {"cluster": info["cluster"], "block_threads": info["block_threads"], "grid": info["grid"],
                        "autotune_ms": tune["ms"]},
-            "graph": True}
+            "graph": True, "bf16_values": bf16}
 
 
 def main():

@@ -302,7 +302,8 @@ typedef struct xplus_batch xplus_batch;
 
 /* nsys systems, system k given as CSR (row_ptrs[k][ns[k]+1], col_idxs[k], values[k], FP64).
  * opts: value_type F32 | BF16 | F16, vector_type F32, sigma, chunk, index16, replace_drop,
- * replace_every, restart_on_replace, device; the others are ignored.  The launch shape starts
+ * replace_every, restart_on_replace, stagnation_gain, stagnation_window, split_ratio, device;
+ * the others are ignored.  The launch shape starts
  * at clusters of 4 CTAs x 512 threads (xplus_batch_set_launch / xplus_batch_autotune). */
 int xplus_batch_create(int nsys, const int* const* row_ptrs, const int* const* col_idxs,
                        const double* const* values, const int* ns, const xplus_opts* opts,

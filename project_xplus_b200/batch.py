@@ -45,7 +45,7 @@ class BatchSolver:
 
     def __init__(self, systems, *, values_dtype="f32", sigma=256, chunk=4, index16=True,
                  replace_drop=1e-2, replace_every=0, restart_on_replace=-1, stagnation_gain=0.05,
-                 stagnation_window=8, device=0):
+                 stagnation_window=8, split_ratio=-1.0, device=0):
         self.systems = [(np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
                          np.ascontiguousarray(v, np.float64)) for rp, ci, v in systems]
         k = len(self.systems)
@@ -57,7 +57,7 @@ class BatchSolver:
                                       index16=int(index16), replace_drop=replace_drop,
                                       replace_every=replace_every, restart_on_replace=restart_on_replace,
                                       stagnation_gain=stagnation_gain, stagnation_window=stagnation_window,
-                                      device=device)
+                                      split_ratio=float(split_ratio), device=device)
         rps = (C.c_void_p * k)(*[ptr(s[0]) for s in self.systems])
         cis = (C.c_void_p * k)(*[ptr(s[1]) for s in self.systems])
         vs = (C.c_void_p * k)(*[ptr(s[2]) for s in self.systems])

@@ -597,6 +597,8 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
     // per-system SELL images in parallel (row-sum form: off-diagonals in the slots)
     std::vector<SellHost> S(static_cast<size_t>(nsys));
     std::vector<std::vector<double>> diag(static_cast<size_t>(nsys));
+    std::vector<double> scale16(static_cast<size_t>(nsys), 1.0);  // FP16: a_ij / scale16 stored
+    const double split_ratio = split_ratio_of(o);
     std::vector<std::string> errs(static_cast<size_t>(nsys));
     std::vector<int> codes(static_cast<size_t>(nsys), 0);
     {
@@ -611,7 +613,18 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
                         jacobi_diag(ns[k], row_ptrs[k], col_idxs[k], values[k], diag[K].data());
                         for (double d : diag[K])
                             require(std::fabs(d) > 1.0e-30, XPLUS_ERR_DATA, "zero diagonal entry while building Jacobi inverse");
-                        sell_build(ns[k], row_ptrs[k], col_idxs[k], values[k], 32, o.sigma, o.chunk, 1, S[K]);
+                        if (o.value_type == XPLUS_F16)
+                            scale16[K] = f16_offdiag_scale(ns[k], row_ptrs[k], col_idxs[k], values[k]);
+                        // two-term entries for the large weights of cancelling rows (16-bit values)
+                        TwoTermCsr two;
+                        if (split_ratio > 0.0)
+                            two_term_entries(ns[k], row_ptrs[k], col_idxs[k], values[k], o.value_type, scale16[K],
+                                             split_ratio, two);
+                        if (two.row_ptr.empty())
+                            sell_build(ns[k], row_ptrs[k], col_idxs[k], values[k], 32, o.sigma, o.chunk, 1, S[K]);
+                        else
+                            sell_build(ns[k], two.row_ptr.data(), two.col_idx.data(), two.values.data(), 32, o.sigma,
+                                       o.chunk, 1, S[K]);
                     } catch (const Error& e) {
                         codes[static_cast<size_t>(k)] = e.code;
                         errs[static_cast<size_t>(k)] = e.what();
@@ -699,10 +712,7 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
             const int r0 = slice0[K] * 32;
             for (int sl = 0; sl < s.n_slices; ++sl)
                 sp[static_cast<size_t>(slice0[K] + sl)] = b0 + s.slice_ptr[static_cast<size_t>(sl)];
-            double vmax = 0.0;
-            for (double x : s.val) vmax = std::max(vmax, std::fabs(x));
-            const double sc = (o.value_type == XPLUS_F16 && vmax > 0.0)
-                                  ? std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(vmax))) - 15) : 1.0;
+            const double sc = scale16[K];
             scale[K] = static_cast<float>(sc);
             for_each_slot(s, [&](int sl, int lane, int64_t pos) {
                 const size_t gpos = static_cast<size_t>(b0 + pos);

@@ -89,6 +89,27 @@ void sell_build(int n, const int* row_ptr, const int* col_idx, const double* val
 void sell_build_via_gpu(int n, const int* row_ptr, const int* col_idx, const double* values, int C,
                         int sigma, int chunk, int diag_split, SellHost& out);
 
+// 16-bit value storage (xplus_opts.split_ratio): a CSR whose selected off-diagonal entries
+// appear twice in a row, first the value rounded to the 16-bit type, then the remainder
+// a_ij - round(a_ij), exact in FP64, so the two terms sum to a_ij exactly and the second,
+// rounded in turn, carries the bits the first lost.  An entry
+// (i, j) is selected when row i or row j has sum_k |a_ik| / a_ii above `ratio` (a row whose
+// weights of both signs cancel in A, where independent rounding errors of the weights do not
+// cancel and can leave the stored operator indefinite) and |a_ij| is above half the smaller of
+// a_ii and a_jj (the weights whose errors matter there).  Empty when nothing is selected.
+struct TwoTermCsr {
+    std::vector<int> row_ptr, col_idx;
+    std::vector<double> values;
+};
+// type XPLUS_BF16 or XPLUS_F16 (FP16 values are stored divided by `scale`)
+void two_term_entries(int n, const int* row_ptr, const int* col_idx, const double* values, int type,
+                      double scale, double ratio, TwoTermCsr& out);
+// FP16 stores a_ij / scale: the power of two that puts the largest off-diagonal |a_ij| just
+// below 2^15, inside FP16's range with a ~1e9 dynamic range still normal
+double f16_offdiag_scale(int n, const int* row_ptr, const int* col_idx, const double* values);
+// the ratio in effect for these options (0: no two-term entries)
+double split_ratio_of(const xplus_opts& o);
+
 template <typename F>
 void parallel_for(int64_t count, F&& f) {
     const int nt = static_cast<int>(std::max<unsigned>(1u, std::min(32u, std::thread::hardware_concurrency())));

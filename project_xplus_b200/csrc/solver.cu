@@ -84,79 +84,15 @@ struct xplus_pcg {
 };
 
 namespace xplus {
+
 namespace {
-
-void cuda_check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-    }
-}
-
-template <typename T>
-T* dalloc(xplus_pcg* h, size_t count) {
-    void* p = nullptr;
-    const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
-    const cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    }
-    h->allocations.push_back(p);
-    return static_cast<T*>(p);
-}
-
-size_t elem_size(int t) { return t == XPLUS_F64 ? 8 : ((t == XPLUS_BF16 || t == XPLUS_F16) ? 2 : 4); }
-
-void require_device(int device) {
-    int count = 0;
-    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
-        cudaGetLastError();
-        throw Error(XPLUS_ERR_CUDA, "no CUDA device available (the solver has no CPU path)");
-    }
-    require(device >= 0 && device < count, XPLUS_ERR_ARG, "device ordinal out of range");
-    cudaDeviceProp prop;
-    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    require(prop.major == 10, XPLUS_ERR_CUDA, "this build targets sm_100 (B200) devices only");
-    int coop = 0;
-    cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device), "attr");
-    require(coop != 0, XPLUS_ERR_CUDA, "device does not support cooperative launch");
-}
-
-// Converts FP64 values to the storage type into a host byte buffer (FP16: v / scale).
-std::vector<unsigned char> convert(const std::vector<double>& v, int type, double scale = 1.0) {
-    std::vector<unsigned char> out(v.size() * elem_size(type));
-    if (type == XPLUS_F64) {
-        std::memcpy(out.data(), v.data(), out.size());
-    } else if (type == XPLUS_F32) {
-        float* o = reinterpret_cast<float*>(out.data());
-        for (size_t i = 0; i < v.size(); ++i) o[i] = static_cast<float>(v[i]);
-    } else if (type == XPLUS_F16) {
-        __half* o = reinterpret_cast<__half*>(out.data());
-        for (size_t i = 0; i < v.size(); ++i) o[i] = __double2half(v[i] / scale);
-    } else {
-        __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(out.data());
-        for (size_t i = 0; i < v.size(); ++i) o[i] = __double2bfloat16(v[i]);
-    }
-    return out;
-}
-
-// A CSR whose selected off-diagonal entries appear twice in a row: first the value rounded to
-// the 16-bit type, then the remainder a_ij - round(a_ij), exact in FP64, so the two terms sum
-// to a_ij exactly and the second, rounded in turn, carries the bits the first lost.  An entry
-// (i, j) is selected when row i or row j has sum_k |a_ik| / a_ii above `ratio` (a row whose
-// weights of both signs cancel in A, where independent rounding errors of the weights do not
-// cancel and can leave the stored operator indefinite) and |a_ij| is above half the smaller of
-// a_ii and a_jj (the weights whose errors matter there).  Empty when nothing is selected.
-struct TwoTermCsr {
-    std::vector<int> row_ptr, col_idx;
-    std::vector<double> values;
-};
 
 double round16(double v, int type, double scale) {
     if (type == XPLUS_F16) return static_cast<double>(__half2float(__double2half(v / scale))) * scale;
     return static_cast<double>(__bfloat162float(__double2bfloat16(v)));
 }
+
+}  // namespace
 
 void two_term_entries(int n, const int* row_ptr, const int* col_idx, const double* values, int type,
                       double scale, double ratio, TwoTermCsr& out) {
@@ -215,6 +151,80 @@ void two_term_entries(int n, const int* row_ptr, const int* col_idx, const doubl
     });
 }
 
+
+double f16_offdiag_scale(int n, const int* row_ptr, const int* col_idx, const double* values) {
+    double m = 0.0;
+    for (int i = 0; i < n; ++i)
+        for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+            if (col_idx[k] != i) m = std::max(m, std::fabs(values[k]));
+    return m > 0.0 ? std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(m))) - 15) : 1.0;
+}
+
+double split_ratio_of(const xplus_opts& o) {
+    if (o.value_type != XPLUS_BF16 && o.value_type != XPLUS_F16) return 0.0;
+    return o.split_ratio >= 0.0 ? o.split_ratio : (o.value_type == XPLUS_BF16 ? 1.5 : 2.0);
+}
+
+}  // namespace xplus
+
+namespace xplus {
+namespace {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+template <typename T>
+T* dalloc(xplus_pcg* h, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    h->allocations.push_back(p);
+    return static_cast<T*>(p);
+}
+
+size_t elem_size(int t) { return t == XPLUS_F64 ? 8 : ((t == XPLUS_BF16 || t == XPLUS_F16) ? 2 : 4); }
+
+void require_device(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, "no CUDA device available (the solver has no CPU path)");
+    }
+    require(device >= 0 && device < count, XPLUS_ERR_ARG, "device ordinal out of range");
+    cudaDeviceProp prop;
+    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    require(prop.major == 10, XPLUS_ERR_CUDA, "this build targets sm_100 (B200) devices only");
+    int coop = 0;
+    cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device), "attr");
+    require(coop != 0, XPLUS_ERR_CUDA, "device does not support cooperative launch");
+}
+
+// Converts FP64 values to the storage type into a host byte buffer (FP16: v / scale).
+std::vector<unsigned char> convert(const std::vector<double>& v, int type, double scale = 1.0) {
+    std::vector<unsigned char> out(v.size() * elem_size(type));
+    if (type == XPLUS_F64) {
+        std::memcpy(out.data(), v.data(), out.size());
+    } else if (type == XPLUS_F32) {
+        float* o = reinterpret_cast<float*>(out.data());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = static_cast<float>(v[i]);
+    } else if (type == XPLUS_F16) {
+        __half* o = reinterpret_cast<__half*>(out.data());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = __double2half(v[i] / scale);
+    } else {
+        __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(out.data());
+        for (size_t i = 0; i < v.size(); ++i) o[i] = __double2bfloat16(v[i]);
+    }
+    return out;
+}
+
 // Handles that raised the process's persisting-L2 limit, and the limit before the first did:
 // the last one to go restores it.
 std::mutex g_l2_mutex;
@@ -269,20 +279,10 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     const bool split = (o.value_type != XPLUS_F64) && o.row_sum_form;
     require((o.value_type != XPLUS_BF16 && o.value_type != XPLUS_F16) || split, XPLUS_ERR_ARG,
             "16-bit values need row_sum_form");
-    const bool low = o.value_type == XPLUS_BF16 || o.value_type == XPLUS_F16;
-    // FP16 stores a_ij / scale16: the power of two that puts the largest off-diagonal |a_ij|
-    // just below 2^15, inside FP16's range with a ~1e9 dynamic range still normal
-    double scale16 = 1.0;
-    if (o.value_type == XPLUS_F16) {
-        double m = 0.0;
-        for (int i = 0; i < n; ++i)
-            for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
-                if (col_idx[k] != i) m = std::max(m, std::fabs(values[k]));
-        scale16 = m > 0.0 ? std::ldexp(1.0, static_cast<int>(std::ceil(std::log2(m))) - 15) : 1.0;
-    }
-    const double split_ratio = o.split_ratio >= 0.0 ? o.split_ratio : (o.value_type == XPLUS_BF16 ? 1.5 : 2.0);
+    const double scale16 = o.value_type == XPLUS_F16 ? f16_offdiag_scale(n, row_ptr, col_idx, values) : 1.0;
+    const double split_ratio = split_ratio_of(o);
     TwoTermCsr two;
-    if (low && split_ratio > 0.0) two_term_entries(n, row_ptr, col_idx, values, o.value_type, scale16, split_ratio, two);
+    if (split_ratio > 0.0) two_term_entries(n, row_ptr, col_idx, values, o.value_type, scale16, split_ratio, two);
     const bool use_two = !two.row_ptr.empty();
     const int* rp_s = use_two ? two.row_ptr.data() : row_ptr;
     const int* ci_s = use_two ? two.col_idx.data() : col_idx;

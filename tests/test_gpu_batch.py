@@ -140,15 +140,17 @@ def test_launch_shapes_and_autotune(gpu, batch_systems):
     best.close()
 
 
-def test_many_uneven_systems(gpu):
+@pytest.mark.parametrize("vt", ["f32", "bf16"])
+def test_many_uneven_systems(gpu, vt):
     """More systems than clusters, sides log-uniform in [45, 128]: the queue hands out every
-    system exactly once and each converges."""
+    system exactly once and each converges, with FP32 values and with BF16 values (two-term
+    entries in cancelling rows, flexible re-conjugation at replacements)."""
     from project_xplus_b200 import generators as g
     from project_xplus_b200.batch import BatchSolver
     sides, sigmas = g.batch_sides(96, 45, 128, seed=11)
     systems = [g.fem2d(int(sd), sigma=float(sg), seed=100 + k, x_seed=100 + k)[0]
                for k, (sd, sg) in enumerate(zip(sides, sigmas))]
-    s = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems])
+    s = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems], values_dtype=vt)
     r = s.solve(np.concatenate([d.b for d in systems]), tau=1e-8)
     assert np.all(r["status"] == 0) and np.all(r["true_rel"] <= 1e-8)
     assert np.all(r["iterations"] > 0)

@@ -238,7 +238,7 @@ int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double
  * solve applies G^T G as two more sliced SpMVs (no triangular solves) and keeps the FP64
  * residual replacement; Jacobi-PCG takes over inside the same launch when the G^T G solve
  * stagnates or reaches fallback_iters iterations (0: only on stagnation).  Needs FP32 vectors,
- * FP32 or FP16 values, row_sum_form and keep_fp64.  reserved[3] of the metrics holds the
+ * FP32, BF16 or FP16 values, row_sum_form and keep_fp64.  reserved[3] of the metrics holds the
  * iteration of the switch to Jacobi (-1: none).
  * ------------------------------------------------------------------------------------ */
 /* G from host values (g_low NULL: back to Jacobi).  row_ptr / col_idx: the CSR pattern given

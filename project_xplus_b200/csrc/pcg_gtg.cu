@@ -485,6 +485,8 @@ GtgKernel gtg_kernel(const KernelKey& k) {
     switch (k.vt) {
         case XPLUS_F32: return k.idx16 ? gtg_pick_chunk<float, short>(k.chunk) : gtg_pick_chunk<float, int>(k.chunk);
         case XPLUS_F16: return k.idx16 ? gtg_pick_chunk<__half, short>(k.chunk) : gtg_pick_chunk<__half, int>(k.chunk);
+        case XPLUS_BF16:
+            return k.idx16 ? gtg_pick_chunk<__nv_bfloat16, short>(k.chunk) : gtg_pick_chunk<__nv_bfloat16, int>(k.chunk);
     }
     return nullptr;
 }

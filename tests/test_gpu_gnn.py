@@ -228,19 +228,19 @@ def test_trained_network_beats_jacobi(gpu):
 
 
 def test_gtg_with_fp16_values(gpu, sys64):
-    """Mixed precision with the factorized preconditioner: FP16 matrix values (power-of-two
-    scale) in the G^T G kernel reach the FP64 true-residual tolerance, in a number of
+    """Mixed precision with the factorized preconditioner: FP16 (power-of-two scale) and BF16
+    matrix values in the G^T G kernel reach the FP64 true-residual tolerance, in a number of
     iterations close to the FP32-value solve with the same G."""
     from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
     from project_xplus_b200.learned import fsai_lower
     d = sys64
     g = fsai_lower(d.row_ptr, d.col_idx, d.values)
     its = {}
-    for vt in ("f32", "f16"):
+    for vt in ("f32", "f16", "bf16"):
         s = PcgSolver(d.row_ptr, d.col_idx, d.values, values_dtype=vt)
         s.set_gtg(g)
         r = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
         assert r.converged and r.residual_rel <= 1e-8 and r.metrics["kernel"] == "pcg_gtg_kernel", (vt, r.status)
         its[vt] = r.iterations
         s.close()
-    assert its["f16"] <= 2 * its["f32"] + 10, its
+    assert its["f16"] <= 2 * its["f32"] + 10 and its["bf16"] <= 2 * its["f32"] + 10, its

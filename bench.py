@@ -430,11 +430,13 @@ def run_b200(args):
         # the exact FSAI of the same pattern (host), both with the in-kernel Jacobi fallback
         from project_xplus_b200.learned import fsai_lower, load_weights
         params, _ = load_weights()
-        for name in ("learned_gtg", "fsai_gtg"):
+        for name in ("learned_gtg", "learned_gtg_scaled", "fsai_gtg"):
             s3 = xp.PcgSolver.from_dataset(d, device=local)
             t0 = time.perf_counter()
-            if name == "learned_gtg":
+            if name.startswith("learned_gtg"):
                 s3.set_gnn(params)
+                if name == "learned_gtg_scaled":
+                    s3.scale_gtg()  # rows of G normalized to (G A G^T)_ii = 1
             else:
                 s3.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))
             setup_ms = (time.perf_counter() - t0) * 1e3
@@ -450,7 +452,7 @@ def run_b200(args):
             s3.close()
         compare["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / kern_mean
         compare["speedup_vs_fp64"] = compare["fp64"]["time_to_tol_ms"] / kern_mean
-        for name in ("learned_gtg", "fsai_gtg"):
+        for name in ("learned_gtg", "learned_gtg_scaled", "fsai_gtg"):
             compare[name]["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / compare[name]["time_to_tol_ms"]
 
     # CPU baseline: the reference's own golden on a bounded sample, rank 0 only, N=1 only

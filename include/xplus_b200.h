@@ -252,6 +252,11 @@ int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
                       const float* params, int fallback_iters, double* infer_ms);
 /* The handle's current G in g_low order (g_low NULL: only *n_glow). */
 int xplus_pcg_get_gtg(xplus_pcg* h, double* g_low, int64_t* n_glow);
+/* Rescales the rows of the handle's current G (learned or given) to (G A G^T)_ii = 1, the
+ * normalization FSAI carries by construction, from the CSR given to xplus_pcg_create (host,
+ * threaded; G is read back from and written to the device).  XPLUS_ERR_DATA when a row has
+ * (G A G^T)_ii <= 0. */
+int xplus_pcg_scale_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values);
 /* Exact factorized sparse approximate inverse on A's lower pattern (host, no GPU): row i
  * solves A[P_i, P_i] g = e_i over P_i = {j <= i : a_ij != 0}, scaled to (G A G^T)_ii = 1.
  * The non-learned G of the same form, in g_low order. */

@@ -101,6 +101,7 @@ _SIGS = {
     "xplus_pcg_set_gtg": (_i, [_p, _p, _p, _p, _i]),
     "xplus_pcg_set_gnn": (_i, [_p, _p, _p, _p, _p, _i, _dp]),
     "xplus_pcg_get_gtg": (_i, [_p, _p, C.POINTER(_i64)]),
+    "xplus_pcg_scale_gtg": (_i, [_p, _p, _p, _p]),
     "xplus_fsai_lower": (_i, [_i, _p, _p, _p, _p]),
     "xplus_gnn_param_count": (_i, []),
     "xplus_gnn_trainer_create": (_i, [_i, _p, _p, _p, _p, _i, _i, C.POINTER(_p)]),

@@ -1009,6 +1009,63 @@ int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
     });
 }
 
+int xplus_pcg_scale_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values) {
+    return guarded([&] {
+        require(h && row_ptr && col_idx && values, XPLUS_ERR_ARG, "null argument");
+        require(h->gtg && h->d_glow != nullptr, XPLUS_ERR_ARG, "no G set on this handle");
+        const int n = h->n;
+        require(row_ptr[0] == 0 && row_ptr[n] == h->nnz, XPLUS_ERR_ARG, "pattern differs from the matrix of the handle");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        std::vector<double> g(static_cast<size_t>(h->n_glow));
+        cuda_check(cudaMemcpy(g.data(), h->d_glow, g.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        // g_low order: row by row, the entries j <= i of the CSR in their CSR order
+        std::vector<int64_t> g0(static_cast<size_t>(n) + 1, 0);
+        for (int i = 0; i < n; ++i) {
+            int c = 0;
+            for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) c += col_idx[q] <= i;
+            g0[static_cast<size_t>(i) + 1] = g0[static_cast<size_t>(i)] + c;
+        }
+        require(g0[static_cast<size_t>(n)] == h->n_glow, XPLUS_ERR_ARG, "pattern differs from the G of the handle");
+        std::vector<int> bad(static_cast<size_t>(n), 0);
+        parallel_for(n, [&](int64_t b, int64_t e) {
+            std::vector<int> slot(static_cast<size_t>(n), -1);  // column -> position in row i's pattern
+            for (int64_t i = b; i < e; ++i) {
+                const int64_t gb = g0[static_cast<size_t>(i)];
+                int t = 0;
+                for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q)
+                    if (col_idx[q] <= i) slot[static_cast<size_t>(col_idx[q])] = t++;
+                // (G A G^T)_ii = sum over k, l in the pattern of g_ik a_kl g_il
+                double d = 0.0;
+                for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) {
+                    const int k = col_idx[q];
+                    if (k > i) continue;
+                    const double gk = g[static_cast<size_t>(gb + slot[static_cast<size_t>(k)])];
+                    if (gk == 0.0) continue;
+                    double acc = 0.0;
+                    for (int r = row_ptr[k]; r < row_ptr[k + 1]; ++r) {
+                        const int l = col_idx[r];
+                        if (l <= i && slot[static_cast<size_t>(l)] >= 0)
+                            acc += values[r] * g[static_cast<size_t>(gb + slot[static_cast<size_t>(l)])];
+                    }
+                    d += gk * acc;
+                }
+                for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q)
+                    if (col_idx[q] <= i) slot[static_cast<size_t>(col_idx[q])] = -1;
+                if (!(d > 0.0)) {
+                    bad[static_cast<size_t>(i)] = 1;
+                    continue;
+                }
+                const double s = 1.0 / std::sqrt(d);
+                for (int64_t u = gb; u < g0[static_cast<size_t>(i) + 1]; ++u) g[static_cast<size_t>(u)] *= s;
+            }
+        });
+        for (int i = 0; i < n; ++i)
+            require(!bad[static_cast<size_t>(i)], XPLUS_ERR_DATA, "a row of G has (G A G^T)_ii <= 0");
+        cuda_check(cudaMemcpy(h->d_glow, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+        gtg_enable(h, h->g_fallback_iters);
+    });
+}
+
 int xplus_pcg_get_gtg(xplus_pcg* h, double* g_low, int64_t* n_glow) {
     return guarded([&] {
         require(h, XPLUS_ERR_ARG, "null handle");

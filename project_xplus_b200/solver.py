@@ -280,6 +280,10 @@ class PcgSolver:
                                     int(fallback_iters), C.byref(ms)))
         return ms.value
 
+    def scale_gtg(self) -> None:
+        """Rescales the rows of the current G to (G A G^T)_ii = 1."""
+        check(lib.xplus_pcg_scale_gtg(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values)))
+
     def get_gtg(self) -> np.ndarray:
         n = C.c_int64()
         check(lib.xplus_pcg_get_gtg(self._h, None, C.byref(n)))

@@ -244,3 +244,29 @@ def test_gtg_with_fp16_values(gpu, sys64):
         its[vt] = r.iterations
         s.close()
     assert its["f16"] <= 2 * its["f32"] + 10 and its["bf16"] <= 2 * its["f32"] + 10, its
+
+
+def test_scale_gtg_normalizes_rows(gpu):
+    """Row normalization of a learned G to (G A G^T)_ii = 1 (checked on the host in FP64):
+    the held-out system still converges, in no more iterations than with the raw G, and an
+    FSAI G, normalized by construction, is left unchanged."""
+    from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
+    from project_xplus_b200 import generators as gen
+    from project_xplus_b200.learned import fsai_lower, load_weights
+    params, _ = load_weights()
+    d = gen.fem2d(150, sigma=2.0, seed=77, perm_seed=77, rcm=True)[0]
+    A = sp.csr_matrix((d.values, d.col_idx, d.row_ptr), shape=(d.n, d.n))
+    s = PcgSolver(d.row_ptr, d.col_idx, d.values)
+    s.set_gnn(params)
+    raw = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    s.scale_gtg()
+    G = _gmat(d, s.get_gtg())
+    np.testing.assert_allclose((G @ A @ G.T).diagonal(), 1.0, rtol=1e-10)
+    scaled = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+    assert raw.converged and scaled.converged and scaled.residual_rel <= 1e-8
+    assert scaled.iterations <= raw.iterations, (scaled.iterations, raw.iterations)
+    f = fsai_lower(d.row_ptr, d.col_idx, d.values)
+    s.set_gtg(f)
+    s.scale_gtg()
+    np.testing.assert_allclose(s.get_gtg(), f, rtol=1e-12)
+    s.close()

@@ -35,9 +35,9 @@ PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 FP64_CG_ITERATIONS = 5581
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the SM-resident kernel per
-# iteration on the 1108x1108 system: 742.2 MB over a captured launch of 100 iterations
-# (ncu --set full of `python -m project_xplus_b200.profile_case --grid 1108 --iters 100`).
-RESIDENT1_DRAM_BYTES_PER_ITER = 742.2e6 / 100
+# iteration on the 1108x1108 system: 618.5 MB over a captured launch of 100 iterations
+# (ncu --set full of `python -m project_xplus_b200.profile_case --grid 1108 --iters 100 --spmv 5`).
+RESIDENT1_DRAM_BYTES_PER_ITER = 618.5e6 / 100
 
 
 def parse():
@@ -492,7 +492,7 @@ def run_b200(args):
                                      if kernel_name == "pcg_resident1_kernel" and args.grid == 1108 else None),
                          "traffic_note": "ncu DRAM bytes of a 100-iteration capture of this kernel on this system, "
                                          "scaled by the iterations of one launch; the matrix stays in L2 and the "
-                                         "vectors in shared memory, so traffic is ~6% of the streaming model",
+                                         "vectors in shared memory, so traffic is ~5% of the streaming model",
                          "kernel": f"{kernel_name}<float,4,short> (FP32 values + vectors, row-sum form)",
                          "bytes_model": "8*nnz + 52*n per iteration (FP32 PCG) + 12*nnz + 28*n per FP64 residual",
                          "peak_kind": hbm_kind,

@@ -10,69 +10,110 @@ namespace xplus {
 namespace dev {
 
 // ---------------------------------------------------------------------------------------
+// Read-only loads of the matrix stream: through L1 (__ldg), or with NA set past it
+// (ld.global.nc.L1::no_allocate), so a kernel that streams the matrix once per iteration
+// keeps its L1 for the neighbour records it gathers again and again.
+__device__ __forceinline__ float ld_na(const float* p) {
+    float v; asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p)); return v; }
+__device__ __forceinline__ float2 ld_na(const float2* p) {
+    float2 v; asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p)); return v; }
+__device__ __forceinline__ float4 ld_na(const float4* p) {
+    float4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_na(const double* p) {
+    double v; asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p)); return v; }
+__device__ __forceinline__ double2 ld_na(const double2* p) {
+    double2 v; asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p)); return v; }
+__device__ __forceinline__ int ld_na(const int* p) {
+    int v; asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p)); return v; }
+__device__ __forceinline__ int2 ld_na(const int2* p) {
+    int2 v; asm volatile("ld.global.nc.L1::no_allocate.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p)); return v; }
+__device__ __forceinline__ int4 ld_na(const int4* p) {
+    int4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ unsigned int ld_na(const unsigned int* p) {
+    unsigned int v; asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p)); return v; }
+__device__ __forceinline__ uint2 ld_na(const uint2* p) {
+    uint2 v; asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p)); return v; }
+__device__ __forceinline__ unsigned short ld_na(const unsigned short* p) {
+    unsigned short v; asm volatile("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p)); return v; }
+__device__ __forceinline__ short ld_na(const short* p) {
+    short v; asm volatile("ld.global.nc.L1::no_allocate.s16 %0, [%1];" : "=h"(v) : "l"(p)); return v; }
+template <bool NA, typename T>
+__device__ __forceinline__ T ldro(const T* p) {
+    if constexpr (NA) return ld_na(p);
+    else return __ldg(p);
+}
+
 // Matrix chunk loads: CHUNK consecutive slots of one row, as one vector load through the
 // read-only path (the matrix never changes inside a kernel).
 // ---------------------------------------------------------------------------------------
-template <typename VT, int CHUNK>
+template <typename VT, int CHUNK, bool NA = false>
 struct ChunkLoad;
 
-template <>
-struct ChunkLoad<float, 1> {
-    static __device__ __forceinline__ void run(const float* p, float* o) { o[0] = __ldg(p); }
+template <bool NA>
+struct ChunkLoad<float, 1, NA> {
+    static __device__ __forceinline__ void run(const float* p, float* o) { o[0] = ldro<NA>(p); }
 };
-template <>
-struct ChunkLoad<float, 2> {
+template <bool NA>
+struct ChunkLoad<float, 2, NA> {
     static __device__ __forceinline__ void run(const float* p, float* o) {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+        const float2 v = ldro<NA>(reinterpret_cast<const float2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
-template <>
-struct ChunkLoad<float, 4> {
+template <bool NA>
+struct ChunkLoad<float, 4, NA> {
     static __device__ __forceinline__ void run(const float* p, float* o) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+        const float4 v = ldro<NA>(reinterpret_cast<const float4*>(p));
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
     }
 };
-template <>
-struct ChunkLoad<double, 1> {
-    static __device__ __forceinline__ void run(const double* p, double* o) { o[0] = __ldg(p); }
+template <bool NA>
+struct ChunkLoad<double, 1, NA> {
+    static __device__ __forceinline__ void run(const double* p, double* o) { o[0] = ldro<NA>(p); }
 };
-template <>
-struct ChunkLoad<double, 2> {
+template <bool NA>
+struct ChunkLoad<double, 2, NA> {
     static __device__ __forceinline__ void run(const double* p, double* o) {
-        const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 v = ldro<NA>(reinterpret_cast<const double2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
-template <>
-struct ChunkLoad<double, 4> {
+template <bool NA>
+struct ChunkLoad<double, 4, NA> {
     static __device__ __forceinline__ void run(const double* p, double* o) {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
-        const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+        const double2 a = ldro<NA>(reinterpret_cast<const double2*>(p));
+        const double2 b = ldro<NA>(reinterpret_cast<const double2*>(p + 2));
         o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
     }
 };
 __device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
-template <>
-struct ChunkLoad<__nv_bfloat16, 1> {
+template <bool NA>
+struct ChunkLoad<__nv_bfloat16, 1, NA> {
     static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
-        const unsigned short v = __ldg(reinterpret_cast<const unsigned short*>(p));
+        const unsigned short v = ldro<NA>(reinterpret_cast<const unsigned short*>(p));
         o[0] = __uint_as_float(static_cast<uint32_t>(v) << 16);
     }
 };
-template <>
-struct ChunkLoad<__nv_bfloat16, 2> {
+template <bool NA>
+struct ChunkLoad<__nv_bfloat16, 2, NA> {
     static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
-        const uint32_t v = __ldg(reinterpret_cast<const unsigned int*>(p));
+        const uint32_t v = ldro<NA>(reinterpret_cast<const unsigned int*>(p));
         o[0] = bf16_lo(v); o[1] = bf16_hi(v);
     }
 };
-template <>
-struct ChunkLoad<__nv_bfloat16, 4> {
+template <bool NA>
+struct ChunkLoad<__nv_bfloat16, 4, NA> {
     static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
-        const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+        const uint2 v = ldro<NA>(reinterpret_cast<const uint2*>(p));
         o[0] = bf16_lo(v.x); o[1] = bf16_hi(v.x); o[2] = bf16_lo(v.y); o[3] = bf16_hi(v.y);
     }
 };
@@ -83,66 +124,66 @@ __device__ __forceinline__ float f16_lo(uint32_t w) {
 __device__ __forceinline__ float f16_hi(uint32_t w) {
     return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
 }
-template <>
-struct ChunkLoad<__half, 1> {
+template <bool NA>
+struct ChunkLoad<__half, 1, NA> {
     static __device__ __forceinline__ void run(const __half* p, float* o) {
-        o[0] = __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p))));
+        o[0] = __half2float(__ushort_as_half(ldro<NA>(reinterpret_cast<const unsigned short*>(p))));
     }
 };
-template <>
-struct ChunkLoad<__half, 2> {
+template <bool NA>
+struct ChunkLoad<__half, 2, NA> {
     static __device__ __forceinline__ void run(const __half* p, float* o) {
-        const uint32_t v = __ldg(reinterpret_cast<const unsigned int*>(p));
+        const uint32_t v = ldro<NA>(reinterpret_cast<const unsigned int*>(p));
         o[0] = f16_lo(v); o[1] = f16_hi(v);
     }
 };
-template <>
-struct ChunkLoad<__half, 4> {
+template <bool NA>
+struct ChunkLoad<__half, 4, NA> {
     static __device__ __forceinline__ void run(const __half* p, float* o) {
-        const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+        const uint2 v = ldro<NA>(reinterpret_cast<const uint2*>(p));
         o[0] = f16_lo(v.x); o[1] = f16_hi(v.x); o[2] = f16_lo(v.y); o[3] = f16_hi(v.y);
     }
 };
 
 // Column loads: absolute int32 columns, or int16 offsets from the row (lossless when the
 // bandwidth of the ordered matrix is below 32768) returned as absolute columns.
-template <int CHUNK, typename IT>
+template <int CHUNK, typename IT, bool NA = false>
 struct ColLoad;
-template <>
-struct ColLoad<1, int> {
-    static __device__ __forceinline__ void run(const int* p, int, int* o) { o[0] = __ldg(p); }
+template <bool NA>
+struct ColLoad<1, int, NA> {
+    static __device__ __forceinline__ void run(const int* p, int, int* o) { o[0] = ldro<NA>(p); }
 };
-template <>
-struct ColLoad<2, int> {
+template <bool NA>
+struct ColLoad<2, int, NA> {
     static __device__ __forceinline__ void run(const int* p, int, int* o) {
-        const int2 v = __ldg(reinterpret_cast<const int2*>(p));
+        const int2 v = ldro<NA>(reinterpret_cast<const int2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
-template <>
-struct ColLoad<4, int> {
+template <bool NA>
+struct ColLoad<4, int, NA> {
     static __device__ __forceinline__ void run(const int* p, int, int* o) {
-        const int4 v = __ldg(reinterpret_cast<const int4*>(p));
+        const int4 v = ldro<NA>(reinterpret_cast<const int4*>(p));
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
     }
 };
 __device__ __forceinline__ int lo16(uint32_t w) { return static_cast<int>(static_cast<short>(w & 0xFFFFu)); }
 __device__ __forceinline__ int hi16(uint32_t w) { return static_cast<int>(static_cast<short>(w >> 16)); }
-template <>
-struct ColLoad<1, short> {
-    static __device__ __forceinline__ void run(const short* p, int row, int* o) { o[0] = row + __ldg(p); }
+template <bool NA>
+struct ColLoad<1, short, NA> {
+    static __device__ __forceinline__ void run(const short* p, int row, int* o) { o[0] = row + ldro<NA>(p); }
 };
-template <>
-struct ColLoad<2, short> {
+template <bool NA>
+struct ColLoad<2, short, NA> {
     static __device__ __forceinline__ void run(const short* p, int row, int* o) {
-        const uint32_t v = __ldg(reinterpret_cast<const unsigned int*>(p));
+        const uint32_t v = ldro<NA>(reinterpret_cast<const unsigned int*>(p));
         o[0] = row + lo16(v); o[1] = row + hi16(v);
     }
 };
-template <>
-struct ColLoad<4, short> {
+template <bool NA>
+struct ColLoad<4, short, NA> {
     static __device__ __forceinline__ void run(const short* p, int row, int* o) {
-        const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+        const uint2 v = ldro<NA>(reinterpret_cast<const uint2*>(p));
         o[0] = row + lo16(v.x); o[1] = row + hi16(v.x); o[2] = row + lo16(v.y); o[3] = row + hi16(v.y);
     }
 };

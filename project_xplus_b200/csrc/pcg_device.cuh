@@ -203,7 +203,8 @@ __device__ __forceinline__ void store_rec(NodeRec<double>* q, double z, double p
 
 // NS slices of one warp at a time (lane = row within each): for every pair of chunks, the
 // value/column loads of all NS rows are issued, then all their neighbour-record gathers,
-// then the arithmetic -- so NS * 2 * CHUNK gathers per thread are in flight together.
+// then the arithmetic -- so NS * 2 * CHUNK gathers per thread are in flight together.  The slot
+// loads bypass L1 (the matrix streams once per iteration); the record gathers keep it.
 // Returns y_k = (A p')_row_k without the row-sum term; pi[k] = p'_row_k.
 template <typename VT, int CHUNK, bool DIFF, typename IT, typename XT, int NS>
 __device__ __forceinline__ void sell_rows_pnew(const int2 (&sl)[NS], const int (&row)[NS], int lane,
@@ -225,8 +226,8 @@ __device__ __forceinline__ void sell_rows_pnew(const int2 (&sl)[NS], const int (
             for (int h = 0; h < 2; ++h) {
                 if (c + h * CHUNK < sl[k].y) {
                     const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
-                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
-                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                    ChunkLoad<VT, CHUNK, true>::run(val + off, v[k][h]);
+                    ColLoad<CHUNK, IT, true>::run(col + off, row[k], cc[k][h]);
                 } else {
 #pragma unroll
                     for (int q = 0; q < CHUNK; ++q) {

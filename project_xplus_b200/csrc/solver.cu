@@ -805,7 +805,10 @@ int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau,
 int xplus_pcg_last_trace(xplus_pcg* h, double* trace, int rows) {
     return guarded([&] {
         require(h && trace && rows > 0 && rows <= h->trace_cap, XPLUS_ERR_ARG, "bad trace request");
-        cuda_check(cudaMemcpy(trace, h->d_trace, static_cast<size_t>(rows) * 5 * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        collect(h, nullptr);  // waits for a pending solve
+        cuda_check(cudaMemcpyAsync(trace, h->d_trace, static_cast<size_t>(rows) * 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                   h->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(h->stream), "sync");
     });
 }
 
@@ -1016,8 +1019,11 @@ int xplus_pcg_scale_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, co
         const int n = h->n;
         require(row_ptr[0] == 0 && row_ptr[n] == h->nnz, XPLUS_ERR_ARG, "pattern differs from the matrix of the handle");
         cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        // every copy on the handle's stream: it is a non-blocking stream, so a copy on the legacy
+        // stream would not be ordered with the fill kernels that read d_glow
         std::vector<double> g(static_cast<size_t>(h->n_glow));
-        cuda_check(cudaMemcpy(g.data(), h->d_glow, g.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        cuda_check(cudaMemcpyAsync(g.data(), h->d_glow, g.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(h->stream), "sync");
         // g_low order: row by row, the entries j <= i of the CSR in their CSR order
         std::vector<int64_t> g0(static_cast<size_t>(n) + 1, 0);
         for (int i = 0; i < n; ++i) {
@@ -1061,8 +1067,8 @@ int xplus_pcg_scale_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, co
         });
         for (int i = 0; i < n; ++i)
             require(!bad[static_cast<size_t>(i)], XPLUS_ERR_DATA, "a row of G has (G A G^T)_ii <= 0");
-        cuda_check(cudaMemcpy(h->d_glow, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
-        gtg_enable(h, h->g_fallback_iters);
+        cuda_check(cudaMemcpyAsync(h->d_glow, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream), "H2D");
+        gtg_enable(h, h->g_fallback_iters);  // fills G and G^T on the same stream, then waits
     });
 }
 
@@ -1072,7 +1078,9 @@ int xplus_pcg_get_gtg(xplus_pcg* h, double* g_low, int64_t* n_glow) {
         if (n_glow) *n_glow = h->n_glow;
         if (!g_low) return;
         require(h->d_glow != nullptr, XPLUS_ERR_ARG, "no G set on this handle");
-        cuda_check(cudaMemcpy(g_low, h->d_glow, static_cast<size_t>(h->n_glow) * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+        cuda_check(cudaMemcpyAsync(g_low, h->d_glow, static_cast<size_t>(h->n_glow) * sizeof(double), cudaMemcpyDeviceToHost,
+                                   h->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(h->stream), "sync");
     });
 }
 

@@ -54,7 +54,12 @@ def parse():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison solves")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched solve")
     ap.add_argument("--no-spmv3d", action="store_true", help="skip the SpMV on the 128^3 3D system")
-    return ap.parse_args()
+    ap.add_argument("--clocks-dir", default=None,
+                    help="directory for the nvidia-smi clock samples (default: a temporary directory)")
+    a = ap.parse_args()
+    if a.clocks_dir:
+        Clocks.out_dir = Path(a.clocks_dir)
+    return a
 
 
 def peaks():
@@ -81,15 +86,20 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    out_dir = None  # --clocks-dir, else a fresh temporary directory per process
+
     def __init__(self, device_index, append=False):
         self.dev = device_index
         self.proc = None
         self.append = append
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{device_index}.csv"
+        if Clocks.out_dir is None:
+            import tempfile
+            Clocks.out_dir = Path(tempfile.mkdtemp(prefix="xplus_bench_clocks_"))
+        self.path = Path(Clocks.out_dir) / f"clocks_rank{device_index}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.f = open(self.path, "a" if self.append else "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],

@@ -182,7 +182,9 @@ int xplus_pcg_solve(xplus_pcg* h, const double* b, const double* x0, double tau,
  * `stream` (a cudaStream_t, NULL = the handle's stream) without waiting for the device: the
  * relative tolerance is scaled by ||b||^2 summed inside the kernel, so b may be produced by
  * earlier work on the same stream.  d_x holds x0 on entry and x on exit.  Fetch the outcome
- * with xplus_pcg_last_metrics() (which waits for the solve). */
+ * with xplus_pcg_last_metrics() (which waits for the solve).  d_b and d_x must be device (or
+ * managed) memory of the handle's GPU: host or other-GPU pointers return XPLUS_ERR_ARG before
+ * anything is enqueued. */
 int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double tau,
                            int tau_mode, int max_iters, void* stream);
 int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);
@@ -331,7 +333,8 @@ int xplus_batch_solve(xplus_batch* h, const double* b, const double* x0, double 
 /* Asynchronous solve on device vectors (d_x: x0 in, x out) enqueued on `stream` (NULL: the
  * handle's stream) as one CUDA graph (gather, persistent launch, scatter).  The graph is
  * captured on the first call and replayed while d_b, d_x, tau, tau_mode, max_iters and the
- * launch shape stay the same. */
+ * launch shape stay the same.  d_b and d_x must be device (or managed) memory of the
+ * handle's GPU: host or other-GPU pointers return XPLUS_ERR_ARG before anything is enqueued. */
 int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, double tau, int tau_mode,
                              int max_iters, void* stream);
 /* Outcome of the last solve, per system (each array nullable, nsys long): status, inner
@@ -374,8 +377,14 @@ void update_p_kernel(const double* z, double* p, double beta, int n);
  * updated as update_xrz_kernel updates them, and metrics[0..1] = {r.z, r.r} is written on
  * the device.  The call is asynchronous on `stream` (a cudaStream_t; NULL = the legacy
  * default stream).
+ *   - Every pointer must be device memory of the current device (or managed memory).
+ *     Host arrays, which update_xrz_kernel accepts and stages, and another GPU's memory
+ *     return XPLUS_ERR_ARG with a message before anything is launched.
  *   - The first call on each device looks the scratch array's device address up with
- *     cudaGetSymbolAddress; make that first call before any stream capture.
+ *     cudaGetSymbolAddress (again after the device's context was reset); make that first
+ *     call before any stream capture.
+ *   - An error left pending on the calling thread by earlier asynchronous work is reported
+ *     as XPLUS_ERR_CUDA, left in place for its owner, and nothing is launched.
  *   - All calls share the one scratch array, which keeps the last call's contents: calls
  *     that overlap on the GPU (other streams, other host threads) race; serialize them.
  *   - n may be at most XPLUS_NOALLOC_MAX_N (1024 reduction blocks x 256 threads x 16

@@ -7,6 +7,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -15,13 +16,34 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 C_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libxplus_ref.so"
+# the reference's multi-kernel host program relinked against libxplus_b200.so (oracle/Makefile relink)
+RELINKED_HOST = HERE / "_ref" / "xplus_host_b200"
+
+
+# Where the reference checkout lies in the build container; XPLUS_REFERENCE_TREE overrides it.
+# Only this build step reads the tree: tests and benchmarks load the prebuilt _ref library.
+_REFERENCE_CHECKOUT = "/root/reference"
+
+
+def reference_tree() -> Path | None:
+    """The reference tree to compile from: $XPLUS_REFERENCE_TREE when set (it must then hold
+    the reference's src/), else the build container's checkout when present, else None."""
+    env = os.environ.get("XPLUS_REFERENCE_TREE")
+    if env:
+        if not (Path(env) / "src").is_dir():
+            raise FileNotFoundError(f"XPLUS_REFERENCE_TREE={env} does not hold the reference's src/")
+        return Path(env)
+    return Path(_REFERENCE_CHECKOUT) if (Path(_REFERENCE_CHECKOUT) / "src").is_dir() else None
 
 
 def build(ref: bool = True) -> None:
-    """Compiles liboracle.so, and the reference library when the reference tree exists."""
+    """Compiles liboracle.so, and the reference library when a reference tree is available."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if ref and Path("/root/reference/src").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    tree = reference_tree() if ref else None
+    if tree is not None:
+        subprocess.run(["make", "-s", "-C", str(HERE), f"REF={tree}", "ref"], check=True)
+        if (HERE.parent / "project_xplus_b200" / "lib" / "libxplus_b200.so").exists():
+            subprocess.run(["make", "-s", "-C", str(HERE), f"REF={tree}", "relink"], check=True)
 
 
 def _p(a):

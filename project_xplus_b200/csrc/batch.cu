@@ -933,6 +933,8 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
         require(h && d_b && d_x, XPLUS_ERR_ARG, "null argument");
         check_tau(tau, tau_mode);
         bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        require_device_memory(d_b, h->device, "d_b");
+        require_device_memory(d_x, h->device, "d_x");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
         const bool same = h->gexec && h->g_b == d_b && h->g_x == d_x && h->g_tau == tau && h->g_mode == tau_mode &&
                           h->g_iters == max_iters && h->g_cluster == h->cluster && h->g_tpb == h->tpb;

@@ -53,6 +53,16 @@ inline void require(bool cond, int code, const char* msg) {
 template <typename F>
 void parallel_for(int64_t count, F&& f);
 
+// Device-pointer arguments of the entry points that launch on caller memory (*_solve_device,
+// *_noalloc): p must be device memory of `device` or managed memory.  Host memory (pageable or
+// pinned) and another GPU's memory are rejected with XPLUS_ERR_ARG before anything is launched,
+// so a wrong pointer is an error code, not a GPU fault.  (multikernel.cu)
+void require_device_memory(const void* p, int device, const char* what);
+// Throws XPLUS_ERR_CUDA if earlier asynchronous work left an error pending on this thread.  The
+// error is left in place (cudaPeekAtLastError) for its owner, and the calling entry point
+// launches nothing, so a later launch check reports only the entry point's own launches.
+void require_no_pending_cuda_error(const char* entry);
+
 // CSR structure checks of src/CsrDataset.hpp:29-52, same messages.
 void validate_csr(int n, const int* row_ptr, const int* col_idx, int64_t nnz_expected);
 

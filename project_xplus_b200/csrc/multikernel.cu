@@ -9,6 +9,7 @@
 // a fixed two-level tree (deterministic, within a few ulps of the sequential sum).
 // Pointers may be device pointers or plain host pointers (staged).  Calls block until the
 // results are in place, as the reference's calls do.
+#include <cuda.h>  // CUcontext only: cuCtxGetCurrent is reached through cudaGetDriverEntryPoint
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -153,6 +154,33 @@ bool device_accessible(const void* p, const void** dev) {
     return false;
 }
 
+}  // namespace
+
+void require_device_memory(const void* p, int device, const char* what) {
+    cudaPointerAttributes attr;
+    const cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // this call's own error
+        throw Error(XPLUS_ERR_ARG, std::string(what) + ": not a pointer CUDA knows (" + cudaGetErrorString(e) + ")");
+    }
+    if (attr.type == cudaMemoryTypeManaged) return;
+    if (attr.type != cudaMemoryTypeDevice)
+        throw Error(XPLUS_ERR_ARG, std::string(what) + ": host memory; this entry point takes device memory of GPU " +
+                                       std::to_string(device));
+    if (attr.device != device)
+        throw Error(XPLUS_ERR_ARG, std::string(what) + ": memory of GPU " + std::to_string(attr.device) +
+                                       ", not of GPU " + std::to_string(device));
+}
+
+void require_no_pending_cuda_error(const char* entry) {
+    const cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        throw Error(XPLUS_ERR_CUDA, std::string(entry) + ": an earlier CUDA error is pending on this thread (" +
+                                        cudaGetErrorString(e) + "); nothing was launched");
+}
+
+namespace {
+
 // One argument of a call: device view of a caller pointer, copied in/out when staged.
 struct Arg {
     void* host = nullptr;
@@ -214,6 +242,7 @@ int nnz_of(Context& c, const int* row_ptr, int n) {
 
 void run_spmv(const int* row_ptr, const int* col_idx, const double* values, const double* x,
               double* y, int n) {
+    require_no_pending_cuda_error("spmv_csr_kernel");
     Context& c = ctx();
     std::lock_guard<std::mutex> g(c.mu);
     ensure_ready(c);
@@ -239,19 +268,41 @@ constexpr int kNoallocBlocks = 1024;
 static __device__ __align__(256) double g_noalloc_partial[2 * kNoallocBlocks];
 static_assert(kNoallocBlocks >= kMaxBlocks, "blocks_for() may use up to kMaxBlocks blocks");
 
-// Device address of g_noalloc_partial on the current device, looked up once per device.
-// In host code the symbol is only a host-side stand-in, so the kernels get this address.
+// The current context, through the driver entry point (the library links only the runtime).
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return reinterpret_cast<Fn>(f);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) throw Error(XPLUS_ERR_CUDA, "cuCtxGetCurrent is not available");
+    return c;
+}
+
+// Device address of g_noalloc_partial in the current context.  In host code the symbol is
+// only a host-side stand-in, so the kernels get this address.  It is looked up again whenever
+// the device's context changed (after cudaDeviceReset the old address is stale).
 double* noalloc_scratch() {
     static std::mutex mu;
+    static CUcontext ctx_of[64] = {};
     static double* addr[64] = {};
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev < 0 || dev >= 64) throw Error(XPLUS_ERR_ARG, "device ordinal out of range");
+    const CUcontext cur = current_context();
     std::lock_guard<std::mutex> g(mu);
-    if (!addr[dev]) {
+    if (!addr[dev] || ctx_of[dev] != cur) {
         void* p = nullptr;
         check(cudaGetSymbolAddress(&p, g_noalloc_partial), "cudaGetSymbolAddress");
         addr[dev] = static_cast<double*>(p);
+        ctx_of[dev] = cur;
     }
     return addr[dev];
 }
@@ -287,6 +338,7 @@ void init_pcg_kernel(const double* b, const double* ax, const double* m_inv, dou
                      double* p, double* metrics, int n) {
     if (n < 0) return;
     abi_call([&] {
+        require_no_pending_cuda_error("init_pcg_kernel");
         Context& c = ctx();
         std::lock_guard<std::mutex> g(c.mu);
         ensure_ready(c);
@@ -310,6 +362,7 @@ void init_pcg_kernel(const double* b, const double* ax, const double* m_inv, dou
 void dot_kernel(const double* a, const double* b, double* out, int n) {
     if (n < 0) return;
     abi_call([&] {
+        require_no_pending_cuda_error("dot_kernel");
         Context& c = ctx();
         std::lock_guard<std::mutex> g(c.mu);
         ensure_ready(c);
@@ -331,6 +384,7 @@ void update_xrz_kernel(double* x, const double* p, double* r, const double* ap,
                        const double* m_inv, double* z, double* metrics, double alpha, int n) {
     if (n < 0) return;
     abi_call([&] {
+        require_no_pending_cuda_error("update_xrz_kernel");
         Context& c = ctx();
         std::lock_guard<std::mutex> g(c.mu);
         ensure_ready(c);
@@ -359,19 +413,35 @@ int xplus_update_xrz_noalloc(double* x, const double* p, double* r, const double
                 "n exceeds the no-allocation limit of " + std::to_string(XPLUS_NOALLOC_MAX_N) + " rows");
         require(metrics != nullptr && (n == 0 || (x && p && r && ap && m_inv && z)), XPLUS_ERR_ARG,
                 "null argument");
+        require_no_pending_cuda_error("xplus_update_xrz_noalloc");
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        // every pointer must be memory the kernels can address on this device: a host array
+        // (which update_xrz_kernel would stage) is an argument error here, not a GPU fault
+        require_device_memory(metrics, dev, "metrics");
+        if (n > 0) {
+            require_device_memory(x, dev, "x");
+            require_device_memory(p, dev, "p");
+            require_device_memory(r, dev, "r");
+            require_device_memory(ap, dev, "ap");
+            require_device_memory(m_inv, dev, "m_inv");
+            require_device_memory(z, dev, "z");
+        }
         double* scratch = noalloc_scratch();
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         // at most kNoallocBlocks blocks, so the partials fit the fixed scratch
         const int blocks = blocks_for(n);
         vec_kernel<<<blocks, kThreads, 0, st>>>(2, n, alpha, x, p, r, ap, m_inv, z, nullptr, nullptr, scratch);
-        finish_kernel<<<1, kThreads, 0, st>>>(scratch, blocks, metrics, 2);
         check(cudaGetLastError(), "update_xrz_noalloc launch");
+        finish_kernel<<<1, kThreads, 0, st>>>(scratch, blocks, metrics, 2);
+        check(cudaGetLastError(), "update_xrz_noalloc finish launch");
     });
 }
 
 void update_p_kernel(const double* z, double* p, double beta, int n) {
     if (n <= 0) return;
     abi_call([&] {
+        require_no_pending_cuda_error("update_p_kernel");
         Context& c = ctx();
         std::lock_guard<std::mutex> g(c.mu);
         ensure_ready(c);

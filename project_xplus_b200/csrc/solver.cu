@@ -817,6 +817,8 @@ int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double 
     return guarded([&] {
         require(h && d_b && d_x, XPLUS_ERR_ARG, "null argument");
         cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        require_device_memory(d_b, h->device, "d_b");
+        require_device_memory(d_x, h->device, "d_x");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
         cuda_check(gather_to_sell(XPLUS_F64, d_b, h->d_b64, h->d_perm, h->n, h->n_pad, st), "gather");
         cuda_check(gather_to_sell(XPLUS_F64, d_x, h->d_x64, h->d_perm, h->n, h->n_pad, st), "gather");

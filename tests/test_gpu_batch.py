@@ -113,6 +113,23 @@ def test_device_graph_path(gpu, batch_systems):
         np.testing.assert_array_equal(d_x.cpu().numpy(), host["x"])  # deterministic
 
 
+def test_device_graph_path_rejects_host_pointers(gpu, batch_systems):
+    """xplus_batch_solve_device: host arrays are an argument error, before any capture."""
+    import torch
+    from project_xplus_b200 import XplusError
+    from project_xplus_b200._lib import XPLUS_ERR_ARG
+    s = _make(batch_systems)
+    b = _b(batch_systems)
+    with pytest.raises(XplusError) as e:
+        s.solve_device(b, np.zeros_like(b), tau=1e-8)
+    assert e.value.code == XPLUS_ERR_ARG and "host memory" in str(e.value)
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros_like(d_b)
+    s.solve_device(d_b, d_x, tau=1e-8)
+    torch.cuda.synchronize()
+    assert list(s.results()["status"]) == [0] * len(SPECS)
+
+
 def test_launch_shapes_and_autotune(gpu, batch_systems):
     from project_xplus_b200 import XplusError
     from project_xplus_b200.batch import autotune_build

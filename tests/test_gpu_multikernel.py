@@ -101,3 +101,28 @@ def test_multi_kernel_host_loop_on_gpu(gpu, oracle):
     ref = oracle.multi_kernel(d, tau)
     assert abs(it - ref["iterations"]) <= 1
     assert np.linalg.norm(x - ref["x"]) <= 1e-9 * np.linalg.norm(ref["x"])
+
+
+@pytest.mark.ref
+@pytest.mark.parametrize("spmv", ["csr", "blocked"])
+def test_reference_host_relinked_against_the_library(gpu, oracle, tmp_path, spmv):
+    """Drop-in check of the five C entry points: the reference's own multi-kernel host program
+    (archived/host/main.cpp, built by oracle/Makefile `relink` from the reference's sources with
+    libxplus_b200.so in place of archived/kernels/cg_kernels.cpp) runs on the n = 1024 system
+    written in the reference's text format.  Exit code 0 means it converged and its own check
+    against the CPU golden (max_abs_diff <= 1e-9, archived/host/main.cpp:139-141) passed."""
+    import re
+    import subprocess
+    if not oracle.RELINKED_HOST.exists():
+        pytest.skip("oracle/_ref/xplus_host_b200 not built (reference tree absent at build time)")
+    d, _ = g.system_2d_small()
+    d.save_text(tmp_path / "ds")
+    r = subprocess.run([str(oracle.RELINKED_HOST), str(tmp_path / "ds"), "--spmv", spmv],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout[-2000:], r.stderr[-2000:])
+    done = re.search(r"\[done\] iter=(\d+) .* status=(\w+)", r.stdout)
+    check = re.search(r"max_abs_diff=([0-9.eE+-]+)", r.stdout)
+    assert done and check, r.stdout[-2000:]
+    ref = oracle.multi_kernel(d, 1e-10, use_ref=True)
+    assert abs(int(done.group(1)) - ref["iterations"]) <= 1
+    assert float(check.group(1)) <= 1e-9

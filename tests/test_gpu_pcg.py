@@ -385,6 +385,29 @@ def test_device_solve_is_stream_ordered(gpu, oracle, kernel, kw):
     s.close()
 
 
+def test_device_solve_rejects_host_pointers(gpu, sys0):
+    """xplus_pcg_solve_device takes device memory of the handle's GPU: numpy (host) arrays
+    are an argument error returned before anything is enqueued, never a GPU fault."""
+    import torch
+    from project_xplus_b200 import XplusError
+    from project_xplus_b200._lib import XPLUS_ERR_ARG
+    d, _ = sys0
+    s = xp.PcgSolver.from_dataset(d)
+    x_h = np.zeros(d.n)
+    with pytest.raises(XplusError) as e:
+        s.solve_device(d.b, x_h, tau=1e-8)
+    assert e.value.code == XPLUS_ERR_ARG and "d_b: host memory" in str(e.value)
+    d_b = torch.from_numpy(d.b).cuda()
+    with pytest.raises(XplusError) as e:
+        s.solve_device(d_b, x_h, tau=1e-8)
+    assert e.value.code == XPLUS_ERR_ARG and "d_x: host memory" in str(e.value)
+    # the handle is still usable afterwards
+    d_x = torch.zeros_like(d_b)
+    s.solve_device(d_b, d_x, tau=1e-8)
+    assert s.last_metrics()["converged"]
+    s.close()
+
+
 def test_cfg_scale_solve_property(gpu, oracle):
     """The 1108x1108 system (n = 1,227,664): FP32 plain kernel with FP64 residual replacement
     reaches 1e-8 FP64 true relative residual; checked on the host in FP64."""

@@ -33,7 +33,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "time-to-1e-8 rel. residual: learned/mixed vs plain Jacobi-PCG; SpMV HBM GB/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-FP64_CG_ITERATIONS = 5581
+# Iterations the reference's run_jacobi_pcg (src/CgSolverGolden.hpp:42-124, built from its
+# sources) takes on the 1108x1108 system to ||r|| <= 1e-8 ||b||: one full solve, 170 s on one
+# core (the reference arm times a bounded sample of it per step).
+GOLDEN_ITERATIONS_1108 = 5569
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the SM-resident kernel per
 # iteration on the 1108x1108 system: 618.5 MB over a captured launch of 100 iterations
 # (ncu --set full of `python -m project_xplus_b200.profile_case --grid 1108 --iters 100 --spmv 5`).
@@ -54,6 +57,7 @@ def parse():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison solves")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched solve")
     ap.add_argument("--no-spmv3d", action="store_true", help="skip the SpMV on the 128^3 3D system")
+    ap.add_argument("--no-config0", action="store_true", help="skip the n = 1024 system's GPU/CPU comparison")
     ap.add_argument("--clocks-dir", default=None,
                     help="directory for the nvidia-smi clock samples (default: a temporary directory)")
     a = ap.parse_args()
@@ -198,9 +202,9 @@ def run_reference(args):
         return 0
     from project_xplus_b200 import generators as g
     d, _ = g.system_2d_large(args.grid)
-    # iterations FP64 Jacobi-PCG needs on this system to reach 1e-8 (measured by the FP64 GPU
-    # solve that bench.py's own arm runs as its "fp64" comparison; the golden's arithmetic)
-    iters_needed = FP64_CG_ITERATIONS if args.grid == 1108 else 4 * args.grid
+    # iterations the reference's own solve needs on this system to reach 1e-8 (measured once in
+    # full); other grids: the FP64 CG count scales with the grid side
+    iters_needed = GOLDEN_ITERATIONS_1108 if args.grid == 1108 else round(GOLDEN_ITERATIONS_1108 * args.grid / 1108)
     samples = []
     for k in range(args.warmup + args.steps):
         per_it, setup, kind = cpu_reference_sample(d, args.cpu_sample_iters)
@@ -440,13 +444,11 @@ def run_b200(args):
         # the exact FSAI of the same pattern (host), both with the in-kernel Jacobi fallback
         from project_xplus_b200.learned import fsai_lower, load_weights
         params, _ = load_weights()
-        for name in ("learned_gtg", "learned_gtg_scaled", "fsai_gtg"):
+        for name in ("learned_gtg", "fsai_gtg"):
             s3 = xp.PcgSolver.from_dataset(d, device=local)
             t0 = time.perf_counter()
-            if name.startswith("learned_gtg"):
-                s3.set_gnn(params)
-                if name == "learned_gtg_scaled":
-                    s3.scale_gtg()  # rows of G normalized to (G A G^T)_ii = 1
+            if name == "learned_gtg":
+                s3.set_gnn(params)  # inference on the GPU, rows normalized to (G A G^T)_ii = 1
             else:
                 s3.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))
             setup_ms = (time.perf_counter() - t0) * 1e3
@@ -462,8 +464,12 @@ def run_b200(args):
             s3.close()
         compare["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / kern_mean
         compare["speedup_vs_fp64"] = compare["fp64"]["time_to_tol_ms"] / kern_mean
-        for name in ("learned_gtg", "learned_gtg_scaled", "fsai_gtg"):
+        for name in ("learned_gtg", "fsai_gtg"):
             compare[name]["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / compare[name]["time_to_tol_ms"]
+        # the learned preconditioner against the headline Jacobi kernel in the same layout (row-sum
+        # form, FP32, int16 columns: this line's own solve) and against FSAI of the same pattern
+        compare["learned_vs_jacobi_same_layout"] = kern_mean / compare["learned_gtg"]["time_to_tol_ms"]
+        compare["learned_vs_fsai"] = compare["fsai_gtg"]["time_to_tol_ms"] / compare["learned_gtg"]["time_to_tol_ms"]
 
     # CPU baseline: the reference's own golden on a bounded sample, rank 0 only, N=1 only
     cpu = None
@@ -475,6 +481,8 @@ def run_b200(args):
                "sample": f"{args.cpu_sample_iters} iterations of the reference run_jacobi_pcg (FP64, 1 thread) on "
                          f"the full system, extrapolated to {ref_iters:.0f} iterations (the FP64 CG iteration "
                          f"count to 1e-8); {per_it * 1e3:.1f} ms/iteration"}
+
+    config0 = run_config0(args, local) if rank == 0 and not args.no_config0 else None
 
     # the batch runs after the single-system handle is gone: that handle keeps its matrix
     # persisting in L2, which the L2-resident batch would otherwise lose
@@ -508,6 +516,7 @@ def run_b200(args):
                          "peak_kind": hbm_kind,
                          "bytes_per_launch": bytes_launch, "launch_ms": kern_mean},
             "compare": compare,
+            "config0": config0,
             "batch": batch,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -519,6 +528,86 @@ def run_b200(args):
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+def run_config0(args, device):
+    """The n = 1024 system (32x32 interior grid, sigma 1.0, x_true ~ U(-1,1) seed 0, x0 = 0) at
+    the reference's own defaults (tau = 1e-10 on r.r, max_iters 0 -> max(4n, 1000),
+    host/run_defaults.hpp:12-13), through three paths:
+      gpu_persistent   xplus_pcg_solve: host arrays in and out, FP64 values and vectors, one
+                       persistent launch per solve
+      gpu_multikernel  the reference's host loop (archived/host/multi_kernel_solver.hpp:100-234)
+                       driving this library's five C entry points (blocking calls, staged host arrays)
+      cpu_reference    the reference's run_local_multi_kernel_solver and run_jacobi_pcg built from
+                       its sources (oracle/_ref), one host thread (the reference has no threading)
+    Each is timed over repeated full solves; x is checked against the golden's."""
+    import project_xplus_b200 as xp
+    from oracle import oracle as O
+    from project_xplus_b200 import generators as g
+    from project_xplus_b200 import kernels as K
+    d, _ = g.system_2d_small()
+    n, tau = d.n, 1e-10
+    ref_lib = O.reflib()
+    gold = O.golden(d, tau, use_ref=ref_lib is not None)
+    out = {"workload": "2d-p1fem-32x32-sigma1 (n=1024), tau 1e-10 on r.r (the reference's run defaults)",
+           "n": n, "nnz": d.nnz, "golden_iterations": gold["iterations"]}
+
+    def timed(fn, reps, warm=3):
+        for _ in range(warm):
+            fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = fn()
+        return (time.perf_counter() - t0) / reps, r
+
+    s = xp.PcgSolver.from_dataset(d, values_dtype="f64", vector_dtype="f64", device=device)
+    dt, r = timed(lambda: s.solve(d.b, d.x0, tau=tau), 50)
+    s.close()
+    out["gpu_persistent"] = {"solves_per_s": 1.0 / dt, "ms_per_solve": dt * 1e3, "iterations": r.iterations,
+                             "kernel_ms": r.kernel_ms, "max_abs_diff_vs_golden": float(np.abs(r.solution - gold["x"]).max())}
+    m_inv = 1.0 / d.extract_jacobi_diag()
+
+    def mk_gpu():
+        x = d.x0.copy()
+        rr_, z, p, y = (np.zeros(n) for _ in range(4))
+        met, dot = np.zeros(2), np.zeros(1)
+        K.spmv_csr_kernel(d.row_ptr, d.col_idx, d.values, x, y, n)
+        K.init_pcg_kernel(d.b, y, m_inv, rr_, z, p, met, n)
+        rz, rr = met
+        it = 0
+        while it < max(4 * n, 1000) and rr > tau:
+            K.spmv_csr_kernel(d.row_ptr, d.col_idx, d.values, p, y, n)
+            K.dot_kernel(p, y, dot, n)
+            alpha = rz / dot[0]
+            K.update_xrz_kernel(x, p, rr_, y, m_inv, z, met, alpha, n)
+            beta = met[0] / rz
+            K.update_p_kernel(z, p, beta, n)
+            rz, rr = met
+            it += 1
+        return it, x
+    dt, (it, x) = timed(mk_gpu, 5, warm=1)
+    out["gpu_multikernel"] = {"solves_per_s": 1.0 / dt, "ms_per_solve": dt * 1e3, "iterations": it,
+                              "max_abs_diff_vs_golden": float(np.abs(x - gold["x"]).max()),
+                              "calls_per_iteration": 5}
+    if ref_lib is not None:
+        import ctypes as C
+        rp, ci, v = (np.ascontiguousarray(a) for a in (d.row_ptr, d.col_idx, d.values))
+        xo = np.empty(n)
+        it_c, st_c = C.c_int(), C.c_int()
+        frr, res = C.c_double(), C.c_double()
+        P = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+
+        def mk_cpu():
+            ref_lib.ref_multi_kernel(n, P(rp), P(ci), P(v), P(d.b), P(d.x0), C.c_double(tau), 0, P(xo),
+                                     C.byref(it_c), C.byref(frr), C.byref(st_c), C.byref(res), None)
+            return it_c.value
+        dt, it = timed(mk_cpu, 200)
+        dt_g, _ = timed(lambda: O.golden(d, tau, use_ref=True), 200)
+        out["cpu_reference"] = {"multi_kernel": {"solves_per_s": 1.0 / dt, "ms_per_solve": dt * 1e3, "iterations": it,
+                                                 "max_abs_diff_vs_golden": float(np.abs(xo - gold["x"]).max())},
+                                "golden": {"solves_per_s": 1.0 / dt_g, "ms_per_solve": dt_g * 1e3},
+                                "cores": 1, "kind": "reference"}
+    return out
 
 
 def _golden_solve(payload):

@@ -190,8 +190,10 @@ int xplus_pcg_solve_device(xplus_pcg* h, const double* d_b, double* d_x, double 
 int xplus_pcg_last_metrics(xplus_pcg* h, xplus_metrics* metrics);
 /* Phase clock of the last solve, read from block 0's %globaltimer (ms, summed over the
  * iterations): {phase A work, grid-barrier wait after A, phase B work, wait after B}; for the
- * one-barrier SM-resident kernel {records + dot-product partials, barrier wait and totals,
- * pending update + search-direction window refill, A p' from shared memory}; for the G^T G
+ * one-barrier SM-resident kernel {publishing the dot-product partials, barrier wait and
+ * totals, pending update + new search direction (the CTA's own rows from shared memory, the
+ * halo from the records), A p' from shared memory with each row's records and dot-product
+ * terms}; for the G^T G
  * kernel {A p', all grid-barrier waits, x/r update + t = G r', z = G^T t}. */
 int xplus_pcg_last_phase_times(xplus_pcg* h, double* ms4);
 /* The same phase clock for every CTA of the last solve: ms[4*b + k], k as above; *blocks is
@@ -248,8 +250,10 @@ int xplus_pcg_control(xplus_pcg* h, const double* b, const double* m_inv, double
 int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* g_low,
                       int fallback_iters);
 /* G predicted on the GPU by the learned network (parameters as xplus_gnn_get_params returns
- * them) from the CSR given to xplus_pcg_create; infer_ms (nullable) gets the host+device
- * time of the inference. */
+ * them) from the CSR given to xplus_pcg_create, its rows then scaled on the GPU to
+ * (G A G^T)_ii = 1 (the network fixes each row's direction; the scale is the normalization
+ * FSAI carries by construction).  XPLUS_ERR_DATA when a row has (G A G^T)_ii <= 0.  infer_ms
+ * (nullable) gets the host+device time of the inference. */
 int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
                       const float* params, int fallback_iters, double* infer_ms);
 /* The handle's current G in g_low order (g_low NULL: only *n_glow). */
@@ -268,11 +272,21 @@ int xplus_fsai_lower(int n, const int* row_ptr, const int* col_idx, const double
  * Learned-preconditioner trainer (no counterpart in the reference).  A 3-layer message-
  * passing network (hidden width 32) over A's graph predicts G: inputs log a_ii (centred),
  * sum_j |a_ij| / a_ii - 1 and a_ij / sqrt(a_ii a_jj); separate message weights for lower
- * and upper neighbours; G_ij = (w . relu(P h_i + bp + Q h_j + c e_ij) + bw) / sqrt(a_jj),
- * G_ii = exp(wd . h_i + bwd) / sqrt(a_ii).  Loss sum_p ||G A G^T v_p - v_p||^2 / (K n) over K
- * probe vectors v ~ N(0, I).  Forward, backward and Adam run on the GPU (FP32 arithmetic,
- * parameters rounded to BF16 in the forward pass, FP32 master copy).
+ * and upper neighbours; G_ij = (w . relu(P h_i + bp + Q h_j + c e_ij + c2 f_ij) + bw) / sqrt(a_jj)
+ * with f_ij = sum_{m < i, m != j} e_jm e_mi (two-step paths from j to i through i's other
+ * lower neighbours, e the scaled off-diagonal entries),
+ * G_ii = exp(wd . h_i + bwd) / sqrt(a_ii).  Two losses (xplus_gnn_set_loss):
+ *   XPLUS_GNN_LOSS_PROBE    sum_p ||G A G^T v_p - v_p||^2 / (K n) over K probe vectors
+ *                           v ~ N(0, I) (the default of a new trainer);
+ *   XPLUS_GNN_LOSS_KAPORIN  (1/n) sum_i [log (G A G^T)_ii - 2 log Ghat_ii], Ghat = G D^1/2:
+ *                           per row log(g A g / g_ii^2) on the row's pattern, free of the
+ *                           row's scale and smallest at the exact FSAI row; summed, n log of
+ *                           Kaporin's condition number of G A G^T once rows are normalized.
+ * Forward, backward and Adam run on the GPU (FP32 arithmetic, parameters rounded to BF16 in
+ * the forward pass, FP32 master copy).
  * ------------------------------------------------------------------------------------ */
+#define XPLUS_GNN_LOSS_PROBE 0
+#define XPLUS_GNN_LOSS_KAPORIN 1
 typedef struct xplus_gnn_trainer xplus_gnn_trainer;
 /* Number of parameters (floats); returns the count, not a status. */
 int xplus_gnn_param_count(void);
@@ -286,13 +300,26 @@ int xplus_gnn_set_params(xplus_gnn_trainer* t, const float* params);
 int xplus_gnn_get_params(xplus_gnn_trainer* t, float* params);
 /* Loss on system `sys` with the probes of `seed`, and its gradient (grad nullable). */
 int xplus_gnn_loss_grad(xplus_gnn_trainer* t, int sys, uint64_t seed, double* loss, float* grad);
+/* Loss of the trainer's later xplus_gnn_loss_grad / xplus_gnn_train calls
+ * (XPLUS_GNN_LOSS_PROBE or XPLUS_GNN_LOSS_KAPORIN; the Kaporin loss ignores seeds). */
+int xplus_gnn_set_loss(xplus_gnn_trainer* t, int kind);
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with a caller-given gradient. */
 int xplus_gnn_adam(xplus_gnn_trainer* t, const float* grad, double lr);
 /* `steps` Adam steps, one system per step (a seeded shuffle every epoch), probes from `seed`
  * and the step, learning rate cosine-decayed from lr to lr_final; losses (nullable) gets the
  * loss of every step. */
 int xplus_gnn_train(xplus_gnn_trainer* t, int steps, double lr, double lr_final, uint64_t seed, double* losses);
-/* G of system `sys` under the current parameters, in g_low order (g_low NULL: only *n_glow). */
+/* Steps [first_step, first_step + steps) of a cosine learning-rate schedule over total_steps
+ * (xplus_gnn_train is the window [0, steps) of a schedule of `steps`): training in windows
+ * over successive sets of resident systems (xplus_gnn_trainer_load) follows one schedule. */
+int xplus_gnn_train_window(xplus_gnn_trainer* t, int steps, double lr, double lr_final, uint64_t seed,
+                           int64_t first_step, int64_t total_steps, double* losses);
+/* Replaces the resident training systems (same CSR arguments as xplus_gnn_trainer_create);
+ * parameters, the Adam state and the loss kind are kept, the workspace grows as needed. */
+int xplus_gnn_trainer_load(xplus_gnn_trainer* t, int nsys, const int* const* row_ptrs,
+                           const int* const* col_idxs, const double* const* values, const int* ns);
+/* G of system `sys` under the current parameters as the network outputs it (rows not
+ * normalized), in g_low order (g_low NULL: only *n_glow). */
 int xplus_gnn_predict(xplus_gnn_trainer* t, int sys, double* g_low, int64_t* n_glow);
 
 /* ------------------------------------------------------------------------------------

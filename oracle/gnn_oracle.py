@@ -14,11 +14,15 @@ the row order the solver is given:
                 h_i <- h_i + relu(s_i)
                 (lower and upper neighbours get their own weights: G is lower-triangular in
                 this order, so what G_ij should be depends on which neighbours precede i)
-  edge head     for j < i, a_ij != 0:  z = relu(P h_i + bp + Q h_j + c e_ij),
-                Ghat_ij = w . z + bw
+  edge head     for j < i, a_ij != 0:  z = relu(P h_i + bp + Q h_j + c e_ij + c2 f_ij),
+                Ghat_ij = w . z + bw, with f_ij = sum_{m < i, m != j} e_jm e_mi (two-step paths
+                from j to i through i's other lower neighbours)
   diagonal      Ghat_ii = exp(wd . h_i + bwd)
   G             G_ij = Ghat_ij / sqrt(a_jj)   (so G = Ghat D^-1/2, and Ghat = I is Jacobi)
-Loss over K probe vectors v ~ N(0, I):  L = sum_p ||G A G^T v_p - v_p||^2 / (K n).
+Losses: the probe loss over K vectors v ~ N(0, I), L = sum_p ||G A G^T v_p - v_p||^2 / (K n),
+and the row-normalized Kaporin loss L = (1/n) sum_i [log (G A G^T)_ii - 2 log Ghat_ii]
+(kaporin_loss; the network is trained with it, and the solver scales G's rows to
+(G A G^T)_ii = 1 after inference).
 The forward pass uses the parameters rounded to BF16 (round to nearest even); gradients are
 taken with respect to the rounded values and applied to the FP32 master copy.
 """
@@ -38,7 +42,7 @@ def layout():
     out = [("W0", (H, 2)), ("b0", (H,))]
     for l in range(LAYERS):
         out += [(f"Wa{l}", (H, H)), (f"ba{l}", (H,)), (f"Wl{l}", (H, H)), (f"Wu{l}", (H, H))]
-    out += [("P", (H, H)), ("bp", (H,)), ("Q", (H, H)), ("c", (H,)), ("w", (H,)), ("bw", (1,)),
+    out += [("P", (H, H)), ("bp", (H,)), ("Q", (H, H)), ("c", (H,)), ("c2", (H,)), ("w", (H,)), ("bw", (1,)),
             ("wd", (H,)), ("bwd", (1,))]
     return out
 
@@ -76,7 +80,7 @@ def init_params(seed: int = 0) -> np.ndarray:
     for name, shape in layout():
         if name in ("w", "bw", "wd", "bwd") or name.startswith("b"):
             d[name] = np.zeros(shape)
-        elif name == "c":
+        elif name in ("c", "c2"):
             d[name] = rng.uniform(-0.5, 0.5, shape)
         else:
             fan_in = shape[1]
@@ -98,7 +102,12 @@ def graph(row_ptr, col_idx, values) -> dict:
     ld = np.log(d)
     x = np.stack([ld - ld.mean(), rowabs / d - 1.0], 1)
     low = c < r
-    return dict(n=n, A=A, d=d, x=x, r=r, c=c, e=e, low=low, lr=r[low], lc=c[low], le=e[low])
+    # f_ij = (L E)_ij on the lower edges: L the strictly lower part of E = the off-diagonal
+    # scaled matrix, so the sum runs over i's lower neighbours m with m != j adjacent to j
+    E = sp.csr_matrix((e, (r, c)), shape=(n, n))
+    L = sp.csr_matrix((e[low], (r[low], c[low])), shape=(n, n))
+    lf = np.asarray((L @ E)[r[low], c[low]]).ravel()
+    return dict(n=n, A=A, d=d, x=x, r=r, c=c, e=e, low=low, lr=r[low], lc=c[low], le=e[low], lf=lf)
 
 
 def _agg(g, vals_lo, vals_up):
@@ -123,7 +132,7 @@ def forward(theta, g, round_bf16=True):
     cache["hs"], cache["ss"] = hs, ss
     ph = h @ p["P"].T + p["bp"]
     qh = h @ p["Q"].T
-    zpre = ph[g["lr"]] + qh[g["lc"]] + np.outer(g["le"], p["c"])
+    zpre = ph[g["lr"]] + qh[g["lc"]] + np.outer(g["le"], p["c"]) + np.outer(g["lf"], p["c2"])
     z = np.maximum(zpre, 0.0)
     go = z @ p["w"] + p["bw"][0]
     gd = np.exp(h @ p["wd"] + p["bwd"][0])
@@ -170,10 +179,9 @@ def loss(theta, g, v, round_bf16=True) -> float:
 
 
 def loss_and_grad(theta, g, v, round_bf16=True):
-    """Loss and its gradient with respect to the (rounded) parameters, FP64, by hand."""
+    """Probe loss and its gradient with respect to the (rounded) parameters, FP64, by hand."""
     n, K = g["n"], v.shape[1]
     go, gd, cache = forward(theta, g, round_bf16)
-    p = cache["p"]
     G = g_matrix(g, go, gd)
     A = g["A"]
     w1 = G.T @ v
@@ -187,7 +195,72 @@ def loss_and_grad(theta, g, v, round_bf16=True):
     dG_off = scale * ((r[g["lr"]] * w2[g["lc"]]).sum(1) + (v[g["lr"]] * y[g["lc"]]).sum(1))
     dG_dia = scale * ((r * w2).sum(1) + (v * y).sum(1))
     dgo = dG_off * isq[g["lc"]]
-    dgd = dG_dia * isq
+    dexp = dG_dia * isq * gd
+    return L, _backward(g, cache, dgo, dexp)
+
+
+def scaled_matrix(g):
+    """A^ = D^-1/2 A D^-1/2 (unit diagonal) as CSR."""
+    isq = 1.0 / np.sqrt(g["d"])
+    return (sp.diags(isq) @ g["A"] @ sp.diags(isq)).tocsr()
+
+
+def ghat_matrix(g, go, gd):
+    """Ghat (the head's output before the D^-1/2 column scaling) as CSR."""
+    n = g["n"]
+    rows = np.concatenate([g["lr"], np.arange(n)])
+    cols = np.concatenate([g["lc"], np.arange(n)])
+    return sp.csr_matrix((np.concatenate([go, gd]), (rows, cols)), shape=(n, n))
+
+
+def kaporin_terms(g, go, gd):
+    """Per-row B_i = (G A G^T)_ii = ghat_i^T A^ ghat_i and U = Ghat A^ restricted to Ghat's
+    pattern: U_ij = (A^ ghat_i)_j for j in the pattern of row i (lower edges, then diagonal)."""
+    Gh = ghat_matrix(g, go, gd)
+    U = (Gh @ scaled_matrix(g)).tocsr()
+    B = np.asarray(U.multiply(Gh).sum(axis=1)).ravel()
+    u_off = np.asarray(U[g["lr"], g["lc"]]).ravel()
+    u_dia = U.diagonal()
+    return B, u_off, u_dia
+
+
+def kaporin_loss(theta, g, round_bf16=True) -> float:
+    """Row-normalized Kaporin loss L = (1/n) sum_i [log (G A G^T)_ii - 2 log G^_ii].
+    Per row it is the log of (g A g) / g_ii^2 over the row's pattern, which is invariant to the
+    row's scale and is smallest for the exact FSAI row (the factorized sparse approximate
+    inverse minimizes Kaporin's condition number det-ratio of G A G^T over the pattern).  Summed
+    over rows it is, up to a constant, n log K(G A G^T) once the rows are scaled to unit
+    (G A G^T)_ii, which the solver does after inference."""
+    go, gd, _ = forward(theta, g, round_bf16)
+    B, _, _ = kaporin_terms(g, go, gd)
+    return float((np.log(B) - 2.0 * np.log(gd)).mean())
+
+
+def kaporin_loss_and_grad(theta, g, round_bf16=True):
+    """Kaporin loss and its gradient, FP64, by hand:
+      dL/dGhat_ij = 2 U_ij / (n B_i)  (j < i),   dL/dt_i = 2 U_ii gd_i / (n B_i) - 2 / n
+    with t_i the diagonal head's pre-exponential value (Ghat_ii = gd_i = exp t_i)."""
+    n = g["n"]
+    go, gd, cache = forward(theta, g, round_bf16)
+    B, u_off, u_dia = kaporin_terms(g, go, gd)
+    L = float((np.log(B) - 2.0 * np.log(gd)).mean())
+    dgo = 2.0 * u_off / (n * B[g["lr"]])
+    dexp = 2.0 * u_dia * gd / (n * B) - 2.0 / n
+    return L, _backward(g, cache, dgo, dexp)
+
+
+def normalize_rows(g, go, gd):
+    """Rows of Ghat scaled to (G A G^T)_ii = 1 (what the solver applies after inference)."""
+    B, _, _ = kaporin_terms(g, go, gd)
+    s = 1.0 / np.sqrt(B)
+    return go * s[g["lr"]], gd * s
+
+
+def _backward(g, cache, dgo, dexp):
+    """Parameter gradient from dL/dGhat on the lower edges (dgo) and dL/dt on the diagonal
+    (dexp = dL/dGhat_ii * Ghat_ii): the same chain for every loss."""
+    n = g["n"]
+    p = cache["p"]
     grads = {name: np.zeros(shape) for name, shape in layout()}
     h = cache["hs"][-1]
     z, zpre = cache["z"], cache["zpre"]
@@ -196,6 +269,7 @@ def loss_and_grad(theta, g, v, round_bf16=True):
     grads["bw"] = np.array([dgo.sum()])
     dz = np.outer(dgo, p["w"]) * (zpre > 0)
     grads["c"] = dz.T @ g["le"]
+    grads["c2"] = dz.T @ g["lf"]
     dph = np.zeros((n, H))
     np.add.at(dph, g["lr"], dz)
     dqh = np.zeros((n, H))
@@ -203,7 +277,6 @@ def loss_and_grad(theta, g, v, round_bf16=True):
     grads["P"] = dph.T @ h
     grads["bp"] = dph.sum(0)
     grads["Q"] = dqh.T @ h
-    dexp = dgd * cache["gd"]
     grads["wd"] = h.T @ dexp
     grads["bwd"] = np.array([dexp.sum()])
     dh = dph @ p["P"] + dqh @ p["Q"] + np.outer(dexp, p["wd"])
@@ -228,7 +301,7 @@ def loss_and_grad(theta, g, v, round_bf16=True):
     dpre0 = dh * (cache["pre0"] > 0)
     grads["W0"] = dpre0.T @ g["x"]
     grads["b0"] = dpre0.sum(0)
-    return L, pack(grads)
+    return pack(grads)
 
 
 def adam(theta, m, v, grad, step, lr, b1=0.9, b2=0.999, eps=1e-8):

@@ -16,8 +16,10 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 C_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libxplus_ref.so"
-# the reference's multi-kernel host program relinked against libxplus_b200.so (oracle/Makefile relink)
+# the reference's multi-kernel host program relinked against libxplus_b200.so, and the same
+# program with the reference's own CPU kernels (oracle/Makefile relink)
 RELINKED_HOST = HERE / "_ref" / "xplus_host_b200"
+REFERENCE_HOST = HERE / "_ref" / "xplus_host_ref"
 
 
 # Where the reference checkout lies in the build container; XPLUS_REFERENCE_TREE overrides it.

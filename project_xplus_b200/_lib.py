@@ -18,6 +18,8 @@ XPLUS_TAU_ABS_RR, XPLUS_TAU_REL_TRUE = 0, 1
 XPLUS_NOALLOC_MAX_N = 4194304
 
 STATUS_NAMES = {0: "converged", 1: "max_iter", 2: "breakdown", 3: "timeout"}
+XPLUS_GNN_LOSS_PROBE = 0
+XPLUS_GNN_LOSS_KAPORIN = 1
 
 
 class XplusOpts(C.Structure):
@@ -109,8 +111,11 @@ _SIGS = {
     "xplus_gnn_set_params": (_i, [_p, _p]),
     "xplus_gnn_get_params": (_i, [_p, _p]),
     "xplus_gnn_loss_grad": (_i, [_p, _i, _u64, _dp, _p]),
+    "xplus_gnn_set_loss": (_i, [_p, _i]),
     "xplus_gnn_adam": (_i, [_p, _p, _d]),
     "xplus_gnn_train": (_i, [_p, _i, _d, _d, _u64, _p]),
+    "xplus_gnn_train_window": (_i, [_p, _i, _d, _d, _u64, _i64, _i64, _p]),
+    "xplus_gnn_trainer_load": (_i, [_p, _i, _p, _p, _p, _p]),
     "xplus_gnn_predict": (_i, [_p, _i, _p, C.POINTER(_i64)]),
     "xplus_batch_create": (_i, [_i, _p, _p, _p, _p, C.POINTER(XplusOpts), C.POINTER(_p)]),
     "xplus_batch_destroy": (_i, [_p]),

@@ -6,10 +6,13 @@
 //   x_i = [log a_ii - mean log a_kk, sum_j |a_ij| / a_ii - 1],  e_ij = a_ij / sqrt(a_ii a_jj)
 //   h = relu(W0 x + b0)
 //   3 x: s_i = Wa h_i + ba + sum_{j<i} e_ij Wl h_j + sum_{j>i} e_ij Wu h_j ; h_i += relu(s_i)
-//   lower edge (i, j<i): Ghat_ij = w . relu(P h_i + bp + Q h_j + c e_ij) + bw
+//   lower edge (i, j<i): Ghat_ij = w . relu(P h_i + bp + Q h_j + c e_ij + c2 f_ij) + bw,
+//     f_ij = sum_{m < i, m != j} e_jm e_mi: the two-step paths from j to i through i's other
+//     lower neighbours (the coupling inside row i's pattern that the exact FSAI row solves)
 //   diagonal:            Ghat_ii = exp(wd . h_i + bwd)
 //   G = Ghat D^-1/2 (an untrained network with a zero output layer gives Jacobi)
-// Loss over K probes v ~ N(0, I): L = sum ||G A G^T v - v||^2 / (K n).
+// Losses: over K probes v ~ N(0, I), L = sum ||G A G^T v - v||^2 / (K n); or the row-normalized
+// Kaporin loss L = (1/n) sum_i [log (G A G^T)_ii - 2 log Ghat_ii].
 // Lower and upper neighbours have their own message weights because G is lower-triangular in
 // the given order: what G_ij should be depends on which neighbours precede row i.
 //
@@ -142,30 +145,134 @@ __global__ void k_aggregate(const int* __restrict__ adj_ptr, const int* __restri
 
 // Edge head and diagonal: warp per row i; lower edges of row i in CSR order.
 __global__ void k_head(const int* __restrict__ low_ptr, const int* __restrict__ low_col,
-                       const float* __restrict__ low_e, const float* __restrict__ ph, const float* __restrict__ qh,
+                       const float* __restrict__ low_e, const float* __restrict__ low_f, const float* __restrict__ ph,
+                       const float* __restrict__ qh,
                        const float* __restrict__ h, const float* __restrict__ isq, const float* __restrict__ wr,
                        ParamOffsets off, float* __restrict__ zpre, float* __restrict__ go, float* __restrict__ gval,
-                       float* __restrict__ gd, float* __restrict__ gdiag, int n) {
+                       float* __restrict__ gd, float* __restrict__ td, float* __restrict__ gdiag, int n) {
     const int lane = threadIdx.x & 31;
     const int i = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     if (i >= n) return;
-    const float c = wr[off.c + lane], w = wr[off.w + lane], bw = wr[off.bw];
+    const float c = wr[off.c + lane], c2 = wr[off.c2 + lane], w = wr[off.w + lane], bw = wr[off.bw];
     const float phv = ph[static_cast<size_t>(i) * H + lane];
     for (int k = low_ptr[i]; k < low_ptr[i + 1]; ++k) {
         const int j = low_col[k];
-        const float zp = phv + qh[static_cast<size_t>(j) * H + lane] + c * low_e[k];
+        const float zp = phv + qh[static_cast<size_t>(j) * H + lane] + c * low_e[k] + c2 * low_f[k];
         if (zpre) zpre[static_cast<size_t>(k) * H + lane] = zp;
         const float g = warp_sum_f(w * fmaxf(zp, 0.0f)) + bw;
         if (lane == 0) {
-            if (go) go[k] = g;
+            go[k] = g;
             gval[k] = g * isq[j];
         }
     }
     const float t = warp_sum_f(wr[off.wd + lane] * h[static_cast<size_t>(i) * H + lane]) + wr[off.bwd];
     if (lane == 0) {
         const float e = expf(t);
-        if (gd) gd[i] = e;
+        gd[i] = e;
+        td[i] = t;
         gdiag[i] = e * isq[i];
+    }
+}
+
+// ---- row-normalized Kaporin loss and the row normalization of G ----
+// Row i's pattern P_i = {lower neighbours j < i (ascending), i}; Ghat_i on it is
+// (go[low_ptr[i]..], gd[i]).  With A^ = D^-1/2 A D^-1/2 (unit diagonal, off-diagonals adj_e):
+//   u_j = (A^ ghat_i)_j = ghat_ij + sum_{m in adj(j), m in P_i} adj_e(j,m) ghat_im   (j in P_i)
+//   B_i = (G A G^T)_ii = sum_{j in P_i} ghat_ij u_j
+// adj(j) and P_i are both ascending, so the membership test is a merge.  Warp per row, lane
+// per pattern entry (loops for rows with more than 32).
+__device__ __forceinline__ float kap_u(int i, int pos, int m, int lp, const int* __restrict__ low_col,
+                                       const float* __restrict__ go, const float* __restrict__ gd,
+                                       const int* __restrict__ adj_ptr, const int* __restrict__ adj_col,
+                                       const float* __restrict__ adj_e) {
+    const int j = pos < m - 1 ? low_col[lp + pos] : i;
+    float u = pos < m - 1 ? go[lp + pos] : gd[i];  // the unit diagonal of A^
+    int t = 0;                                      // cursor in P_i
+    for (int q = adj_ptr[j]; q < adj_ptr[j + 1]; ++q) {
+        const int c = adj_col[q];
+        if (c > i) break;  // P_i has nothing above i
+        while (t < m - 1 && low_col[lp + t] < c) ++t;
+        const int pc = t < m - 1 ? low_col[lp + t] : i;
+        if (pc == c) u = fmaf(adj_e[q], t < m - 1 ? go[lp + t] : gd[i], u);
+    }
+    return u;
+}
+
+// mode 0 (training): rowloss_i = log B_i - 2 t_i; dgo_k = 2 u_j / (n B_i) on the lower edges,
+//   dexp_i = 2 u_i gd_i / (n B_i) - 2 / n on the diagonal (dL/dt_i).
+// mode 1 (inference): rows of G (gval, gdiag) scaled by 1 / sqrt(B_i), so (G A G^T)_ii = 1.
+// A row with B_i <= 0 or not finite counts in *bad and is left as it is.
+__global__ void k_kaporin(const int* __restrict__ low_ptr, const int* __restrict__ low_col,
+                          const int* __restrict__ adj_ptr, const int* __restrict__ adj_col,
+                          const float* __restrict__ adj_e, const float* __restrict__ go,
+                          const float* __restrict__ gd, const float* __restrict__ td, int n, int mode,
+                          float* __restrict__ rowloss, float* __restrict__ dgo, float* __restrict__ dexp,
+                          float* __restrict__ gval, float* __restrict__ gdiag, int* __restrict__ bad) {
+    const int lane = threadIdx.x & 31;
+    const int i = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    const int lp = low_ptr[i];
+    const int m = low_ptr[i + 1] - lp + 1;
+    float part = 0.0f;
+    float u0 = 0.0f;  // u of this lane's first entry (rows of at most 32 entries need no recompute)
+    for (int pos = lane; pos < m; pos += 32) {
+        const float u = kap_u(i, pos, m, lp, low_col, go, gd, adj_ptr, adj_col, adj_e);
+        if (pos == lane) u0 = u;
+        part = fmaf(pos < m - 1 ? go[lp + pos] : gd[i], u, part);
+    }
+    const float B = warp_sum_f(part);
+    const bool ok = B > 0.0f && isfinite(B);
+    if (!ok) {
+        if (lane == 0) atomicAdd(bad, 1);
+        if (mode == 0) {
+            for (int pos = lane; pos < m - 1; pos += 32) dgo[lp + pos] = 0.0f;
+            if (lane == 0) {
+                rowloss[i] = 0.0f;
+                dexp[i] = 0.0f;
+            }
+        }
+        return;
+    }
+    if (mode == 1) {
+        const float s = rsqrtf(B);
+        for (int pos = lane; pos < m - 1; pos += 32) gval[lp + pos] *= s;
+        if (lane == 0) gdiag[i] *= s;
+        return;
+    }
+    const float inv_n = 1.0f / static_cast<float>(n);
+    const float c = 2.0f * inv_n / B;
+    for (int pos = lane; pos < m; pos += 32) {
+        const float u = pos == lane ? u0 : kap_u(i, pos, m, lp, low_col, go, gd, adj_ptr, adj_col, adj_e);
+        if (pos < m - 1) dgo[lp + pos] = c * u;
+        else dexp[i] = c * u * gd[i] - 2.0f * inv_n;
+    }
+    if (lane == 0) rowloss[i] = logf(B) - 2.0f * td[i];
+}
+
+// sum partials of v over [count] (FP64 per block, fixed order)
+__global__ void __launch_bounds__(256) k_sum_partial(const float* __restrict__ v, long long count,
+                                                     double* __restrict__ partial) {
+    __shared__ double red[8];
+    double s = 0.0;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < count;
+         t += static_cast<long long>(gridDim.x) * blockDim.x)
+        s += static_cast<double>(v[t]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += red[q];
+        partial[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_dsum_final(const double* __restrict__ partial, int blocks, double scale, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < blocks; ++b) s += partial[b];
+        *out = s * scale;
     }
 }
 
@@ -358,29 +465,36 @@ __global__ void k_partial_final(const float* __restrict__ partial, int blocks, i
 }
 
 // Edge-head parameter partials over lower edges (warp per edge, grid-stride):
-//   dw[f] += dgo relu(zpre_f), dc[f] += dgo w_f [zpre_f > 0] e, dbw += dgo
+//   dw[f] += dgo relu(zpre_f), dc[f] += dgo w_f [zpre_f > 0] e, dc2[f] += dgo w_f [zpre_f > 0] f,
+//   dbw += dgo;  partial row layout [dw (H) | dc (H) | dc2 (H) | dbw (1)]
+constexpr int kEdgeRow = 3 * H + 1;
 __global__ void __launch_bounds__(256) k_edge_partial(const float* __restrict__ zpre, const float* __restrict__ dgo,
-                                                      const float* __restrict__ low_e, const float* __restrict__ wr,
-                                                      ParamOffsets off, int n_low, float* __restrict__ partial) {
-    __shared__ float red[8][2 * H + 1];
+                                                      const float* __restrict__ low_e, const float* __restrict__ low_f,
+                                                      const float* __restrict__ wr, ParamOffsets off, int n_low,
+                                                      float* __restrict__ partial) {
+    __shared__ float red[8][kEdgeRow];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const float w = wr[off.w + lane];
-    float aw = 0.0f, ac = 0.0f, ab = 0.0f;
+    float aw = 0.0f, ac = 0.0f, ac2 = 0.0f, ab = 0.0f;
     for (int k = blockIdx.x * 8 + warp; k < n_low; k += gridDim.x * 8) {
         const float z = zpre[static_cast<size_t>(k) * H + lane];
         const float d = dgo[k];
         aw = fmaf(d, fmaxf(z, 0.0f), aw);
-        if (z > 0.0f) ac = fmaf(d * w, low_e[k], ac);
+        if (z > 0.0f) {
+            ac = fmaf(d * w, low_e[k], ac);
+            ac2 = fmaf(d * w, low_f[k], ac2);
+        }
         ab += d;
     }
     red[warp][lane] = aw;
     red[warp][H + lane] = ac;
-    if (lane == 0) red[warp][2 * H] = ab;
+    red[warp][2 * H + lane] = ac2;
+    if (lane == 0) red[warp][3 * H] = ab;
     __syncthreads();
-    for (int o = threadIdx.x; o < 2 * H + 1; o += blockDim.x) {
+    for (int o = threadIdx.x; o < kEdgeRow; o += blockDim.x) {
         float s = 0.0f;
         for (int q = 0; q < 8; ++q) s += red[q][o];
-        partial[static_cast<size_t>(blockIdx.x) * (2 * H + 1) + o] = s;
+        partial[static_cast<size_t>(blockIdx.x) * kEdgeRow + o] = s;
     }
 }
 
@@ -470,6 +584,7 @@ ParamOffsets param_offsets() {
     o.bp = p; p += H;
     o.Q = p; p += H * H;
     o.c = p; p += H;
+    o.c2 = p; p += H;
     o.w = p; p += H;
     o.bw = p; p += 1;
     o.wd = p; p += H;
@@ -597,6 +712,29 @@ void HostGraph::build(int n_, const int* row_ptr, const int* col_idx, const doub
             }
         }
     });
+    // f_ij = sum over i's other lower neighbours m of e_jm e_mi (rows in parallel; adj(j) is
+    // ascending, so each e_jm is a binary search)
+    low_f.assign(static_cast<size_t>(n_low), 0.0f);
+    parallel_rows(n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            const int l0 = low_ptr[static_cast<size_t>(i)], l1 = low_ptr[static_cast<size_t>(i) + 1];
+            for (int k = l0; k < l1; ++k) {
+                const int j = low_col[static_cast<size_t>(k)];
+                const int* a0 = adj_col.data() + adj_ptr[static_cast<size_t>(j)];
+                const int* a1 = adj_col.data() + adj_ptr[static_cast<size_t>(j) + 1];
+                double f = 0.0;
+                for (int q = l0; q < l1; ++q) {
+                    if (q == k) continue;
+                    const int m = low_col[static_cast<size_t>(q)];
+                    const int* at = std::lower_bound(a0, a1, m);
+                    if (at != a1 && *at == m)
+                        f += static_cast<double>(adj_e[static_cast<size_t>(at - adj_col.data())]) *
+                             static_cast<double>(low_e[static_cast<size_t>(q)]);
+                }
+                low_f[static_cast<size_t>(k)] = static_cast<float>(f);
+            }
+        }
+    });
     // lower edges grouped by column: up(j) = {k : low_col[k] == j}, by increasing row
     up_ptr.assign(N + 1, 0);
     for (int k = 0; k < n_low; ++k) ++up_ptr[static_cast<size_t>(low_col[static_cast<size_t>(k)]) + 1];
@@ -654,6 +792,7 @@ void DevGraph::upload(const HostGraph& g, Arena& ar, cudaStream_t st) {
     low_col = up(ar, g.low_col, st);
     low_row = up(ar, g.low_row, st);
     low_e = up(ar, g.low_e, st);
+    low_f = up(ar, g.low_f, st);
     up_ptr = up(ar, g.up_ptr, st);
     up_k = up(ar, g.up_k, st);
     up_row = up(ar, g.up_row, st);
@@ -678,11 +817,13 @@ void Work::alloc(Arena& ar, int max_n, int max_low, int K_, bool train) {
     qh = ar.get<float>(nH);
     gval = ar.get<float>(static_cast<size_t>(max_low));
     gdiag = ar.get<float>(static_cast<size_t>(max_n));
-    if (!train) return;
-    zpre = ar.get<float>(lH);
     go = ar.get<float>(static_cast<size_t>(max_low));
     gd = ar.get<float>(static_cast<size_t>(max_n));
-    const size_t nK = static_cast<size_t>(max_n) * K;
+    td = ar.get<float>(static_cast<size_t>(max_n));
+    bad = ar.get<int>(1);
+    if (!train) return;
+    zpre = ar.get<float>(lH);
+    const size_t nK = static_cast<size_t>(max_n) * std::max(K, 1);
     v = ar.get<float>(nK);
     w1 = ar.get<float>(nK);
     w2 = ar.get<float>(nK);
@@ -699,12 +840,20 @@ void Work::alloc(Arena& ar, int max_n, int max_low, int K_, bool train) {
     dph = ar.get<float>(nH);
     dqh = ar.get<float>(nH);
     partial = ar.get<float>(static_cast<size_t>(kRedBlocks) * (H * H + H));
+    dpartial = ar.get<double>(static_cast<size_t>(kRedBlocks));
     loss = ar.get<double>(1);
 }
 
 static void kcheck(const char* what) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static void kcheck_status(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
 }
 
 void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream_t st) {
@@ -725,10 +874,21 @@ void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream
     Lin3 L{{wr + off.P, wr + off.Q, nullptr}, {wr + off.bp, nullptr, nullptr}, {w.ph, w.qh, nullptr}, 2};
     k_node_lin<<<lin_blocks, 256, 0, st>>>(w.h[kLayers], L, n);
     kcheck("gnn head lin");
-    k_head<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.low_col, g.low_e, w.ph, w.qh, w.h[kLayers], g.isq, wr, off,
-                                         train ? w.zpre : nullptr, train ? w.go : nullptr, w.gval,
-                                         train ? w.gd : nullptr, w.gdiag, n);
+    k_head<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.low_col, g.low_e, g.low_f, w.ph, w.qh, w.h[kLayers], g.isq, wr, off,
+                                         train ? w.zpre : nullptr, w.go, w.gval, w.gd, w.td, w.gdiag, n);
     kcheck("gnn head");
+}
+
+void normalize_rows(const DevGraph& g, Work& w, cudaStream_t st) {
+    const int nodes_blocks = blocks_for(static_cast<long long>(g.n) * 32, 256);
+    kcheck_status(cudaMemsetAsync(w.bad, 0, sizeof(int), st), "gnn memset");
+    k_kaporin<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.low_col, g.adj_ptr, g.adj_col, g.adj_e, w.go, w.gd, w.td,
+                                            g.n, 1, nullptr, nullptr, nullptr, w.gval, w.gdiag, w.bad);
+    kcheck("gnn normalize rows");
+    int bad = 0;
+    kcheck_status(cudaMemcpyAsync(&bad, w.bad, sizeof(int), cudaMemcpyDeviceToHost, st), "gnn D2H");
+    kcheck_status(cudaStreamSynchronize(st), "gnn sync");
+    require(bad == 0, XPLUS_ERR_DATA, "a row of the predicted G has (G A G^T)_ii <= 0 or not finite");
 }
 
 void g_to_low(const DevGraph& g, const Work& w, double* d_glow, cudaStream_t st) {
@@ -760,7 +920,20 @@ static void wd_grad(const float* coef, const float* X, int n, Work& w, float* gr
 }
 
 void loss_backward(const DevGraph& g, const float* wr, Work& w, float* grad, unsigned long long seed, cudaStream_t st) {
-    const ParamOffsets off = param_offsets();
+    if (w.loss_kind == kLossKaporin) {
+        const int n = g.n;
+        const int nodes_blocks = blocks_for(static_cast<long long>(n) * 32, 256);
+        kcheck_status(cudaMemsetAsync(w.bad, 0, sizeof(int), st), "gnn memset");
+        k_kaporin<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.low_col, g.adj_ptr, g.adj_col, g.adj_e, w.go, w.gd, w.td,
+                                                n, 0, w.r, w.dgo, w.dexp, nullptr, nullptr, w.bad);
+        kcheck("gnn kaporin");
+        const int lb = std::min(kRedBlocks, blocks_for(n, 256));
+        k_sum_partial<<<lb, 256, 0, st>>>(w.r, n, w.dpartial);
+        k_dsum_final<<<1, 32, 0, st>>>(w.dpartial, lb, 1.0 / static_cast<double>(n), w.loss);
+        kcheck("gnn kaporin loss");
+        if (grad) backward_from_dg(g, wr, w, grad, st);
+        return;
+    }
     const int n = g.n, K = w.K;
     const long long nK = static_cast<long long>(n) * K;
     const int pb = blocks_for(nK, 256);
@@ -782,6 +955,14 @@ void loss_backward(const DevGraph& g, const float* wr, Work& w, float* grad, uns
     k_dG<<<blocks_for(static_cast<long long>(g.n_low) + n, 256), 256, 0, st>>>(g.low_row, g.low_col, g.isq, w.r, w.w2, w.v,
                                                                               w.y, w.gd, w.dgo, w.dexp, g.n_low, n, K, scale);
     kcheck("gnn dG");
+    backward_from_dg(g, wr, w, grad, st);
+}
+
+// Parameter gradient from dL/dGhat on the lower edges (w.dgo) and dL/dt on the diagonal
+// (w.dexp): the chain every loss shares.
+void backward_from_dg(const DevGraph& g, const float* wr, Work& w, float* grad, cudaStream_t st) {
+    const ParamOffsets off = param_offsets();
+    const int n = g.n;
     const int nodes_blocks = blocks_for(static_cast<long long>(n) * 32, 256);
     const int lin_blocks = std::min(blocks_for(n, 8), 148 * 8);
     k_head_back<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.up_ptr, g.up_k, w.zpre, w.dgo, wr, off, w.dph, w.dqh, n);
@@ -789,12 +970,13 @@ void loss_backward(const DevGraph& g, const float* wr, Work& w, float* grad, uns
     // edge-head parameters w, c, bw
     {
         const int eb = std::max(1, std::min(kRedBlocks, blocks_for(g.n_low, 8)));
-        k_edge_partial<<<eb, 256, 0, st>>>(w.zpre, w.dgo, g.low_e, wr, off, g.n_low, w.partial);
+        k_edge_partial<<<eb, 256, 0, st>>>(w.zpre, w.dgo, g.low_e, g.low_f, wr, off, g.n_low, w.partial);
         kcheck("gnn edge partial");
-        // partial rows: [dw (H) | dc (H) | dbw (1)]
-        k_partial_final<<<1, 128, 0, st>>>(w.partial, eb, 2 * H + 1, H, 0, grad, off.w, -1);
-        k_partial_final<<<1, 128, 0, st>>>(w.partial + H, eb, 2 * H + 1, H, 0, grad, off.c, -1);
-        k_partial_final<<<1, 32, 0, st>>>(w.partial + 2 * H, eb, 2 * H + 1, 1, 0, grad, off.bw, -1);
+        // partial rows: [dw (H) | dc (H) | dc2 (H) | dbw (1)]
+        k_partial_final<<<1, 128, 0, st>>>(w.partial, eb, kEdgeRow, H, 0, grad, off.w, -1);
+        k_partial_final<<<1, 128, 0, st>>>(w.partial + H, eb, kEdgeRow, H, 0, grad, off.c, -1);
+        k_partial_final<<<1, 128, 0, st>>>(w.partial + 2 * H, eb, kEdgeRow, H, 0, grad, off.c2, -1);
+        k_partial_final<<<1, 32, 0, st>>>(w.partial + 3 * H, eb, kEdgeRow, 1, 0, grad, off.bw, -1);
         kcheck("gnn edge final");
     }
     const float* hL = w.h[kLayers];

@@ -15,7 +15,7 @@ constexpr int kLayers = 3;
 struct ParamOffsets {
     int W0, b0;
     int Wa[kLayers], ba[kLayers], Wl[kLayers], Wu[kLayers];
-    int P, bp, Q, c, w, bw, wd, bwd;
+    int P, bp, Q, c, c2, w, bw, wd, bwd;
     int total;
 };
 ParamOffsets param_offsets();
@@ -27,6 +27,7 @@ struct HostGraph {
     std::vector<float> adj_e;            // a_ij / sqrt(a_ii a_jj)
     std::vector<int> low_ptr, low_col, low_row;  // strictly lower edges by row (k index)
     std::vector<float> low_e;
+    std::vector<float> low_f;                    // sum_{m < i, m != j} e_jm e_mi per lower edge
     std::vector<int> up_ptr, up_k, up_row;       // lower edges grouped by column
     std::vector<int> a_ptr, a_col;               // A (all entries, FP32) for the probe loss
     std::vector<float> a_val;
@@ -49,22 +50,28 @@ struct DevGraph {
     int *adj_ptr = nullptr, *adj_col = nullptr, *low_ptr = nullptr, *low_col = nullptr, *low_row = nullptr;
     int *up_ptr = nullptr, *up_k = nullptr, *up_row = nullptr, *a_ptr = nullptr, *a_col = nullptr;
     int *pos_low = nullptr, *pos_diag = nullptr;
-    float *adj_e = nullptr, *low_e = nullptr, *a_val = nullptr, *x = nullptr, *isq = nullptr;
+    float *adj_e = nullptr, *low_e = nullptr, *low_f = nullptr, *a_val = nullptr, *x = nullptr, *isq = nullptr;
     void upload(const HostGraph& g, Arena& ar, cudaStream_t st);
 };
 
 // Activations and temporaries, sized for the largest system.
+constexpr int kLossProbe = 0;    // sum ||G A G^T v - v||^2 / (K n) over K probes
+constexpr int kLossKaporin = 1;  // (1/n) sum_i [log (G A G^T)_ii - 2 log Ghat_ii]
+
 struct Work {
     int K = 0;
+    int loss_kind = kLossProbe;
     float* h[kLayers + 1] = {};
     float* s[kLayers] = {};
     float *a = nullptr, *hl = nullptr, *hu = nullptr, *ph = nullptr, *qh = nullptr;
     float *gval = nullptr, *gdiag = nullptr;           // G values (lower edges, diagonal)
-    float *zpre = nullptr, *go = nullptr, *gd = nullptr;
+    float *zpre = nullptr, *go = nullptr, *gd = nullptr, *td = nullptr;  // Ghat lower, Ghat_ii, log Ghat_ii
+    int* bad = nullptr;
     float *v = nullptr, *w1 = nullptr, *w2 = nullptr, *r = nullptr, *t = nullptr, *y = nullptr;
     float *dgo = nullptr, *dexp = nullptr;
     float *dh = nullptr, *dh2 = nullptr, *ds = nullptr, *dhl = nullptr, *dhu = nullptr, *dph = nullptr, *dqh = nullptr;
     float* partial = nullptr;
+    double* dpartial = nullptr;
     double* loss = nullptr;
     void alloc(Arena& ar, int max_n, int max_low, int K, bool train);
 };
@@ -73,8 +80,12 @@ struct Work {
 void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream_t st);
 // G values into A's CSR order of the entries with col <= row (FP64 device array, n_glow long).
 void g_to_low(const DevGraph& g, const Work& w, double* d_glow, cudaStream_t st);
-// Probe loss (into w.loss) and, when grad != nullptr, its gradient with respect to wr.
+// Rows of the predicted G (w.gval, w.gdiag) scaled to (G A G^T)_ii = 1; waits for the stream.
+void normalize_rows(const DevGraph& g, Work& w, cudaStream_t st);
+// The loss w.loss_kind selects (into w.loss) and, when grad != nullptr, its gradient with
+// respect to wr.  seed draws the probes of the probe loss.
 void loss_backward(const DevGraph& g, const float* wr, Work& w, float* grad, unsigned long long seed, cudaStream_t st);
+void backward_from_dg(const DevGraph& g, const float* wr, Work& w, float* grad, cudaStream_t st);
 void adam_step(float* theta, const float* grad, float* m, float* v, int P, float lr, int step, cudaStream_t st);
 void round_params(const float* master, float* wr, int P, cudaStream_t st);
 

@@ -5,8 +5,12 @@
 //
 // Arithmetic: every product and sum is rounded on its own (__dmul_rn/__dadd_rn: no FMA
 // contraction), which is what the reference's x86-64 build computes.  The SpMV and the
-// element-wise updates are therefore bit-identical to the reference; the dot products use
-// a fixed two-level tree (deterministic, within a few ulps of the sequential sum).
+// element-wise updates are therefore bit-identical to the reference.  The dot products
+// (dot_kernel, and r.z, r.r of init_pcg_kernel / update_xrz_kernel) are summed in the
+// reference's order, one element after the other from index 0, for n <= kSeqMaxN, so the
+// whole path is bit-identical there (the reference itself stops at n <= 1024,
+// include/cg_common.hpp:11); above that they use a fixed two-level tree (deterministic,
+// within a few ulps of the sequential sum).
 // Pointers may be device pointers or plain host pointers (staged).  Calls block until the
 // results are in place, as the reference's calls do.
 #include <cuda.h>  // CUcontext only: cuCtxGetCurrent is reached through cudaGetDriverEntryPoint
@@ -23,6 +27,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 1024;
+// Largest n whose dot products are summed sequentially (one dependent FP64 add per element,
+// about 0.1 ms at this size); larger n use the tree.
+constexpr int kSeqMaxN = 65536;
 
 __global__ void csr_spmv_f64_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
                                     const double* __restrict__ v, const double* __restrict__ x,
@@ -91,6 +98,29 @@ __global__ void vec_kernel(int mode, int n, double alpha, double* x, const doubl
         partial[2 * blockIdx.x] = s0;
         partial[2 * blockIdx.x + 1] = s1;
     }
+}
+
+// Sequential sums in the reference's order: lane 0 sums a_i * b_i, lane 1 sums c_i * d_i
+// (nout == 2), each product and each sum rounded on its own.  The products are recomputed
+// from the vectors the element-wise kernel wrote, exactly as that kernel computed them.
+__global__ void seq_dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                               const double* __restrict__ c, const double* __restrict__ d, int n,
+                               double* __restrict__ out, int nout) {
+    const int lane = threadIdx.x;
+    if (lane >= nout) return;
+    const double* u = lane == 0 ? a : c;
+    const double* v = lane == 0 ? b : d;
+    double acc = 0.0;
+    int i = 0;
+    for (; i + 8 <= n; i += 8) {
+        double q[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) q[k] = __dmul_rn(u[i + k], v[i + k]);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc = __dadd_rn(acc, q[k]);
+    }
+    for (; i < n; ++i) acc = __dadd_rn(acc, __dmul_rn(u[i], v[i]));
+    out[lane] = acc;
 }
 
 __global__ void finish_kernel(const double* partial, int nparts, double* out, int nout) {
@@ -307,6 +337,18 @@ double* noalloc_scratch() {
     return addr[dev];
 }
 
+// The dot products of a call: summed in the reference's order from the vectors (a.b, and
+// a.a with nout == 2: r.z and r.r) when n <= kSeqMaxN, else the tree over the element-wise
+// kernel's block partials.
+void finish_dots(const double* partial, int blocks, const double* a, const double* b, int n, double* out, int nout,
+                 cudaStream_t st) {
+    if (n <= kSeqMaxN)
+        seq_dot_kernel<<<1, 32, 0, st>>>(a, b, a, a, n, out, nout);
+    else
+        finish_kernel<<<1, kThreads, 0, st>>>(partial, blocks, out, nout);
+    check(cudaGetLastError(), "dot finish launch");
+}
+
 template <typename F>
 void abi_call(F&& f) {
     const int rc = guarded(f);
@@ -352,8 +394,9 @@ void init_pcg_kernel(const double* b, const double* ax, const double* m_inv, dou
             1, n, 0.0, nullptr, nullptr, static_cast<double*>(ar.dev), static_cast<const double*>(aax.dev),
             static_cast<const double*>(am.dev), static_cast<double*>(az.dev), static_cast<double*>(ap.dev),
             static_cast<const double*>(ab.dev), c.partial);
-        finish_kernel<<<1, kThreads, 0, c.stream>>>(c.partial, blocks, static_cast<double*>(amet.dev), 2);
         check(cudaGetLastError(), "init_pcg launch");
+        finish_dots(c.partial, blocks, static_cast<const double*>(ar.dev), static_cast<const double*>(az.dev), n,
+                    static_cast<double*>(amet.dev), 2, c.stream);
         unbind(c, ar); unbind(c, az); unbind(c, ap); unbind(c, amet);
         check(cudaStreamSynchronize(c.stream), "sync");
     });
@@ -370,11 +413,14 @@ void dot_kernel(const double* a, const double* b, double* out, int n) {
         Arg aa = bind(c, 0, a, vb, true, false), ab = bind(c, 1, b, vb, true, false);
         Arg ao = bind(c, 2, out, sizeof(double), false, true);
         const int blocks = blocks_for(n);
-        vec_kernel<<<blocks, kThreads, 0, c.stream>>>(
-            0, n, 0.0, static_cast<double*>(aa.dev), static_cast<const double*>(ab.dev), nullptr,
-            nullptr, nullptr, nullptr, nullptr, nullptr, c.partial);
-        finish_kernel<<<1, kThreads, 0, c.stream>>>(c.partial, blocks, static_cast<double*>(ao.dev), 1);
-        check(cudaGetLastError(), "dot launch");
+        if (n > kSeqMaxN) {
+            vec_kernel<<<blocks, kThreads, 0, c.stream>>>(
+                0, n, 0.0, static_cast<double*>(aa.dev), static_cast<const double*>(ab.dev), nullptr,
+                nullptr, nullptr, nullptr, nullptr, nullptr, c.partial);
+            check(cudaGetLastError(), "dot launch");
+        }
+        finish_dots(c.partial, blocks, static_cast<const double*>(aa.dev), static_cast<const double*>(ab.dev), n,
+                    static_cast<double*>(ao.dev), 1, c.stream);
         unbind(c, ao);
         check(cudaStreamSynchronize(c.stream), "sync");
     });
@@ -398,8 +444,9 @@ void update_xrz_kernel(double* x, const double* p, double* r, const double* ap,
             2, n, alpha, static_cast<double*>(ax.dev), static_cast<const double*>(ap_.dev),
             static_cast<double*>(ar.dev), static_cast<const double*>(aap.dev),
             static_cast<const double*>(am.dev), static_cast<double*>(az.dev), nullptr, nullptr, c.partial);
-        finish_kernel<<<1, kThreads, 0, c.stream>>>(c.partial, blocks, static_cast<double*>(amet.dev), 2);
         check(cudaGetLastError(), "update_xrz launch");
+        finish_dots(c.partial, blocks, static_cast<const double*>(ar.dev), static_cast<const double*>(az.dev), n,
+                    static_cast<double*>(amet.dev), 2, c.stream);
         unbind(c, ax); unbind(c, ar); unbind(c, az); unbind(c, amet);
         check(cudaStreamSynchronize(c.stream), "sync");
     });
@@ -433,8 +480,7 @@ int xplus_update_xrz_noalloc(double* x, const double* p, double* r, const double
         const int blocks = blocks_for(n);
         vec_kernel<<<blocks, kThreads, 0, st>>>(2, n, alpha, x, p, r, ap, m_inv, z, nullptr, nullptr, scratch);
         check(cudaGetLastError(), "update_xrz_noalloc launch");
-        finish_kernel<<<1, kThreads, 0, st>>>(scratch, blocks, metrics, 2);
-        check(cudaGetLastError(), "update_xrz_noalloc finish launch");
+        finish_dots(scratch, blocks, r, z, n, metrics, 2, st);
     });
 }
 

@@ -419,6 +419,8 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
         dxv[t] = 0.0f;
         apv[t] = 0.0f;
     }
+    // the band's p' is rebuilt from its own previous value (beta = 0 the first time)
+    for (int t = threadIdx.x; t < wn; t += blockDim.x) pw[t] = 0.0f;
     if (threadIdx.x == 0) {
         for (int k = 0; k < 5; ++k) s_clk[k] = 0;
         s_clk[5] = globaltimer_ns();
@@ -500,100 +502,117 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 status = XPLUS_BREAKDOWN;
                 break;
             }
-            // ---- apply the previous update to the band, then the new window p' ----
+            // ---- the previous update and the new p' ----
+            // Own band, from shared memory: the records this CTA published last iteration are
+            // {m r, m Ap', p'} of these very values, so p'_new = fma(beta, p', fma(-alpha, m Ap',
+            // m r)) here is bit-identical to what the neighbours rebuild from the records; then
+            // the pending update dx += alpha p', r -= alpha Ap'.  Only the halo reads records.
             const float al_prev = static_cast<float>(pend);
-            if (pend != 0.0) {
-                apply_update(al_prev);
-                if (it % flush_every == 0) flush_dx();
-                __syncthreads();
+            const bool upd = pend != 0.0;
+            const bool flush = upd && it % flush_every == 0;
+            const float be = static_cast<float>(beta);
+            for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+                float* pp = pw + (r0 + t - w0);
+                const float pv = *pp;
+                const float r_ = rv[t], ap_ = apv[t], m = mi[t];
+                const float mr = m * r_;
+                const float ma = upd ? m * ap_ : 0.0f;  // the records' m Ap' is 0 after a residual
+                *pp = __fmaf_rn(be, pv, __fmaf_rn(-al_prev, ma, mr));
+                if (upd) {
+                    const float d = __fmaf_rn(al_prev, pv, dxv[t]);
+                    rv[t] = r_ - al_prev * ap_;
+                    if (flush) {
+                        a.x64[r0 + t] += static_cast<double>(d);
+                        dxv[t] = 0.0f;
+                    } else {
+                        dxv[t] = d;
+                    }
+                }
             }
             pend = 0.0;
             {
-                const float be = static_cast<float>(beta);
+                // halo [w0, r0) and [r0 + nb, w0 + wn) from the records, in float4 groups
                 const float4* zr4 = reinterpret_cast<const float4*>(rec_zr(gen) + w0);
                 const float4* za4 = reinterpret_cast<const float4*>(rec_za(gen) + w0);
                 const float4* p4 = reinterpret_cast<const float4*>(rec_p(gen) + w0);
                 float4* pw4 = reinterpret_cast<float4*>(pw);
-                // four float4 groups per thread in flight: all twelve loads before any store
-                constexpr int U = 4;
-                const int nq = wn >> 2, bd = static_cast<int>(blockDim.x);
-                int t = threadIdx.x;
-                for (; t + (U - 1) * bd < nq; t += U * bd) {
-                    float4 z[U], q[U], p[U];
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        z[u] = zr4[t + u * bd];
-                        q[u] = za4[t + u * bd];
-                        p[u] = p4[t + u * bd];
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        float4 o;
-                        o.x = __fmaf_rn(be, p[u].x, __fmaf_rn(-al_prev, q[u].x, z[u].x));
-                        o.y = __fmaf_rn(be, p[u].y, __fmaf_rn(-al_prev, q[u].y, z[u].y));
-                        o.z = __fmaf_rn(be, p[u].z, __fmaf_rn(-al_prev, q[u].z, z[u].z));
-                        o.w = __fmaf_rn(be, p[u].w, __fmaf_rn(-al_prev, q[u].w, z[u].w));
-                        pw4[t + u * bd] = o;
-                    }
-                }
-                for (; t < nq; t += bd) {
-                    const float4 z = zr4[t], q = za4[t], p = p4[t];
+                const int nlo = (r0 - w0) >> 2;
+                const int hi0 = (r0 + nb - w0) >> 2;
+                const int nh = nlo + (wn >> 2) - hi0;
+                auto qof = [&](int u) { return u < nlo ? u : hi0 + (u - nlo); };
+                auto fill = [&](const float4& z, const float4& q, const float4& p) {
                     float4 o;
                     o.x = __fmaf_rn(be, p.x, __fmaf_rn(-al_prev, q.x, z.x));
                     o.y = __fmaf_rn(be, p.y, __fmaf_rn(-al_prev, q.y, z.y));
                     o.z = __fmaf_rn(be, p.z, __fmaf_rn(-al_prev, q.z, z.z));
                     o.w = __fmaf_rn(be, p.w, __fmaf_rn(-al_prev, q.w, z.w));
-                    pw4[t] = o;
+                    return o;
+                };
+                // four float4 groups per thread in flight: all twelve loads before any store
+                constexpr int U = 4;
+                const int bd = static_cast<int>(blockDim.x);
+                int u = threadIdx.x;
+                for (; u + (U - 1) * bd < nh; u += U * bd) {
+                    float4 z[U], q[U], p[U];
+#pragma unroll
+                    for (int v = 0; v < U; ++v) {
+                        const int qq = qof(u + v * bd);
+                        z[v] = zr4[qq];
+                        q[v] = za4[qq];
+                        p[v] = p4[qq];
+                    }
+#pragma unroll
+                    for (int v = 0; v < U; ++v) pw4[qof(u + v * bd)] = fill(z[v], q[v], p[v]);
+                }
+                for (; u < nh; u += bd) {
+                    const int qq = qof(u);
+                    pw4[qq] = fill(zr4[qq], za4[qq], p4[qq]);
                 }
                 __syncthreads();
             }
             clock(2);
-            // ---- Ap' from shared memory ----
-            for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
-                int2 sl[NS];
-                int row[NS];
-                float pi[NS], y[NS];
-#pragma unroll
-                for (int k = 0; k < NS; ++k) {
-                    const int s = s0 + k * wpb;
-                    const bool on = s < se;
-                    sl[k] = on ? s_slice[s - sb] : make_int2(0, 0);
-                    row[k] = on ? s * 32 + lane : -1;
-                    pi[k] = on ? pw[row[k] - w0] : 0.0f;
-                }
-                sell_rows_smem<VT, CHUNK, IT, NS>(sl, row, lane, col, val, pw, w0, pi, y);
-#pragma unroll
-                for (int k = 0; k < NS; ++k) {
-                    if (row[k] < 0) continue;
-                    const int t = row[k] - r0;
-                    apv[t] = y[k] * a.val_scale + rsv[t] * pi[k];
-                }
-            }
-            __syncthreads();
-            clock(3);
-            // ---- records of the next generation and the seven sums ----
+            // ---- Ap' from shared memory, then each row's records of the next generation and
+            // its terms of the seven sums (the row's own values only: no CTA barrier between) ----
             {
                 double acc[kPartials1] = {0, 0, 0, 0, 0, 0, 0};
                 const int g1 = gen ^ 1;
                 float* zr1 = rec_zr(g1);
                 float* za1 = rec_za(g1);
                 float* p1 = rec_p(g1);
-                for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-                    const float pv = pw[r0 + t - w0];
-                    const float r_ = rv[t], ap_ = apv[t], m = mi[t];
-                    const float mr = m * r_, ma = m * ap_;
-                    zr1[r0 + t] = mr;
-                    za1[r0 + t] = ma;
-                    p1[r0 + t] = pv;
-                    const double dr = r_, da = ap_, dm = m;
-                    acc[0] += static_cast<double>(pv) * da;
-                    acc[1] += dm * dr * dr;
-                    acc[2] += dm * dr * da;
-                    acc[3] += dm * da * da;
-                    acc[4] += dr * dr;
-                    acc[5] += dr * da;
-                    acc[6] += da * da;
+                for (int s0 = sb + warp; s0 < se; s0 += NS * wpb) {
+                    int2 sl[NS];
+                    int row[NS];
+                    float pi[NS], y[NS];
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        const int s = s0 + k * wpb;
+                        const bool on = s < se;
+                        sl[k] = on ? s_slice[s - sb] : make_int2(0, 0);
+                        row[k] = on ? s * 32 + lane : -1;
+                        pi[k] = on ? pw[row[k] - w0] : 0.0f;
+                    }
+                    sell_rows_smem<VT, CHUNK, IT, NS>(sl, row, lane, col, val, pw, w0, pi, y);
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) {
+                        if (row[k] < 0) continue;
+                        const int t = row[k] - r0;
+                        const float ap_ = y[k] * a.val_scale + rsv[t] * pi[k];
+                        apv[t] = ap_;
+                        const float r_ = rv[t], m = mi[t];
+                        zr1[row[k]] = m * r_;
+                        za1[row[k]] = m * ap_;
+                        p1[row[k]] = pi[k];
+                        const double dr = r_, da = ap_, dm = m;
+                        acc[0] += static_cast<double>(pi[k]) * da;
+                        acc[1] += dm * dr * dr;
+                        acc[2] += dm * dr * da;
+                        acc[3] += dm * da * da;
+                        acc[4] += dr * dr;
+                        acc[5] += dr * da;
+                        acc[6] += da * da;
+                    }
                 }
+                clock(3);
                 cur_bank = next_bank();
                 publish<kPartials1>(acc, s_red, cur_bank);
             }

@@ -1001,6 +1001,7 @@ int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
             cuda_check(cudaMemcpyAsync(master, params, static_cast<size_t>(P) * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
             gnn::round_params(master, wr, P, st);
             gnn::forward(dg, wr, w, false, st);
+            gnn::normalize_rows(dg, w, st);  // (G A G^T)_ii = 1: the network fixes only each row's direction
             gnn::g_to_low(dg, w, h->d_glow, st);
             gtg_enable(h, fallback_iters);
         } catch (...) {

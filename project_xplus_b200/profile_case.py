@@ -66,8 +66,11 @@ def main() -> None:
     for _ in range(a.spmv):
         _lib.check(_lib.lib.xplus_pcg_spmv_device(s.handle, xs, ys, None))
     y = s.spmv(np.ones(d.n))
+    ph = s.phase_times()
+    per_it = [round(1e3 * v / max(1, r.iterations), 2) for v in ph["median_ms"]]
     print(f"n={d.n} nnz={d.nnz} iterations={r.iterations} kernel_ms={r.kernel_ms:.3f} kernel={r.metrics['kernel']} "
-          f"us/iter={1e3 * r.kernel_ms / max(1, r.iterations):.2f} info={s.info()} y0={y[0]:.6e}")
+          f"us/iter={1e3 * r.kernel_ms / max(1, r.iterations):.2f} phase_us/iter(median CTA)={per_it} "
+          f"info={s.info()} y0={y[0]:.6e}")
     s.close()
 
 

@@ -252,6 +252,18 @@ class PcgSolver:
         check(lib.xplus_pcg_solve_device(self._h, ptr(d_b), ptr(d_x), float(tau), int(tau_mode),
                                          int(max_iters), s))
 
+    def phase_times(self) -> dict:
+        """Phase clock of the last solve (ms summed over its iterations): block 0's four
+        phases (xplus_pcg_last_phase_times) and the median over all CTAs of each phase
+        (xplus_pcg_last_block_times)."""
+        p = np.empty(4, np.float64)
+        check(lib.xplus_pcg_last_phase_times(self._h, ptr(p)))
+        nb = C.c_int()
+        check(lib.xplus_pcg_last_block_times(self._h, None, 0, C.byref(nb)))
+        blk = np.empty(4 * nb.value, np.float64)
+        check(lib.xplus_pcg_last_block_times(self._h, ptr(blk), nb.value, C.byref(nb)))
+        return {"block0_ms": p.tolist(), "median_ms": np.median(blk.reshape(-1, 4), axis=0).tolist()}
+
     def last_metrics(self) -> dict:
         """Outcome of the last solve (waits for it): status, iterations, replacements,
         true relative residual, kernel time and the kernel's own counters."""

@@ -11,6 +11,7 @@ if str(ROOT) not in sys.path:
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU")
     config.addinivalue_line("markers", "ref: needs the reference built from source (oracle/_ref)")
+    config.addinivalue_line("markers", "slow: takes minutes (a full-size oracle solve on one host core)")
 
 
 def pytest_collection_modifyitems(config, items):

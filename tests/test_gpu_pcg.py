@@ -147,6 +147,25 @@ def test_plain_fp32_final_x_matches_fp64_oracle(gpu, oracle, sys0):
     assert res <= 1e-12 and abs(res - r.residual_rel) <= 1e-3 * res + 1e-18
 
 
+@pytest.mark.slow
+def test_config1_final_x_matches_fp64_oracle(gpu, oracle):
+    """The 1108x1108 system (n = 1,227,664): the benchmarked FP32 kernel (FP32 values and
+    vectors, row-sum form, FP64 residual replacement) against the oracle's FP64 golden solve
+    (src/CgSolverGolden.hpp:42-124, restated), both run to 1e-12 relative residual: final x
+    within 1e-6 relative.  The oracle solve takes about four minutes on one host core."""
+    d, xt = g.system_2d_large()
+    nb = float(np.linalg.norm(d.b))
+    s = xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=4)
+    r = s.solve(d.b, None, tau=1e-12, tau_mode=xp.XPLUS_TAU_REL_TRUE, max_iters=40000)
+    s.close()
+    assert r.status == "converged" and r.residual_rel <= 1e-12, (r.status, r.iterations, r.residual_rel)
+    ref = oracle.golden(d, (1e-12 * nb) ** 2, 40000)
+    assert ref["converged"]
+    err = np.linalg.norm(r.solution - ref["x"]) / np.linalg.norm(ref["x"])
+    assert err <= 1e-6, err
+    assert oracle.residual_norm(d, r.solution) / nb <= 1e-12
+
+
 SPLIT_RATIO = {"bf16": 1.5, "f16": 2.0}  # default split_ratio of 16-bit values
 
 

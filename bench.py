@@ -694,6 +694,8 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
     # launch shape tuned for FP32
     s16 = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems], values_dtype="bf16")
     s16.set_launch(info["cluster"], info["block_threads"])
+    lane = info["split_lane"]
+    s16.set_split_lane(lane["count"], lane["cluster"], lane["block_threads"])
     for _ in range(args.warmup):
         x.zero_()
         s16.solve_device(b, x, tau=args.tol, stream=stream)
@@ -728,7 +730,7 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
             "system_ms": {"max": float(r["system_ms"].max()), "median": float(np.median(r["system_ms"])),
                           "sum": float(r["system_ms"].sum())},
             "launch": {"cluster": info["cluster"], "block_threads": info["block_threads"], "grid": info["grid"],
-                       "autotune_ms": tune["ms"]},
+                       "autotune_ms": tune["ms"], "largest_systems_lane": info["split_lane"]},
             "graph": True, "bf16_values": bf16}
 
 

@@ -256,6 +256,15 @@ int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
  * (nullable) gets the host+device time of the inference. */
 int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
                       const float* params, int fallback_iters, double* infer_ms);
+/* xplus_pcg_set_gnn (which is this with refine_sweeps = 1) with the number of refinement sweeps
+ * (0..16) run on the GPU between inference and normalization: each sweep takes the lower
+ * entries j of every row i in ascending order and sets Ghat_ij to the minimizer of the row's
+ * quadratic form (G A G^T)_ii at fixed Ghat_ii, a Gauss-Seidel step on the row's FSAI system
+ * A[P_i, P_i] g = e_i.  Every step lowers the row's Kaporin term, so a sweep never makes a row
+ * worse; it fixes rows the network cannot resolve, chiefly the two ends of a very stiff
+ * element (a_ij^2 close to a_ii a_jj), where the row's best ratio G_ij / G_ii is sharp. */
+int xplus_pcg_set_gnn_ex(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
+                         const float* params, int fallback_iters, int refine_sweeps, double* infer_ms);
 /* The handle's current G in g_low order (g_low NULL: only *n_glow). */
 int xplus_pcg_get_gtg(xplus_pcg* h, double* g_low, int64_t* n_glow);
 /* Rescales the rows of the handle's current G (learned or given) to (G A G^T)_ii = 1, the
@@ -346,11 +355,23 @@ int xplus_batch_destroy(xplus_batch* h);
 /* cluster in {1, 2, 4, 8} CTAs, block_threads in {128, 256, 512}; the grid is as many
  * clusters as the device holds at once.  XPLUS_ERR_CUDA when the shape cannot launch. */
 int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads);
+/* The `count` largest systems (by nnz * sqrt(n)) in a launch of their own, concurrent with the
+ * launch of the rest on a second stream, with clusters of `cluster` CTAs in {4, 8, 16} (16 is
+ * beyond the portable limit, allowed on B200) of block_threads threads, one cluster per system;
+ * count 0: one launch for all.  No wait spans two clusters, so the two launches need no
+ * co-residency; the largest system, which otherwise runs on a main-launch cluster for the
+ * whole makespan, gets up to 16 SMs.  XPLUS_ERR_CUDA when the shape cannot launch. */
+int xplus_batch_set_split(xplus_batch* h, int count, int cluster, int block_threads);
+/* The current split: count (0: none), cluster, block_threads and grid of its launch. */
+int xplus_batch_split_info(xplus_batch* h, int* count, int* cluster, int* block_threads, int* grid);
 /* The launch-shape autotuner: times every cluster x block_threads shape that launches and keeps
- * the fastest, with x0 = 0 for every system.  iters > 0: that many PCG iterations per system on
- * b = 1; iters <= 0: every system solved to FP64 true relative residual tau (0 < tau < 1) on the
- * right-hand side of the last solve (b = 1 before any solve), so the queue's makespan on the
- * caller's workload is what is timed.  Returns the shape and its time (min of 2 runs). */
+ * the fastest, with x0 = 0 for every system; then, on that shape, splits off the 1, 2, 4, 8 or
+ * 16 largest systems (at most a quarter of them) into clusters of 16 x 512, 8 x 512 or 16 x 256
+ * and keeps a split when it is faster (xplus_batch_split_info reports it).  iters > 0: that many
+ * PCG iterations per system on b = 1; iters <= 0: every system solved to FP64 true relative
+ * residual tau (0 < tau < 1) on the right-hand side of the last solve (b = 1 before any solve),
+ * so the queue's makespan on the caller's workload is what is timed.  Returns the main shape
+ * and the best time (min of 2 runs). */
 int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, int* block_threads,
                          double* best_ms);
 /* Blocking solve with host vectors of length sum(ns) (x0 NULL: zeros).  tau / tau_mode /

@@ -249,6 +249,30 @@ def kaporin_loss_and_grad(theta, g, round_bf16=True):
     return L, _backward(g, cache, dgo, dexp)
 
 
+def refine_rows(g, go, gd, sweeps=1):
+    """Gauss-Seidel sweeps on each row's quadratic form ghat^T A^[P_i, P_i] ghat at fixed
+    Ghat_ii: for the lower entries j of row i in ascending order, ghat_ij -= (A^ ghat_i)_j
+    (A^_jj = 1).  Returns the new lower values (graph order); the diagonal is unchanged."""
+    n = g["n"]
+    lr, lc = g["lr"], g["lc"]
+    cnt = np.bincount(lr, minlength=n)
+    lptr = np.concatenate([[0], np.cumsum(cnt)])
+    Ah = scaled_matrix(g)
+    go = np.array(go, np.float64)
+    for _ in range(sweeps):
+        for k in range(int(cnt.max()) if n else 0):
+            rows = np.nonzero(cnt > k)[0]
+            e_k = lptr[rows] + k                    # the entry being set, row by row
+            j = lc[e_k]
+            u = gd[rows] * np.asarray(Ah[j, rows]).ravel()   # the diagonal entry of the pattern
+            for q in range(int(cnt.max())):
+                has = cnt[rows] > q
+                eq = lptr[rows[has]] + q
+                u[has] += go[eq] * np.asarray(Ah[j[has], lc[eq]]).ravel()
+            go[e_k] -= u
+    return go
+
+
 def normalize_rows(g, go, gd):
     """Rows of Ghat scaled to (G A G^T)_ii = 1 (what the solver applies after inference)."""
     B, _, _ = kaporin_terms(g, go, gd)

@@ -102,6 +102,7 @@ _SIGS = {
     "xplus_update_xrz_noalloc": (_i, [_p, _p, _p, _p, _p, _p, _p, _d, _i, _p]),
     "xplus_pcg_set_gtg": (_i, [_p, _p, _p, _p, _i]),
     "xplus_pcg_set_gnn": (_i, [_p, _p, _p, _p, _p, _i, _dp]),
+    "xplus_pcg_set_gnn_ex": (_i, [_p, _p, _p, _p, _p, _i, _i, _dp]),
     "xplus_pcg_get_gtg": (_i, [_p, _p, C.POINTER(_i64)]),
     "xplus_pcg_scale_gtg": (_i, [_p, _p, _p, _p]),
     "xplus_fsai_lower": (_i, [_i, _p, _p, _p, _p]),
@@ -120,6 +121,8 @@ _SIGS = {
     "xplus_batch_create": (_i, [_i, _p, _p, _p, _p, C.POINTER(XplusOpts), C.POINTER(_p)]),
     "xplus_batch_destroy": (_i, [_p]),
     "xplus_batch_set_launch": (_i, [_p, _i, _i]),
+    "xplus_batch_set_split": (_i, [_p, _i, _i, _i]),
+    "xplus_batch_split_info": (_i, [_p, _ip, _ip, _ip, _ip]),
     "xplus_batch_autotune": (_i, [_p, _i, _d, _ip, _ip, _dp]),
     "xplus_batch_solve": (_i, [_p, _p, _p, _d, _i, _i, _p]),
     "xplus_batch_solve_device": (_i, [_p, _p, _p, _d, _i, _i, _p]),

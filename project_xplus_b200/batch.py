@@ -90,16 +90,26 @@ class BatchSolver:
         check(lib.xplus_batch_info(self._h, C.byref(n), C.byref(nnz), C.byref(cl), C.byref(tpb), C.byref(grid),
                                    C.byref(sp)))
         return dict(total_n=n.value, total_nnz=nnz.value, cluster=cl.value, block_threads=tpb.value,
-                    grid=grid.value, spmv_bytes=sp.value)
+                    grid=grid.value, spmv_bytes=sp.value, split_lane=self.split_lane())
+
+    def set_split_lane(self, count: int, cluster: int = 16, block_threads: int = 512) -> None:
+        """The `count` largest systems in a concurrent launch of their own (0: none)."""
+        check(lib.xplus_batch_set_split(self._h, int(count), int(cluster), int(block_threads)))
+
+    def split_lane(self) -> dict:
+        k, cl, tpb, grid = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib.xplus_batch_split_info(self._h, C.byref(k), C.byref(cl), C.byref(tpb), C.byref(grid)))
+        return dict(count=k.value, cluster=cl.value, block_threads=tpb.value, grid=grid.value)
 
     def set_launch(self, cluster: int, block_threads: int) -> None:
         check(lib.xplus_batch_set_launch(self._h, int(cluster), int(block_threads)))
 
     def autotune(self, iters: int = 0, tau: float = 1e-8) -> dict:
-        """Launch shape: fixed `iters` iterations per system, or (iters=0) full solves to tau."""
+        """Launch shape, then the lane of the largest systems: fixed `iters` iterations per
+        system, or (iters=0) full solves to tau."""
         cl, tpb, ms = C.c_int(), C.c_int(), C.c_double()
         check(lib.xplus_batch_autotune(self._h, int(iters), float(tau), C.byref(cl), C.byref(tpb), C.byref(ms)))
-        return dict(cluster=cl.value, block_threads=tpb.value, ms=ms.value)
+        return dict(cluster=cl.value, block_threads=tpb.value, ms=ms.value, split_lane=self.split_lane())
 
     def split(self, x) -> list[np.ndarray]:
         return [x[self.offsets[k]:self.offsets[k + 1]] for k in range(self.nsys)]

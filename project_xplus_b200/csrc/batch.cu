@@ -37,8 +37,9 @@ using namespace dev;
 
 struct BatchArgs {
     int nsys;
+    int q_begin, q_end;       // this launch takes queue positions [q_begin, q_end)
     const int* order;         // queue: system ids in the order they are taken
-    int* head;                // queue head (atomic), zero at launch
+    int* head;                // this launch's queue head (atomic), zero at launch
     const int* sys_slice0;    // [nsys + 1] first global slice of each system
     const int* sys_n;         // rows of each system
     const float* sys_scale;   // stored off-diagonal value = a_ij / scale (FP16), else 1
@@ -139,11 +140,11 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
     int pbank = 0, ibank = 0;
 
     for (;;) {
-        if (crank == 0 && threadIdx.x == 0) s_item[ibank] = atomicAdd(a.head, 1);
+        if (crank == 0 && threadIdx.x == 0) s_item[ibank] = a.q_begin + atomicAdd(a.head, 1);
         cl.sync();
         const int qi = *cl.map_shared_rank(&s_item[ibank], 0);
         ibank ^= 1;
-        if (qi >= a.nsys) {
+        if (qi >= a.q_end) {
             // every CTA has read rank 0's queue item before any CTA of the cluster exits: a
             // CTA's shared memory must outlive all distributed-shared-memory reads of it
             cl.sync();
@@ -443,6 +444,11 @@ struct xplus_batch {
     bool idx16 = true;
     xplus::BatchKernel kernel = nullptr;
     int cluster = 4, tpb = 512, grid = 0;
+    // the `split` largest systems in a launch of their own (clusters of cluster2 CTAs of tpb2
+    // threads, one cluster per system) on a second stream, beside the launch of the rest
+    int split = 0, cluster2 = 16, tpb2 = 512, grid2 = 0;
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<int> sys_n;
     std::vector<int64_t> sys_off;   // original-order offsets of each system in b / x
     // device data
@@ -477,7 +483,7 @@ struct xplus_batch {
     const double* g_b = nullptr;
     double* g_x = nullptr;
     double g_tau = 0.0;
-    int g_mode = -1, g_iters = 0, g_cluster = 0, g_tpb = 0;
+    int g_mode = -1, g_iters = 0, g_cluster = 0, g_tpb = 0, g_split = -1, g_cluster2 = 0, g_tpb2 = 0;
     bool pending = false;
     bool have_b = false;   // d_b64 holds the (gathered) right-hand side of a solve
     double last_ms = 0.0;
@@ -517,8 +523,12 @@ void batch_destroy(xplus_batch* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     for (void* p : h->allocations) cudaFree(p);
+    if (h->stream2) cudaStreamSynchronize(h->stream2);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->stream2) cudaStreamDestroy(h->stream2);
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaGetLastError();
     delete h;
@@ -542,6 +552,22 @@ int active_clusters(xplus_batch* h, int cluster, int tpb) {
         return 0;
     }
     return num;
+}
+
+void set_split(xplus_batch* h, int count, int cluster, int tpb) {
+    require(count >= 0 && count <= h->nsys, XPLUS_ERR_ARG, "split count must be in [0, nsys]");
+    require(cluster == 4 || cluster == 8 || cluster == 16, XPLUS_ERR_ARG, "split cluster must be 4, 8 or 16");
+    require(tpb == 128 || tpb == 256 || tpb == 512, XPLUS_ERR_ARG, "block_threads must be 128, 256 or 512");
+    if (count == 0) {
+        h->split = 0;
+        return;
+    }
+    const int num = active_clusters(h, cluster, tpb);
+    require(num > 0, XPLUS_ERR_CUDA, "split cluster shape not launchable on this device");
+    h->split = count;
+    h->cluster2 = cluster;
+    h->tpb2 = tpb;
+    h->grid2 = std::min(num, count) * cluster;
 }
 
 void set_launch(xplus_batch* h, int cluster, int tpb) {
@@ -691,6 +717,10 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
         h->idx16 = idx16;
         h->kernel = pick_kernel(o.value_type, o.chunk, idx16);
         require(h->kernel != nullptr, XPLUS_ERR_ARG, "no batch kernel for these options");
+        // clusters of 16 CTAs (beyond the portable 8) for the lane of the largest systems
+        if (cudaFuncSetAttribute(reinterpret_cast<const void*>(h->kernel),
+                                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+            cudaGetLastError();  // then 16 is simply not launchable (active_clusters returns 0)
 
         // concatenated host image
         const size_t R = static_cast<size_t>(h->rows);
@@ -750,12 +780,15 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
         });
 
         bcheck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        bcheck(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking), "cudaStreamCreate");
         bcheck(cudaEventCreate(&h->ev0), "cudaEventCreate");
         bcheck(cudaEventCreate(&h->ev1), "cudaEventCreate");
+        bcheck(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+        bcheck(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "cudaEventCreate");
         std::vector<int> sysn(ns, ns + nsys);
         std::vector<float> rsf(rs.begin(), rs.end()), mif(mi.begin(), mi.end());
         h->d_order = balloc<int>(h, order.size());
-        h->d_head = balloc<int>(h, 1);
+        h->d_head = balloc<int>(h, 2);
         h->d_slice0 = balloc<int>(h, slice0.size());
         h->d_sysn = balloc<int>(h, sysn.size());
         h->d_scale = balloc<float>(h, scale.size());
@@ -838,19 +871,38 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     a.out_repl = h->d_repl;
     a.out_true_rel = h->d_true_rel;
     a.out_ns = h->d_ns;
-    bcheck(cudaMemsetAsync(h->d_head, 0, sizeof(int), st), "memset");
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(tpb);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    bcheck(cudaLaunchKernelEx(&cfg, h->kernel, a), "batch PCG launch");
+    bcheck(cudaMemsetAsync(h->d_head, 0, 2 * sizeof(int), st), "memset");
+    auto launch = [&](const BatchArgs& args, int c, int t, int g, cudaStream_t s, const char* what) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(g);
+        cfg.blockDim = dim3(t);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        bcheck(cudaLaunchKernelEx(&cfg, h->kernel, args), what);
+    };
+    const int split = std::min(h->split, h->nsys);
+    if (split > 0) {
+        // the largest systems first, on the second stream (fork / join through events, which
+        // stream capture turns into parallel graph branches); no wait crosses the launches
+        BatchArgs big = a;
+        big.q_begin = 0;
+        big.q_end = split;
+        big.head = h->d_head + 1;
+        bcheck(cudaEventRecord(h->ev_fork, st), "event");
+        bcheck(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0), "wait");
+        launch(big, h->cluster2, h->tpb2, h->grid2, h->stream2, "batch PCG launch (largest systems)");
+        bcheck(cudaEventRecord(h->ev_join, h->stream2), "event");
+    }
+    a.q_begin = split;
+    a.q_end = h->nsys;
+    launch(a, cluster, tpb, grid, st, "batch PCG launch");
+    if (split > 0) bcheck(cudaStreamWaitEvent(st, h->ev_join, 0), "wait");
 }
 
 void check_tau(double tau, int tau_mode) {
@@ -905,6 +957,14 @@ int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads) {
     });
 }
 
+int xplus_batch_set_split(xplus_batch* h, int count, int cluster, int block_threads) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        set_split(h, count, cluster, block_threads);
+    });
+}
+
 int xplus_batch_solve(xplus_batch* h, const double* b, const double* x0, double tau, int tau_mode,
                       int max_iters, double* x_out) {
     return guarded([&] {
@@ -937,7 +997,8 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
         require_device_memory(d_x, h->device, "d_x");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
         const bool same = h->gexec && h->g_b == d_b && h->g_x == d_x && h->g_tau == tau && h->g_mode == tau_mode &&
-                          h->g_iters == max_iters && h->g_cluster == h->cluster && h->g_tpb == h->tpb;
+                          h->g_iters == max_iters && h->g_cluster == h->cluster && h->g_tpb == h->tpb &&
+                          h->g_split == h->split && h->g_cluster2 == h->cluster2 && h->g_tpb2 == h->tpb2;
         if (!same) {
             if (h->gexec) {
                 bcheck(cudaGraphExecDestroy(h->gexec), "graph destroy");
@@ -965,6 +1026,9 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
             h->g_iters = max_iters;
             h->g_cluster = h->cluster;
             h->g_tpb = h->tpb;
+            h->g_split = h->split;
+            h->g_cluster2 = h->cluster2;
+            h->g_tpb2 = h->tpb2;
         }
         bcheck(cudaEventRecord(h->ev0, st), "event");
         bcheck(cudaGraphLaunch(h->gexec, st), "graph launch");
@@ -1015,6 +1079,26 @@ int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, in
             bcheck(cudaStreamSynchronize(st), "sync");
             bcheck(cudaMemcpy(ones.data(), h->d_b64, ones.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
         }
+        // best of two launches of the current split with main shape (c, t)
+        auto time_shape = [&](int c, int t, int num) {
+            double ms_min = 1e300;
+            for (int rep = 0; rep < 2; ++rep) {
+                bcheck(cudaMemcpyAsync(h->d_b64, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+                bcheck(cudaMemsetAsync(h->d_x64, 0, ones.size() * sizeof(double), st), "memset");
+                bcheck(cudaEventRecord(h->ev0, st), "event");
+                if (fixed) enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, c, t, num * c, st);
+                else enqueue_kernel(h, tau, XPLUS_TAU_REL_TRUE, 0, c, t, num * c, st);
+                bcheck(cudaEventRecord(h->ev1, st), "event");
+                bcheck(cudaEventSynchronize(h->ev1), "sync");
+                float ms = 0.0f;
+                bcheck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
+                ms_min = std::min(ms_min, static_cast<double>(ms));
+            }
+            return ms_min;
+        };
+        // stage 1: the main launch's shape, every system in it
+        const int split0 = h->split, c20 = h->cluster2, t20 = h->tpb2;
+        h->split = 0;
         double best = 1e300;
         int bc = h->cluster, bt = h->tpb;
         const int clusters[4] = {1, 2, 4, 8};
@@ -1023,30 +1107,51 @@ int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, in
             for (int t : threads) {
                 const int num = active_clusters(h, c, t);
                 if (num <= 0) continue;
-                double ms_min = 1e300;
-                for (int rep = 0; rep < 2; ++rep) {
-                    bcheck(cudaMemcpyAsync(h->d_b64, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
-                    bcheck(cudaMemsetAsync(h->d_x64, 0, ones.size() * sizeof(double), st), "memset");
-                    bcheck(cudaEventRecord(h->ev0, st), "event");
-                    if (fixed) enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, c, t, num * c, st);
-                    else enqueue_kernel(h, tau, XPLUS_TAU_REL_TRUE, 0, c, t, num * c, st);
-                    bcheck(cudaEventRecord(h->ev1, st), "event");
-                    bcheck(cudaEventSynchronize(h->ev1), "sync");
-                    float ms = 0.0f;
-                    bcheck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
-                    ms_min = std::min(ms_min, static_cast<double>(ms));
-                }
-                if (ms_min < best) {
-                    best = ms_min;
+                const double ms = time_shape(c, t, num);
+                if (ms < best) {
+                    best = ms;
                     bc = c;
                     bt = t;
                 }
             }
         require(best < 1e300, XPLUS_ERR_CUDA, "no launchable cluster shape");
         set_launch(h, bc, bt);
+        // stage 2: the largest systems in a lane of their own with bigger clusters, beside the
+        // rest on that shape (the largest system otherwise sets the makespan on its own)
+        int bs = 0, bc2 = c20, bt2 = t20;
+        (void)split0;
+        {
+            const int counts[5] = {1, 2, 4, 8, 16};
+            const int shapes2[3][2] = {{16, 512}, {8, 512}, {16, 256}};
+            for (int k : counts) {
+                if (k > h->nsys / 4) break;
+                for (const auto& sh : shapes2) {
+                    if (active_clusters(h, sh[0], sh[1]) <= 0) continue;
+                    set_split(h, k, sh[0], sh[1]);
+                    const double ms = time_shape(h->cluster, h->tpb, h->grid / h->cluster);
+                    if (ms < best) {
+                        best = ms;
+                        bs = k;
+                        bc2 = sh[0];
+                        bt2 = sh[1];
+                    }
+                }
+            }
+        }
+        set_split(h, bs, bc2, bt2);
         if (cluster) *cluster = bc;
         if (block_threads) *block_threads = bt;
         if (best_ms) *best_ms = best;
+    });
+}
+
+int xplus_batch_split_info(xplus_batch* h, int* count, int* cluster, int* block_threads, int* grid) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        if (count) *count = h->split;
+        if (cluster) *cluster = h->cluster2;
+        if (block_threads) *block_threads = h->tpb2;
+        if (grid) *grid = h->split > 0 ? h->grid2 : 0;
     });
 }
 

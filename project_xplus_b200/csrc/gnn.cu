@@ -198,6 +198,46 @@ __device__ __forceinline__ float kap_u(int i, int pos, int m, int lp, const int*
     return u;
 }
 
+// One Gauss-Seidel sweep on each row's quadratic form g^T A^[P_i, P_i] g with Ghat_ii held:
+// for the lower entries j of row i in ascending order, ghat_ij -= (A^ ghat_i)_j, the exact
+// minimizer in that coordinate (A^_jj = 1).  Every step lowers (G A G^T)_ii at a fixed Ghat_ii,
+// so every row's Kaporin term log (G A G^T)_ii - 2 log Ghat_ii decreases (or stays): a strongly
+// coupled pair (a_ij^2 close to a_ii a_jj), whose best ratio ghat_ij / ghat_ii = -e_ij the
+// network cannot resolve to the precision the near-singular block needs, is set exactly.
+// Thread per row; the row's values are read back after this thread's own writes, so they go
+// through plain (coherent) loads.  gval follows go (gval = go / sqrt(a_jj)).
+__device__ __forceinline__ float kap_u_rw(int i, int pos, int m, int lp, const int* __restrict__ low_col,
+                                          const float* go, float gdi, const int* __restrict__ adj_ptr,
+                                          const int* __restrict__ adj_col, const float* __restrict__ adj_e) {
+    const int j = pos < m - 1 ? low_col[lp + pos] : i;
+    float u = pos < m - 1 ? go[lp + pos] : gdi;
+    int t = 0;
+    for (int q = adj_ptr[j]; q < adj_ptr[j + 1]; ++q) {
+        const int c = adj_col[q];
+        if (c > i) break;
+        while (t < m - 1 && low_col[lp + t] < c) ++t;
+        const int pc = t < m - 1 ? low_col[lp + t] : i;
+        if (pc == c) u = fmaf(adj_e[q], t < m - 1 ? go[lp + t] : gdi, u);
+    }
+    return u;
+}
+
+__global__ void k_row_sweep(const int* __restrict__ low_ptr, const int* __restrict__ low_col,
+                            const int* __restrict__ adj_ptr, const int* __restrict__ adj_col,
+                            const float* __restrict__ adj_e, const float* __restrict__ isq, float* go,
+                            const float* __restrict__ gd, float* __restrict__ gval, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int lp = low_ptr[i];
+    const int m = low_ptr[i + 1] - lp + 1;
+    const float gdi = gd[i];
+    for (int pos = 0; pos < m - 1; ++pos) {
+        const float v = go[lp + pos] - kap_u_rw(i, pos, m, lp, low_col, go, gdi, adj_ptr, adj_col, adj_e);
+        go[lp + pos] = v;
+        gval[lp + pos] = v * isq[low_col[lp + pos]];
+    }
+}
+
 // mode 0 (training): rowloss_i = log B_i - 2 t_i; dgo_k = 2 u_j / (n B_i) on the lower edges,
 //   dexp_i = 2 u_i gd_i / (n B_i) - 2 / n on the diagonal (dL/dt_i).
 // mode 1 (inference): rows of G (gval, gdiag) scaled by 1 / sqrt(B_i), so (G A G^T)_ii = 1.
@@ -877,6 +917,14 @@ void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream
     k_head<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.low_col, g.low_e, g.low_f, w.ph, w.qh, w.h[kLayers], g.isq, wr, off,
                                          train ? w.zpre : nullptr, w.go, w.gval, w.gd, w.td, w.gdiag, n);
     kcheck("gnn head");
+}
+
+void refine_rows(const DevGraph& g, Work& w, int sweeps, cudaStream_t st) {
+    for (int k = 0; k < sweeps; ++k) {
+        k_row_sweep<<<blocks_for(g.n, 128), 128, 0, st>>>(g.low_ptr, g.low_col, g.adj_ptr, g.adj_col, g.adj_e, g.isq,
+                                                          w.go, w.gd, w.gval, g.n);
+        kcheck("gnn row sweep");
+    }
 }
 
 void normalize_rows(const DevGraph& g, Work& w, cudaStream_t st) {

@@ -80,6 +80,9 @@ struct Work {
 void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream_t st);
 // G values into A's CSR order of the entries with col <= row (FP64 device array, n_glow long).
 void g_to_low(const DevGraph& g, const Work& w, double* d_glow, cudaStream_t st);
+// `sweeps` Gauss-Seidel sweeps over each row of the predicted Ghat (w.go, w.gval) on the row's
+// quadratic form g^T A^[P_i, P_i] g at fixed Ghat_ii: every row's Kaporin term decreases.
+void refine_rows(const DevGraph& g, Work& w, int sweeps, cudaStream_t st);
 // Rows of the predicted G (w.gval, w.gdiag) scaled to (G A G^T)_ii = 1; waits for the stream.
 void normalize_rows(const DevGraph& g, Work& w, cudaStream_t st);
 // The loss w.loss_kind selects (into w.loss) and, when grad != nullptr, its gradient with

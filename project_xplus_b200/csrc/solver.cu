@@ -979,9 +979,15 @@ int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
 
 int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
                       const float* params, int fallback_iters, double* infer_ms) {
+    return xplus_pcg_set_gnn_ex(h, row_ptr, col_idx, values, params, fallback_iters, 1, infer_ms);
+}
+
+int xplus_pcg_set_gnn_ex(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
+                         const float* params, int fallback_iters, int refine_sweeps, double* infer_ms) {
     return guarded([&] {
         require(h && values && params, XPLUS_ERR_ARG, "null argument");
         require(fallback_iters >= 0, XPLUS_ERR_ARG, "fallback_iters must be >= 0");
+        require(refine_sweeps >= 0 && refine_sweeps <= 16, XPLUS_ERR_ARG, "refine_sweeps must be in [0, 16]");
         cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
         gtg_layout(h, row_ptr, col_idx);
         const auto t0 = std::chrono::steady_clock::now();
@@ -1001,6 +1007,7 @@ int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
             cuda_check(cudaMemcpyAsync(master, params, static_cast<size_t>(P) * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
             gnn::round_params(master, wr, P, st);
             gnn::forward(dg, wr, w, false, st);
+            gnn::refine_rows(dg, w, refine_sweeps, st);
             gnn::normalize_rows(dg, w, st);  // (G A G^T)_ii = 1: the network fixes only each row's direction
             gnn::g_to_low(dg, w, h->d_glow, st);
             gtg_enable(h, fallback_iters);

@@ -42,6 +42,7 @@ def main() -> None:
     ap.add_argument("--values", default="f32")
     ap.add_argument("--vectors", default="f32")
     ap.add_argument("--chunk", type=int, default=4)
+    ap.add_argument("--sigma", type=int, default=256, help="SELL sort window")
     ap.add_argument("--dim3", type=int, default=0, help="use the 3D P1-FEM system with this grid side instead")
     ap.add_argument("--plain", action="store_true",
                     help="plain layout: values with the diagonal, int32 columns (no row-sum form)")
@@ -53,7 +54,7 @@ def main() -> None:
         return
     d, _ = g.system_3d(a.dim3) if a.dim3 else g.system_2d_large(a.grid)
     extra = dict(row_sum_form=False, index16=False) if a.plain else {}
-    s = PcgSolver.from_dataset(d, values_dtype=a.values, vector_dtype=a.vectors, chunk=a.chunk, **extra)
+    s = PcgSolver.from_dataset(d, values_dtype=a.values, vector_dtype=a.vectors, chunk=a.chunk, sigma=a.sigma, **extra)
     if a.gtg == "fsai":
         from .learned import fsai_lower
         s.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))

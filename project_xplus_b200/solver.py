@@ -280,16 +280,17 @@ class PcgSolver:
         g = None if g_low is None else np.ascontiguousarray(g_low, np.float64)
         check(lib.xplus_pcg_set_gtg(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(g), int(fallback_iters)))
 
-    def set_gnn(self, params=None, fallback_iters: int = 0) -> float:
+    def set_gnn(self, params=None, fallback_iters: int = 0, refine_sweeps: int = 1) -> float:
         """M^-1 = G^T G with G predicted on the GPU by the learned network (default: the
-        shipped weights).  Returns the inference time in ms."""
+        shipped weights), refined by `refine_sweeps` Gauss-Seidel sweeps on each row's quadratic
+        form and normalized to (G A G^T)_ii = 1.  Returns the inference time in ms."""
         from .learned import load_weights
         if params is None:
             params, _ = load_weights()
         p = np.ascontiguousarray(params, np.float32)
         ms = C.c_double()
-        check(lib.xplus_pcg_set_gnn(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), ptr(p),
-                                    int(fallback_iters), C.byref(ms)))
+        check(lib.xplus_pcg_set_gnn_ex(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(self.values), ptr(p),
+                                       int(fallback_iters), int(refine_sweeps), C.byref(ms)))
         return ms.value
 
     def scale_gtg(self) -> None:

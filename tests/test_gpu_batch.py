@@ -130,6 +130,40 @@ def test_device_graph_path_rejects_host_pointers(gpu, batch_systems):
     assert list(s.results()["status"]) == [0] * len(SPECS)
 
 
+@pytest.mark.parametrize("count,cluster,tpb", [(1, 16, 512), (2, 8, 512), (7, 16, 256)])
+def test_lane_of_the_largest_systems(gpu, batch_systems, count, cluster, tpb):
+    """The largest systems in a concurrent launch of their own with bigger clusters (16 CTAs is
+    beyond the portable limit): every system still reaches the tolerance, the split systems'
+    iteration counts stay within the dot-product rounding of the one-launch solve, and the
+    graph-captured device path agrees with the host path bit for bit."""
+    import torch
+    s = _make(batch_systems)
+    b = _b(batch_systems)
+    one = s.solve(b, tau=1e-8)
+    s.set_split_lane(count, cluster, tpb)
+    lane = s.split_lane()
+    assert lane["count"] == count and lane["cluster"] == cluster and lane["grid"] % cluster == 0
+    two = s.solve(b, tau=1e-8)
+    assert list(two["status"]) == [0] * len(SPECS)
+    assert np.all(two["true_rel"] <= 1e-8)
+    for k in range(len(SPECS)):
+        assert abs(int(two["iterations"][k]) - int(one["iterations"][k])) <= max(3, 0.03 * one["iterations"][k])
+    for (d, _), x in zip(batch_systems, s.split(two["x"])):
+        assert np.linalg.norm(d.b - _spmv(d, x)) / np.linalg.norm(d.b) <= 1.5e-8
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros_like(d_b)
+    st = torch.cuda.Stream()
+    for _ in range(2):
+        d_x.zero_()
+        torch.cuda.synchronize()
+        s.solve_device(d_b, d_x, tau=1e-8, stream=st)
+        st.synchronize()
+        np.testing.assert_array_equal(d_x.cpu().numpy(), two["x"])
+    s.set_split_lane(0)
+    assert s.split_lane()["count"] == 0
+    s.close()
+
+
 def test_launch_shapes_and_autotune(gpu, batch_systems):
     from project_xplus_b200 import XplusError
     from project_xplus_b200.batch import autotune_build

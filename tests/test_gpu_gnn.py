@@ -258,28 +258,36 @@ def test_gtg_with_fsai_matches_fp64_pcg(gpu, sys64):
 
 
 def test_solver_inference_matches_trainer(trainer):
-    """The solver's inference is the trainer's forward pass with every row then scaled on the
-    GPU to (G A G^T)_ii = 1: against the oracle's forward and row normalization, and the
-    normalization itself checked in FP64 on the host."""
+    """The solver's inference is the trainer's forward pass, then (by default) one Gauss-Seidel
+    sweep on every row's quadratic form, then every row scaled on the GPU to (G A G^T)_ii = 1:
+    against the oracle's forward, sweep and row normalization, and the normalization itself
+    checked in FP64 on the host."""
     from project_xplus_b200 import PcgSolver
     t, syss = trainer
     theta = _params(4)
     t.set_params(theta)
+    A_of = lambda d: sp.csr_matrix((d.values, d.col_idx, d.row_ptr), shape=(d.n, d.n))  # noqa: E731
     for k, d in enumerate(syss):
-        s = PcgSolver(d.row_ptr, d.col_idx, d.values)
-        s.set_gnn(theta)
-        got = s.get_gtg()
         g = O.graph(d.row_ptr, d.col_idx, d.values)
         go, gd, _ = O.forward(theta.astype(np.float64), g, round_bf16=True)
+        s = PcgSolver(d.row_ptr, d.col_idx, d.values)
+        # no sweep: the network's rows, normalized
+        s.set_gnn(theta, refine_sweeps=0)
+        got = s.get_gtg()
         ref = _glow_from_oracle(d, *O.normalize_rows(g, go, gd))
         np.testing.assert_allclose(got, ref, rtol=5e-4, atol=5e-5 * np.abs(ref).max())
-        A = sp.csr_matrix((d.values, d.col_idx, d.row_ptr), shape=(d.n, d.n))
         G = _gmat(d, got)
-        np.testing.assert_allclose((G @ A @ G.T).diagonal(), 1.0, rtol=2e-5)
-        # the unnormalized trainer output has the same row directions
-        raw = _gmat(d, t.predict(k))
+        np.testing.assert_allclose((G @ A_of(d) @ G.T).diagonal(), 1.0, rtol=2e-5)
+        raw = _gmat(d, t.predict(k))  # the trainer's output has the same row directions
         ratio = np.asarray(G.multiply(raw).sum(axis=1)).ravel() / np.asarray(raw.multiply(raw).sum(axis=1)).ravel()
         np.testing.assert_allclose(G.toarray(), (sp.diags(ratio) @ raw).toarray(), rtol=1e-5, atol=1e-6 * abs(got).max())
+        # the default: one sweep, then normalization
+        s.set_gnn(theta)
+        got1 = s.get_gtg()
+        ref1 = _glow_from_oracle(d, *O.normalize_rows(g, O.refine_rows(g, go, gd, 1), gd))
+        np.testing.assert_allclose(got1, ref1, rtol=1e-3, atol=1e-4 * np.abs(ref1).max())
+        G1 = _gmat(d, got1)
+        np.testing.assert_allclose((G1 @ A_of(d) @ G1.T).diagonal(), 1.0, rtol=2e-5)
         s.close()
 
 

@@ -476,10 +476,25 @@ int xplus_gen_fem3d(int g, double sigma, double jitter, uint64_t seed, int64_t p
 
 /* Reverse Cuthill-McKee ordering of a structurally symmetric CSR: perm[new] = old. */
 int xplus_rcm(int n, const int* row_ptr, const int* col_idx, int* perm);
+/* The same reverse Cuthill-McKee ordering computed on the GPU from a device CSR, bit-identical
+ * to xplus_rcm: one cooperative launch per BFS builds the Cuthill-McKee levels in parallel
+ * (each node of the next level goes to its lowest-positioned neighbour in the current level,
+ * each parent's children ordered by (degree, index)), the pseudo-peripheral search and the
+ * component order as xplus_rcm has them.  A graph it does not cover (a node with more than 64
+ * children in one level, or a repeated column in a row) is ordered by the host function instead,
+ * with the same result; *used_gpu (nullable) says which ran.  Device pointers of the current
+ * GPU; blocks until d_perm is written.  No reference counterpart (the reference orders on the
+ * host while packing, host/cuper_control_matrix.hpp:130-207). */
+int xplus_rcm_device(int n, const int* d_row_ptr, const int* d_col_idx, int* d_perm, int* used_gpu, void* stream);
 /* B = P A P^T for perm[new] = old (columns sorted ascending in each output row). */
 int xplus_permute_symmetric(int n, const int* row_ptr, const int* col_idx, const double* values,
                             const int* perm, int* out_row_ptr, int* out_col_idx,
                             double* out_values);
+/* xplus_permute_symmetric on device arrays (thread per output row, stable ordering of the
+ * renumbered columns), bit-identical to it; blocks until the outputs are written. */
+int xplus_permute_symmetric_device(int n, const int* d_row_ptr, const int* d_col_idx, const double* d_values,
+                                   const int* d_perm, int* d_out_row_ptr, int* d_out_col_idx,
+                                   double* d_out_values, void* stream);
 
 /* SELL-C-sigma layout (host builder; the device copies come from the same function).
  * Two-phase: pass NULL outputs to get n_slices, slots.  perm[new] = old row,

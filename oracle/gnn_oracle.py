@@ -23,8 +23,10 @@ Losses: the probe loss over K vectors v ~ N(0, I), L = sum_p ||G A G^T v_p - v_p
 and the row-normalized Kaporin loss L = (1/n) sum_i [log (G A G^T)_ii - 2 log Ghat_ii]
 (kaporin_loss; the network is trained with it, and the solver scales G's rows to
 (G A G^T)_ii = 1 after inference).
-The forward pass uses the parameters rounded to BF16 (round to nearest even); gradients are
-taken with respect to the rounded values and applied to the FP32 master copy.
+The forward pass uses the parameters rounded to BF16 (round to nearest even), and the node
+products W h and D W take their node operand rounded to BF16 too (they run on the tensor
+cores, FP32 accumulation); gradients are taken with respect to the rounded values and applied
+to the FP32 master copy.
 """
 from __future__ import annotations
 
@@ -118,20 +120,30 @@ def _agg(g, vals_lo, vals_up):
     return m
 
 
+def _tc(a, on):
+    """An operand of the node products W h and D W, which run on the tensor cores: rounded to
+    BF16 (through FP32, as the GPU holds it) when the rounded model is evaluated."""
+    return bf16_round(a) if on else a
+
+
 def forward(theta, g, round_bf16=True):
+    """round_bf16: the parameters, and the node activations entering the products W h, rounded
+    to BF16 as on the GPU; False: the exact FP64 model (for finite differences)."""
     p = unpack(bf16_round(theta) if round_bf16 else np.asarray(theta, np.float64))
-    cache = {"p": p}
+    cache = {"p": p, "rb": round_bf16}
     pre0 = g["x"] @ p["W0"].T + p["b0"]
     h = np.maximum(pre0, 0.0)
     cache["pre0"], hs, ss = pre0, [h], []
     for l in range(LAYERS):
-        s = h @ p[f"Wa{l}"].T + p[f"ba{l}"] + _agg(g, h @ p[f"Wl{l}"].T, h @ p[f"Wu{l}"].T)
+        hb = _tc(h, round_bf16)
+        s = hb @ p[f"Wa{l}"].T + p[f"ba{l}"] + _agg(g, hb @ p[f"Wl{l}"].T, hb @ p[f"Wu{l}"].T)
         h = h + np.maximum(s, 0.0)
         ss.append(s)
         hs.append(h)
     cache["hs"], cache["ss"] = hs, ss
-    ph = h @ p["P"].T + p["bp"]
-    qh = h @ p["Q"].T
+    hb = _tc(h, round_bf16)
+    ph = hb @ p["P"].T + p["bp"]
+    qh = hb @ p["Q"].T
     zpre = ph[g["lr"]] + qh[g["lc"]] + np.outer(g["le"], p["c"]) + np.outer(g["lf"], p["c2"])
     z = np.maximum(zpre, 0.0)
     go = z @ p["w"] + p["bw"][0]
@@ -303,7 +315,8 @@ def _backward(g, cache, dgo, dexp):
     grads["Q"] = dqh.T @ h
     grads["wd"] = h.T @ dexp
     grads["bwd"] = np.array([dexp.sum()])
-    dh = dph @ p["P"] + dqh @ p["Q"] + np.outer(dexp, p["wd"])
+    rb = cache["rb"]
+    dh = _tc(dph, rb) @ p["P"] + _tc(dqh, rb) @ p["Q"] + np.outer(dexp, p["wd"])
     # layers, last to first
     for l in reversed(range(LAYERS)):
         hin = cache["hs"][l]
@@ -321,7 +334,7 @@ def _backward(g, cache, dgo, dexp):
         grads[f"ba{l}"] = ds.sum(0)
         grads[f"Wl{l}"] = dhl.T @ hin
         grads[f"Wu{l}"] = dhu.T @ hin
-        dh = dh + ds @ p[f"Wa{l}"] + dhl @ p[f"Wl{l}"] + dhu @ p[f"Wu{l}"]
+        dh = dh + _tc(ds, rb) @ p[f"Wa{l}"] + _tc(dhl, rb) @ p[f"Wl{l}"] + _tc(dhu, rb) @ p[f"Wu{l}"]
     dpre0 = dh * (cache["pre0"] > 0)
     grads["W0"] = dpre0.T @ g["x"]
     grads["b0"] = dpre0.sum(0)

@@ -89,6 +89,8 @@ _SIGS = {
     "xplus_gen_fem2d": (_i, [_i, _d, _d, _u64, _i64, _i, _u64, _ip, _ip, _p, _p, _p, _p, _p]),
     "xplus_gen_fem3d": (_i, [_i, _d, _d, _u64, _i64, _i, _u64, _ip, _ip, _p, _p, _p, _p, _p]),
     "xplus_rcm": (_i, [_i, _p, _p, _p]),
+    "xplus_rcm_device": (_i, [_i, _p, _p, _p, _ip, _p]),
+    "xplus_permute_symmetric_device": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p]),
     "xplus_permute_symmetric": (_i, [_i, _p, _p, _p, _p, _p, _p, _p]),
     "xplus_sell_build": (_i, [_i, _p, _p, _p, _i, _i, _i, _i, _ip, C.POINTER(_i64), _p, _p, _p, _p, _p, _p]),
     "xplus_sell_build_device": (_i, [_i, _p, _p, _p, _i, _i, _i, _i, _ip, C.POINTER(_i64), _p, _p, _p, _p, _p, _p, _p]),

@@ -11,6 +11,8 @@
 //     lower neighbours (the coupling inside row i's pattern that the exact FSAI row solves)
 //   diagonal:            Ghat_ii = exp(wd . h_i + bwd)
 //   G = Ghat D^-1/2 (an untrained network with a zero output layer gives Jacobi)
+// The node products W h (and D W in the backward pass) run on the tensor cores with the node
+// activations rounded to BF16 (BF16 weights, FP32 accumulation); the rest is FP32.
 // Losses: over K probes v ~ N(0, I), L = sum ||G A G^T v - v||^2 / (K n); or the row-normalized
 // Kaporin loss L = (1/n) sum_i [log (G A G^T)_ii - 2 log Ghat_ii].
 // Lower and upper neighbours have their own message weights because G is lower-triangular in
@@ -60,8 +62,57 @@ __global__ void k_input(const float* __restrict__ x, const float* __restrict__ W
     h0[t] = fmaxf(v, 0.0f);
 }
 
-// Up to three products Y_m = W_m h (+ b_m) per node; W_m [H][H] row-major (out, in), staged
-// transposed in shared memory so lane `out` reads a conflict-free column.
+// ---- node products on the tensor cores ----
+// A warp takes 16 nodes at a time: mma.sync m16n8k16 (BF16 operands, FP32 accumulation), the
+// 16 x 32 node block as A (two k-steps of 16 features), a weight matrix as B, four n-tiles of
+// 8 outputs.  Node activations are rounded to BF16 as they enter the product (the weights are
+// BF16 already); sums, biases and everything outside these products stay FP32.
+// Fragment layout of m16n8k16 (g = lane / 4, t = lane % 4):
+//   A regs {A[g][2t..+1], A[g+8][2t..+1], A[g][2t+8..+9], A[g+8][2t+8..+9]}
+//   B regs {B[2t..+1][g], B[2t+8..+9][g]},  C {C[g][2t..+1], C[g+8][2t..+1]}
+constexpr int HP = H + 8;  // row stride (BF16) of the staged weights: conflict-free B loads
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float2 ld_row2(const float* src, int r, int n, int c) {
+    return r < n ? *reinterpret_cast<const float2*>(src + static_cast<size_t>(r) * H + c) : make_float2(0.0f, 0.0f);
+}
+
+// A fragments of rows [r0, r0 + 16), features [16 s, 16 s + 16) of src ([n][H] FP32)
+__device__ __forceinline__ void load_a(const float* __restrict__ src, int r0, int n, int s, int g, int t,
+                                       uint32_t (&a)[4]) {
+    const int c = 16 * s + 2 * t;
+    const float2 x0 = ld_row2(src, r0 + g, n, c), x1 = ld_row2(src, r0 + g + 8, n, c);
+    const float2 x2 = ld_row2(src, r0 + g, n, c + 8), x3 = ld_row2(src, r0 + g + 8, n, c + 8);
+    a[0] = pack_bf16(x0.x, x0.y);
+    a[1] = pack_bf16(x1.x, x1.y);
+    a[2] = pack_bf16(x2.x, x2.y);
+    a[3] = pack_bf16(x3.x, x3.y);
+}
+
+// acc[j] += A (16 x 16, k-step s) times B = staged[n][k] for the n-tile j (n = 8 j + g)
+__device__ __forceinline__ void mma_row(float (&acc)[4][4], const uint32_t (&a)[4], const __nv_bfloat16* ws, int s,
+                                        int g, int t) {
+    const uint32_t* w32 = reinterpret_cast<const uint32_t*>(ws);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int base = ((8 * j + g) * HP + 16 * s + 2 * t) >> 1;
+        mma_bf16(acc[j], a, w32[base], w32[base + 4]);
+    }
+}
+
+// Up to three products Y_m = W_m h (+ b_m) per node; W_m [H][H] row-major (out, in) is B with
+// B[k][n] = W_m[n][k], staged as Ws[n][k] (BF16).
 struct Lin3 {
     const float* W[3];
     const float* b[3];
@@ -70,32 +121,42 @@ struct Lin3 {
 };
 
 __global__ void __launch_bounds__(256) k_node_lin(const float* __restrict__ h, Lin3 L, int n) {
-    __shared__ float WT[3][H * H];
-    for (int q = threadIdx.x; q < L.count * H * H; q += blockDim.x) {
-        const int m = q / (H * H), r = q % (H * H), o = r / H, k = r % H;
-        WT[m][k * H + o] = L.W[m][r];
-    }
+    __shared__ __align__(16) __nv_bfloat16 Ws[3][H * HP];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)  // compile-time m: the parameter struct stays out of local memory
+        if (m < L.count)
+            for (int r = threadIdx.x; r < H * H; r += blockDim.x) Ws[m][(r / H) * HP + r % H] = __float2bfloat16_rn(L.W[m][r]);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int warps = blockDim.x >> 5;
-    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
-        const float hv = h[static_cast<size_t>(i) * H + lane];
-        float acc[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll 8
-        for (int k = 0; k < H; ++k) {
-            const float hk = __shfl_sync(0xffffffffu, hv, k);
+    for (int r0 = (blockIdx.x * warps + (threadIdx.x >> 5)) * 16; r0 < n; r0 += gridDim.x * warps * 16) {
+        uint32_t a[2][4];
+        load_a(h, r0, n, 0, g, t, a[0]);
+        load_a(h, r0, n, 1, g, t, a[1]);
 #pragma unroll
-            for (int m = 0; m < 3; ++m)
-                if (m < L.count) acc[m] = fmaf(hk, WT[m][k * H + lane], acc[m]);
+        for (int m = 0; m < 3; ++m) {
+            if (m >= L.count) continue;
+            float acc[4][4] = {};
+            mma_row(acc, a[0], Ws[m], 0, g, t);
+            mma_row(acc, a[1], Ws[m], 1, g, t);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = 8 * j + 2 * t;
+                const float b0 = L.b[m] ? L.b[m][c] : 0.0f, b1 = L.b[m] ? L.b[m][c + 1] : 0.0f;
+                if (r0 + g < n)
+                    *reinterpret_cast<float2*>(L.Y[m] + static_cast<size_t>(r0 + g) * H + c) =
+                        make_float2(acc[j][0] + b0, acc[j][1] + b1);
+                if (r0 + g + 8 < n)
+                    *reinterpret_cast<float2*>(L.Y[m] + static_cast<size_t>(r0 + g + 8) * H + c) =
+                        make_float2(acc[j][2] + b0, acc[j][3] + b1);
+            }
         }
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-            if (m < L.count) L.Y[m][static_cast<size_t>(i) * H + lane] = acc[m] + (L.b[m] ? L.b[m][lane] : 0.0f);
     }
 }
 
-// Transposed products for the backward pass: dX = sum_m D_m W_m (+ dexp (x) wd), W_m [H][H]
-// row-major staged as is (lane `in` reads W[out][in], conflict-free).  dX = accumulate ? dX + . : .
+// Transposed products for the backward pass: dX = sum_m D_m W_m (+ dexp (x) wd), i.e. B with
+// B[k][n] = W_m[k][n] (k = output feature, n = input feature), staged as Ws[n][k] (BF16).
+// dX = accumulate ? dX + . : .
 struct BackLin {
     const float* W[3];
     const float* D[3];
@@ -106,22 +167,46 @@ struct BackLin {
 };
 
 __global__ void __launch_bounds__(256) k_node_backlin(BackLin B, float* __restrict__ dX, int n) {
-    __shared__ float Ws[3][H * H];
-    for (int q = threadIdx.x; q < B.count * H * H; q += blockDim.x) Ws[q / (H * H)][q % (H * H)] = B.W[q / (H * H)][q % (H * H)];
+    __shared__ __align__(16) __nv_bfloat16 Ws[3][H * HP];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+        if (m < B.count)
+            for (int r = threadIdx.x; r < H * H; r += blockDim.x) Ws[m][(r % H) * HP + r / H] = __float2bfloat16_rn(B.W[m][r]);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int warps = blockDim.x >> 5;
-    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
-        float acc = B.accumulate ? dX[static_cast<size_t>(i) * H + lane] : 0.0f;
+    for (int r0 = (blockIdx.x * warps + (threadIdx.x >> 5)) * 16; r0 < n; r0 += gridDim.x * warps * 16) {
+        float acc[4][4] = {};
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            if (m >= B.count) break;
-            const float dv = B.D[m][static_cast<size_t>(i) * H + lane];
-#pragma unroll 8
-            for (int o = 0; o < H; ++o) acc = fmaf(__shfl_sync(0xffffffffu, dv, o), Ws[m][o * H + lane], acc);
+            if (m >= B.count) continue;
+            uint32_t a[4];
+            load_a(B.D[m], r0, n, 0, g, t, a);
+            mma_row(acc, a, Ws[m], 0, g, t);
+            load_a(B.D[m], r0, n, 1, g, t, a);
+            mma_row(acc, a, Ws[m], 1, g, t);
         }
-        if (B.dexp) acc = fmaf(B.dexp[i], B.wd[lane], acc);
-        dX[static_cast<size_t>(i) * H + lane] = acc;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = 8 * j + 2 * t;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int r = r0 + g + 8 * half;
+                if (r >= n) continue;
+                float2 v = make_float2(acc[j][2 * half], acc[j][2 * half + 1]);
+                float2* out = reinterpret_cast<float2*>(dX + static_cast<size_t>(r) * H + c);
+                if (B.accumulate) {
+                    const float2 o = *out;
+                    v.x += o.x;
+                    v.y += o.y;
+                }
+                if (B.dexp) {
+                    v.x = fmaf(B.dexp[r], B.wd[c], v.x);
+                    v.y = fmaf(B.dexp[r], B.wd[c + 1], v.y);
+                }
+                *out = v;
+            }
+        }
     }
 }
 
@@ -900,7 +985,7 @@ void forward(const DevGraph& g, const float* wr, Work& w, bool train, cudaStream
     const ParamOffsets off = param_offsets();
     const int n = g.n;
     const int nodes_blocks = blocks_for(static_cast<long long>(n) * 32, 256);
-    const int lin_blocks = std::min(blocks_for(n, 8), 148 * 8);
+    const int lin_blocks = std::min(blocks_for(n, 8 * 16), 148 * 8);  // 8 warps of 16-node tiles
     k_input<<<blocks_for(static_cast<long long>(n) * H, 256), 256, 0, st>>>(g.x, wr + off.W0, wr + off.b0, w.h[0], n);
     kcheck("gnn input");
     for (int l = 0; l < kLayers; ++l) {
@@ -1012,7 +1097,7 @@ void backward_from_dg(const DevGraph& g, const float* wr, Work& w, float* grad, 
     const ParamOffsets off = param_offsets();
     const int n = g.n;
     const int nodes_blocks = blocks_for(static_cast<long long>(n) * 32, 256);
-    const int lin_blocks = std::min(blocks_for(n, 8), 148 * 8);
+    const int lin_blocks = std::min(blocks_for(n, 8 * 16), 148 * 8);  // 8 warps of 16-node tiles
     k_head_back<<<nodes_blocks, 256, 0, st>>>(g.low_ptr, g.up_ptr, g.up_k, w.zpre, w.dgo, wr, off, w.dph, w.dqh, n);
     kcheck("gnn head back");
     // edge-head parameters w, c, bw

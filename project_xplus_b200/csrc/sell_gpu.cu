@@ -14,7 +14,13 @@
 #include <algorithm>
 #include <vector>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cfloat>
+
 #include "common.hpp"
+#include "layout_gpu.hpp"
 
 namespace xplus {
 namespace {
@@ -296,6 +302,240 @@ void sell_build_via_gpu(int n, const int* row_ptr, const int* col_idx, const dou
         throw;
     }
     cudaStreamDestroy(st);
+}
+
+// ---------------------------------------------------------------------------------------
+// The rest of the device-side create (layout_gpu.hpp)
+// ---------------------------------------------------------------------------------------
+namespace {
+
+// first diagonal entry of each row; bad[0] = rows without one, bad[1] = rows whose entry is
+// zero (|a_ii| <= DBL_MIN, the host test)
+__global__ void k_diag_first(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                             int n, double* __restrict__ diag, int* __restrict__ bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    bool found = false;
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+        if (ci[k] == i) {
+            d = v[k];
+            found = true;
+            break;
+        }
+    diag[i] = d;
+    if (!found) atomicAdd(bad, 1);
+    else if (fabs(d) <= DBL_MIN) atomicAdd(bad + 1, 1);
+}
+
+// slot positions of SELL row r: pos(j) = ptr[s] + (j / chunk) 32 chunk + l chunk + j % chunk
+__device__ __forceinline__ long long slot_of(const long long* ptr, int r, int j, int chunk) {
+    return ptr[r >> 5] + static_cast<long long>(j / chunk) * 32 * chunk + (r & 31) * chunk + (j % chunk);
+}
+
+__global__ void k_pack16(const long long* __restrict__ ptr, const int* __restrict__ width, int n_pad, int chunk,
+                         const int* __restrict__ col, short* __restrict__ col16, int* __restrict__ far) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_pad) return;
+    const int w = width[r >> 5];
+    for (int j = 0; j < w; ++j) {
+        const long long pos = slot_of(ptr, r, j, chunk);
+        const int d = col[pos] - r;
+        if (d < -32768 || d > 32767) atomicOr(far, 1);
+        col16[pos] = static_cast<short>(d);
+    }
+}
+
+__global__ void k_convert(const double* __restrict__ in, long long count, int type, double scale, void* __restrict__ out) {
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const double x = in[q];
+    if (type == XPLUS_F32) static_cast<float*>(out)[q] = __double2float_rn(x);
+    else if (type == XPLUS_F16) static_cast<__half*>(out)[q] = __double2half(x / scale);
+    else if (type == XPLUS_BF16) static_cast<__nv_bfloat16*>(out)[q] = __double2bfloat16(x);
+    else static_cast<double*>(out)[q] = x;
+}
+
+__device__ __forceinline__ void store_vec(void* out, int i, int type, double x) {
+    if (type == XPLUS_F64) static_cast<double*>(out)[i] = x;
+    else static_cast<float*>(out)[i] = __double2float_rn(x);
+}
+
+__global__ void k_row_vectors(const int* __restrict__ rp, const double* __restrict__ v, const int* __restrict__ perm,
+                              const double* __restrict__ diag_csr, int n, int n_pad, int vtype,
+                              double* __restrict__ diag64, void* __restrict__ minv, void* __restrict__ rowsum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    double d = 0.0, m = 0.0, rs = 0.0;
+    if (i < n) {
+        const int old = perm[i];
+        d = diag_csr[old];
+        m = 1.0 / d;
+        if (rowsum)
+            for (int k = rp[old]; k < rp[old + 1]; ++k) rs += v[k];
+    }
+    if (diag64) diag64[i] = d;
+    store_vec(minv, i, vtype, m);
+    if (rowsum) store_vec(rowsum, i, vtype, rs);
+}
+
+__global__ void k_count_below(const double* __restrict__ v, int n, double eps, int* __restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && fabs(v[i]) <= eps) atomicAdd(count, 1);
+}
+
+// one CTA per resident block: min / max column of its slots
+__global__ void k_windows(const long long* __restrict__ ptr, const int* __restrict__ col, int n_slices, int n_pad,
+                          int per, int2* __restrict__ win) {
+    __shared__ int s_lo[32], s_hi[32];
+    const int b = blockIdx.x;
+    const int sb = b * per, se = min(n_slices, sb + per);
+    if (se <= sb) {
+        if (threadIdx.x == 0) win[b] = make_int2(0, 0);
+        return;
+    }
+    int lo = sb * 32, hi = se * 32;
+    for (long long pos = ptr[sb] + threadIdx.x; pos < ptr[se]; pos += blockDim.x) {
+        const int c = col[pos];
+        lo = min(lo, c);
+        hi = max(hi, c + 1);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_lo[threadIdx.x >> 5] = lo;
+        s_hi[threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            lo = min(lo, s_lo[w]);
+            hi = max(hi, s_hi[w]);
+        }
+        lo &= ~3;  // 16-byte aligned window
+        hi = min(n_pad, (hi + 3) & ~3);
+        win[b] = make_int2(lo, hi - lo);
+    }
+}
+
+}  // namespace
+
+DeviceCsr::~DeviceCsr() {
+    for (void* p : owned) cudaFree(p);
+}
+
+void upload_csr(int n, const int* row_ptr, const int* col_idx, const double* values, DeviceCsr& csr, cudaStream_t st) {
+    csr.n = n;
+    csr.nnz = row_ptr[n];
+    require(csr.nnz >= 0, XPLUS_ERR_DATA, "row_ptr[n] must equal nnz");
+    auto get = [&](size_t bytes) {
+        void* p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        csr.owned.push_back(p);
+        return p;
+    };
+    csr.rp = static_cast<int*>(get((static_cast<size_t>(n) + 1) * sizeof(int)));
+    csr.ci = static_cast<int*>(get(static_cast<size_t>(csr.nnz) * sizeof(int)));
+    csr.v = static_cast<double*>(get(static_cast<size_t>(csr.nnz) * sizeof(double)));
+    ck(cudaMemcpyAsync(csr.rp, row_ptr, (static_cast<size_t>(n) + 1) * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    ck(cudaMemcpyAsync(csr.ci, col_idx, static_cast<size_t>(csr.nnz) * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    ck(cudaMemcpyAsync(csr.v, values, static_cast<size_t>(csr.nnz) * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+    // structure checks on the device; the host validator supplies the message of a failure
+    DevTmp tmp;
+    int* bad = tmp.get<int>(1);
+    int h_bad = 0;
+    const int tb = 256;
+    ck(cudaMemsetAsync(bad, 0, sizeof(int), st), "memset");
+    k_check_rows<<<(n + tb - 1) / tb, tb, 0, st>>>(csr.rp, n, bad);
+    ck(cudaGetLastError(), "csr check");
+    ck(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "sync");
+    if (h_bad == 0 && csr.nnz > 0) {
+        k_check_cols<<<static_cast<unsigned>((csr.nnz + tb - 1) / tb), tb, 0, st>>>(csr.ci, csr.nnz, n, bad);
+        ck(cudaGetLastError(), "csr check");
+        ck(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaStreamSynchronize(st), "sync");
+    }
+    if (h_bad != 0) {
+        validate_csr(n, row_ptr, col_idx, csr.nnz);
+        throw Error(XPLUS_ERR_DATA, "invalid CSR structure");
+    }
+}
+
+void jacobi_diag_device(const DeviceCsr& csr, const int* row_ptr, const int* col_idx, const double* values,
+                        double* d_diag, cudaStream_t st) {
+    DevTmp tmp;
+    int* bad = tmp.get<int>(2);
+    int h_bad[2] = {0, 0};
+    ck(cudaMemsetAsync(bad, 0, 2 * sizeof(int), st), "memset");
+    k_diag_first<<<(csr.n + 255) / 256, 256, 0, st>>>(csr.rp, csr.ci, csr.v, csr.n, d_diag, bad);
+    ck(cudaGetLastError(), "jacobi diag");
+    ck(cudaMemcpyAsync(h_bad, bad, sizeof(h_bad), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "sync");
+    if (h_bad[0] || h_bad[1]) {
+        std::vector<double> d(static_cast<size_t>(csr.n));
+        jacobi_diag(csr.n, row_ptr, col_idx, values, d.data());  // throws the reference's message
+        throw Error(XPLUS_ERR_DATA, "missing or zero diagonal entry");
+    }
+}
+
+void sell_layout_device(const DeviceCsr& csr, int sigma, int chunk, int diag_split, int* n_slices, int64_t* slots,
+                        int* d_perm, long long* d_slice_ptr, int* d_width, int* d_col32, double* d_val64,
+                        double* d_diag_sell, cudaStream_t st) {
+    sell_build_device(csr.n, csr.rp, csr.ci, csr.v, 32, sigma, chunk, diag_split, n_slices, slots, d_perm,
+                      reinterpret_cast<int64_t*>(d_slice_ptr), d_width, d_col32, d_val64, d_diag_sell, st);
+}
+
+bool pack_index16_device(const long long* d_slice_ptr, const int* d_width, int n_slices, int chunk,
+                         const int* d_col32, short* d_col16, cudaStream_t st) {
+    DevTmp tmp;
+    int* far = tmp.get<int>(1);
+    int h_far = 0;
+    const int n_pad = n_slices * 32;
+    ck(cudaMemsetAsync(far, 0, sizeof(int), st), "memset");
+    k_pack16<<<(n_pad + 255) / 256, 256, 0, st>>>(d_slice_ptr, d_width, n_pad, chunk, d_col32, d_col16, far);
+    ck(cudaGetLastError(), "pack int16");
+    ck(cudaMemcpyAsync(&h_far, far, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "sync");
+    return h_far == 0;
+}
+
+void count_below(const double* d_v, int n, double eps, int* d_count, cudaStream_t st) {
+    k_count_below<<<(n + 255) / 256, 256, 0, st>>>(d_v, n, eps, d_count);
+    ck(cudaGetLastError(), "count below");
+}
+
+void convert_device(const double* d_in, int64_t count, int type, double scale, void* d_out, cudaStream_t st) {
+    if (count <= 0) return;
+    k_convert<<<static_cast<unsigned>((count + 255) / 256), 256, 0, st>>>(d_in, count, type, scale, d_out);
+    ck(cudaGetLastError(), "convert values");
+}
+
+void row_vectors_device(const DeviceCsr& csr, const int* d_perm, const double* d_diag_csr, int n_pad, int vtype,
+                        double* d_diag64, void* d_minv, void* d_rowsum, cudaStream_t st) {
+    k_row_vectors<<<(n_pad + 255) / 256, 256, 0, st>>>(csr.rp, csr.v, d_perm, d_diag_csr, csr.n, n_pad, vtype, d_diag64,
+                                                        d_minv, d_rowsum);
+    ck(cudaGetLastError(), "row vectors");
+}
+
+std::vector<int2> resident_windows_device(const long long* d_slice_ptr, const int* d_col32, int n_slices, int n_pad,
+                                          int grid, cudaStream_t st) {
+    DevTmp tmp;
+    int2* win = tmp.get<int2>(static_cast<size_t>(grid));
+    const int per = (n_slices + grid - 1) / grid;
+    k_windows<<<grid, 256, 0, st>>>(d_slice_ptr, d_col32, n_slices, n_pad, per, win);
+    ck(cudaGetLastError(), "resident windows");
+    std::vector<int2> out(static_cast<size_t>(grid));
+    ck(cudaMemcpyAsync(out.data(), win, out.size() * sizeof(int2), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "sync");
+    return out;
 }
 
 }  // namespace xplus

@@ -20,6 +20,7 @@
 
 #include "common.hpp"
 #include "gnn.hpp"
+#include "layout_gpu.hpp"
 #include "pcg_kernels.cuh"
 
 struct xplus_pcg {
@@ -257,6 +258,252 @@ void destroy(xplus_pcg* h) {
     delete h;
 }
 
+// Columns and values in one allocation, so one L2 access-policy window covers both.
+unsigned char* alloc_matrix(xplus_pcg* h, const xplus_opts& o, size_t col_bytes, size_t val_bytes) {
+    unsigned char* mat = dalloc<unsigned char>(h, col_bytes + val_bytes);
+    h->d_col = mat;
+    h->d_val = mat + col_bytes;
+    if (o.l2_persist) {
+        int max_window = 0;
+        cudaDeviceProp prop;
+        cuda_check(cudaGetDeviceProperties(&prop, o.device), "props");
+        cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, o.device), "attr");
+        const size_t bytes = std::min(col_bytes + val_bytes, static_cast<size_t>(max_window));
+        size_t limit = 0;
+        const size_t want = std::min(bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
+        {
+            std::lock_guard<std::mutex> lk(g_l2_mutex);
+            cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+            if (g_l2_wants.empty()) g_l2_limit_before = limit;
+            if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
+            g_l2_wants.insert(want);
+            h->l2_want = want;
+            h->l2_user = true;
+        }
+        cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+        if (bytes > 0 && limit > 0) {
+            h->window.base_ptr = mat;
+            h->window.num_bytes = bytes;
+            h->window.hitRatio = std::min(1.0f, static_cast<float>(limit) / static_cast<float>(bytes));
+            h->window.hitProp = cudaAccessPropertyPersisting;
+            h->window.missProp = cudaAccessPropertyStreaming;
+        }
+    }
+    return mat;
+}
+
+// Device temporaries of one create call, freed when it returns.
+struct CreateTmp {
+    std::vector<void*> p;
+    template <typename T>
+    T* get(size_t count) {
+        void* q = nullptr;
+        const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 256));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(XPLUS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        p.push_back(q);
+        return static_cast<T*>(q);
+    }
+    ~CreateTmp() {
+        for (void* q : p) cudaFree(q);
+    }
+};
+
+// The layout on the GPU from one device copy of the CSR: checks, Jacobi diagonal, SELL image,
+// int16 offsets, value conversion, FP64 copy, row vectors and the resident windows, every
+// array bit-identical to the host path (create_layout_host).  `grid` > 0: windows for that
+// many resident blocks.
+void create_layout_device(xplus_pcg* h, const xplus_opts& o, bool split, int n, const int* row_ptr,
+                          const int* col_idx, const double* values, int grid, std::vector<int2>& win) {
+    cudaStream_t st = h->stream;
+    CreateTmp tmp;
+    DeviceCsr csr;
+    upload_csr(n, row_ptr, col_idx, values, csr, st);
+    double* d_diag_csr = tmp.get<double>(static_cast<size_t>(n));
+    jacobi_diag_device(csr, row_ptr, col_idx, values, d_diag_csr, st);
+    {
+        // the host path's second test (kBreakdownEps), with its message
+        int tiny = 0;
+        const double eps = 1.0e-30;
+        int* d_tiny = tmp.get<int>(1);
+        cuda_check(cudaMemsetAsync(d_tiny, 0, sizeof(int), st), "memset");
+        count_below(d_diag_csr, n, eps, d_tiny, st);
+        cuda_check(cudaMemcpyAsync(&tiny, d_tiny, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        require(tiny == 0, XPLUS_ERR_DATA, "zero diagonal entry while building Jacobi inverse");
+    }
+    int ns = 0;
+    int64_t slots = 0;
+    sell_layout_device(csr, o.sigma, o.chunk, split ? 1 : 0, &ns, &slots, nullptr, nullptr, nullptr, nullptr, nullptr,
+                       nullptr, st);
+    h->n_slices = ns;
+    h->n_pad = ns * 32;
+    h->slots = slots;
+    const size_t np = static_cast<size_t>(h->n_pad);
+    const size_t xs = elem_size(o.vector_type);
+    h->d_perm = dalloc<int>(h, static_cast<size_t>(n));
+    h->d_slice_ptr = dalloc<long long>(h, static_cast<size_t>(ns) + 1);
+    int* width = tmp.get<int>(static_cast<size_t>(ns));
+    int* col32 = tmp.get<int>(static_cast<size_t>(slots));
+    const bool keep64 = o.keep_fp64 != 0 && o.value_type != XPLUS_F64;
+    double* val64 = keep64 ? dalloc<double>(h, static_cast<size_t>(slots)) : tmp.get<double>(static_cast<size_t>(slots));
+    sell_layout_device(csr, o.sigma, o.chunk, split ? 1 : 0, &ns, &slots, h->d_perm, h->d_slice_ptr, width, col32,
+                       val64, nullptr, st);
+    // int16 offsets from the row when the ordered bandwidth allows (lossless)
+    bool idx16 = o.index16 != 0;
+    short* col16 = nullptr;
+    if (idx16) {
+        col16 = tmp.get<short>(static_cast<size_t>(slots));
+        idx16 = pack_index16_device(h->d_slice_ptr, width, ns, o.chunk, col32, col16, st);
+    }
+    h->key.idx16 = idx16 ? 1 : 0;
+    const size_t col_bytes = (static_cast<size_t>(slots) * (idx16 ? 2 : 4) + 255) / 256 * 256;
+    const size_t val_bytes = static_cast<size_t>(slots) * elem_size(o.value_type);
+    alloc_matrix(h, o, col_bytes, val_bytes);
+    cuda_check(cudaMemcpyAsync(h->d_col, idx16 ? static_cast<const void*>(col16) : static_cast<const void*>(col32),
+                               static_cast<size_t>(slots) * (idx16 ? 2 : 4), cudaMemcpyDeviceToDevice, st), "D2D");
+    h->val_scale = o.value_type == XPLUS_F16 ? f16_offdiag_scale(n, row_ptr, col_idx, values) : 1.0;
+    convert_device(val64, slots, o.value_type, h->val_scale, h->d_val, st);
+    if (keep64) h->d_val64 = val64;
+    else if (o.value_type == XPLUS_F64) h->d_val64 = static_cast<double*>(h->d_val);
+    // Jacobi inverse in SELL order (host/pcg_common.hpp:42-54: m_inv = 1 / diag), from the exact
+    // FP64 diagonal; in the row-sum form also the row sums and the FP64 diagonal
+    h->d_minv = dalloc<unsigned char>(h, np * xs);
+    if (split) {
+        h->d_rowsum = dalloc<unsigned char>(h, np * xs);
+        h->d_diag64 = dalloc<double>(h, np);
+    }
+    row_vectors_device(csr, h->d_perm, d_diag_csr, h->n_pad, o.vector_type, split ? h->d_diag64 : nullptr, h->d_minv,
+                       split ? h->d_rowsum : nullptr, st);
+    h->perm.resize(static_cast<size_t>(n));
+    cuda_check(cudaMemcpyAsync(h->perm.data(), h->d_perm, static_cast<size_t>(n) * sizeof(int), cudaMemcpyDeviceToHost, st),
+               "D2H");
+    if (grid > 0) win = resident_windows_device(h->d_slice_ptr, col32, ns, h->n_pad, grid, st);
+    cuda_check(cudaStreamSynchronize(st), "sync");  // the temporaries go next
+}
+
+// The layout on the host (the reference for create_layout_device): the 16-bit two-term
+// rewrite, sort windows above 4096, or build_on_gpu = 0.  diag: the CSR's Jacobi diagonal.
+void create_layout_host(xplus_pcg* h, const xplus_opts& o, bool split, int n, const int* row_ptr,
+                        const int* col_idx, const double* values, const std::vector<double>& diag, int grid,
+                        std::vector<int2>& win) {
+    const double scale16 = o.value_type == XPLUS_F16 ? f16_offdiag_scale(n, row_ptr, col_idx, values) : 1.0;
+    const double split_ratio = split_ratio_of(o);
+    TwoTermCsr two;
+    if (split_ratio > 0.0) two_term_entries(n, row_ptr, col_idx, values, o.value_type, scale16, split_ratio, two);
+    const bool use_two = !two.row_ptr.empty();
+    const int* rp_s = use_two ? two.row_ptr.data() : row_ptr;
+    const int* ci_s = use_two ? two.col_idx.data() : col_idx;
+    const double* va_s = use_two ? two.values.data() : values;
+    SellHost S;
+    if (o.build_on_gpu && o.sigma <= 4096)
+        sell_build_via_gpu(n, rp_s, ci_s, va_s, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+    else
+        sell_build(n, rp_s, ci_s, va_s, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+    h->n_pad = S.n_pad;
+    h->n_slices = S.n_slices;
+    h->slots = S.slots;
+    h->perm = S.perm;
+    cudaStream_t st = h->stream;
+    const size_t np = static_cast<size_t>(S.n_pad);
+    const size_t xs = elem_size(o.vector_type);
+    h->d_slice_ptr = dalloc<long long>(h, S.slice_ptr.size());
+    // int16 offsets from the row when the ordered bandwidth allows (lossless)
+    bool idx16 = o.index16 != 0;
+    std::vector<short> col16;
+    if (idx16) {
+        col16.resize(static_cast<size_t>(S.slots));
+        // slot (j/chunk) 32 chunk + lane chunk + j%chunk of slice sl belongs to row 32 sl + lane
+        std::vector<unsigned char> far(static_cast<size_t>(S.n_slices), 0);
+        const int ch = o.chunk;
+        parallel_for(S.n_slices, [&](int64_t b, int64_t e) {
+            for (int64_t sl = b; sl < e; ++sl) {
+                const int64_t base = S.slice_ptr[static_cast<size_t>(sl)];
+                const int64_t groups = (S.slice_ptr[static_cast<size_t>(sl) + 1] - base) / (32 * ch);
+                for (int64_t jg = 0; jg < groups; ++jg)
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int row = static_cast<int>(sl) * 32 + lane;
+                        const int64_t p0 = base + jg * 32 * ch + lane * ch;
+                        for (int q = 0; q < ch; ++q) {
+                            const int d = S.col[static_cast<size_t>(p0 + q)] - row;
+                            if (d < -32768 || d > 32767) far[static_cast<size_t>(sl)] = 1;
+                            col16[static_cast<size_t>(p0 + q)] = static_cast<short>(d);
+                        }
+                    }
+            }
+        });
+        for (unsigned char f : far)
+            if (f) idx16 = false;
+    }
+    h->key.idx16 = idx16 ? 1 : 0;
+    const size_t col_bytes = (static_cast<size_t>(S.slots) * (idx16 ? 2 : 4) + 255) / 256 * 256;
+    const size_t val_bytes = static_cast<size_t>(S.slots) * elem_size(o.value_type);
+    alloc_matrix(h, o, col_bytes, val_bytes);
+    h->d_perm = dalloc<int>(h, static_cast<size_t>(n));
+    h->d_minv = dalloc<unsigned char>(h, np * xs);
+    std::vector<long long> sp(S.slice_ptr.begin(), S.slice_ptr.end());
+    cuda_check(cudaMemcpyAsync(h->d_slice_ptr, sp.data(), sp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
+    if (h->key.idx16)
+        cuda_check(cudaMemcpyAsync(h->d_col, col16.data(), col16.size() * sizeof(short), cudaMemcpyHostToDevice, st), "H2D");
+    else
+        cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaMemcpyAsync(h->d_perm, S.perm.data(), S.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    h->val_scale = o.value_type == XPLUS_F16 ? scale16 : 1.0;
+    std::vector<unsigned char> vbytes = convert(S.val, o.value_type, h->val_scale);
+    cuda_check(cudaMemcpyAsync(h->d_val, vbytes.data(), vbytes.size(), cudaMemcpyHostToDevice, st), "H2D");
+    const bool keep64 = o.keep_fp64 != 0 && o.value_type != XPLUS_F64;
+    if (keep64) {
+        h->d_val64 = dalloc<double>(h, static_cast<size_t>(S.slots));
+        cuda_check(cudaMemcpyAsync(h->d_val64, S.val.data(), S.val.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+    } else if (o.value_type == XPLUS_F64) {
+        h->d_val64 = static_cast<double*>(h->d_val);
+    }
+    // Jacobi inverse in SELL order (host/pcg_common.hpp:42-54: m_inv = 1 / diag), from
+    // the exact FP64 diagonal.
+    std::vector<double> dsell(np, 0.0), minv(np, 0.0);
+    for (int i = 0; i < n; ++i) {
+        dsell[static_cast<size_t>(i)] = diag[static_cast<size_t>(S.perm[static_cast<size_t>(i)])];
+        minv[static_cast<size_t>(i)] = 1.0 / dsell[static_cast<size_t>(i)];
+    }
+    if (split) {
+        std::vector<double> rs(np, 0.0);
+        parallel_for(n, [&](int64_t b, int64_t e) {
+            for (int64_t i = b; i < e; ++i) {
+                const int old = S.perm[static_cast<size_t>(i)];
+                double acc = 0.0;
+                for (int k = row_ptr[old]; k < row_ptr[old + 1]; ++k) acc += values[k];
+                rs[static_cast<size_t>(i)] = acc;
+            }
+        });
+        std::vector<unsigned char> rb = convert(rs, o.vector_type);
+        h->d_rowsum = dalloc<unsigned char>(h, np * xs);
+        cuda_check(cudaMemcpyAsync(h->d_rowsum, rb.data(), rb.size(), cudaMemcpyHostToDevice, st), "H2D");
+        h->d_diag64 = dalloc<double>(h, np);
+        cuda_check(cudaMemcpyAsync(h->d_diag64, dsell.data(), np * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+    }
+    std::vector<unsigned char> mb = convert(minv, o.vector_type);
+    cuda_check(cudaMemcpyAsync(h->d_minv, mb.data(), mb.size(), cudaMemcpyHostToDevice, st), "H2D");
+    if (grid > 0) {
+        const int per_block = (S.n_slices + grid - 1) / grid;
+        win.assign(static_cast<size_t>(grid), make_int2(0, 0));
+        for (int b = 0; b < grid; ++b) {
+            const int sb = b * per_block, se = std::min(S.n_slices, sb + per_block);
+            if (se <= sb) continue;
+            int lo = sb * 32, hi = se * 32;
+            for (int64_t pos = S.slice_ptr[static_cast<size_t>(sb)]; pos < S.slice_ptr[static_cast<size_t>(se)]; ++pos) {
+                lo = std::min(lo, S.col[static_cast<size_t>(pos)]);
+                hi = std::max(hi, S.col[static_cast<size_t>(pos)] + 1);
+            }
+            lo &= ~3;  // 16-byte aligned window
+            hi = std::min(S.n_pad, (hi + 3) & ~3);
+            win[static_cast<size_t>(b)] = make_int2(lo, hi - lo);
+        }
+    }
+    cuda_check(cudaStreamSynchronize(st), "sync");  // the host images go next
+}
+
 void create(const int* row_ptr, const int* col_idx, const double* values, int n,
             const xplus_opts* opts_in, xplus_pcg** out) {
     require(row_ptr && col_idx && values && out, XPLUS_ERR_ARG, "null argument");
@@ -272,34 +519,27 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
     require(o.chunk == 1 || o.chunk == 2 || o.chunk == 4, XPLUS_ERR_ARG, "chunk must be 1, 2 or 4");
     require(o.sigma >= 1, XPLUS_ERR_ARG, "sigma must be >= 1");
     require(o.restart_on_replace >= -1 && o.restart_on_replace <= 4, XPLUS_ERR_ARG, "restart_on_replace must be -1..4");
-    validate_csr(n, row_ptr, col_idx, row_ptr[n]);
-    std::vector<double> diag(static_cast<size_t>(n));
-    jacobi_diag(n, row_ptr, col_idx, values, diag.data());
-    for (int i = 0; i < n; ++i)
-        require(std::fabs(diag[static_cast<size_t>(i)]) > 1.0e-30, XPLUS_ERR_DATA,
-                "zero diagonal entry while building Jacobi inverse");
-    require_device(o.device);
-    cuda_check(cudaSetDevice(o.device), "cudaSetDevice");
-
     // Row-sum form for FP32/BF16 values: slots hold the off-diagonal weights, the row sums
     // s_i = sum_j a_ij (FP64 sum) are kept apart in the vector type, and the FP64 diagonal
     // stays apart for the true residual.
     const bool split = (o.value_type != XPLUS_F64) && o.row_sum_form;
     require((o.value_type != XPLUS_BF16 && o.value_type != XPLUS_F16) || split, XPLUS_ERR_ARG,
             "16-bit values need row_sum_form");
-    const double scale16 = o.value_type == XPLUS_F16 ? f16_offdiag_scale(n, row_ptr, col_idx, values) : 1.0;
-    const double split_ratio = split_ratio_of(o);
-    TwoTermCsr two;
-    if (split_ratio > 0.0) two_term_entries(n, row_ptr, col_idx, values, o.value_type, scale16, split_ratio, two);
-    const bool use_two = !two.row_ptr.empty();
-    const int* rp_s = use_two ? two.row_ptr.data() : row_ptr;
-    const int* ci_s = use_two ? two.col_idx.data() : col_idx;
-    const double* va_s = use_two ? two.values.data() : values;
-    SellHost S;
-    if (o.build_on_gpu && o.sigma <= 4096)
-        sell_build_via_gpu(n, rp_s, ci_s, va_s, 32, o.sigma, o.chunk, split ? 1 : 0, S);
-    else
-        sell_build(n, rp_s, ci_s, va_s, 32, o.sigma, o.chunk, split ? 1 : 0, S);
+    // Everything is derived on the GPU from one device copy of the CSR, unless the 16-bit
+    // two-term rewrite (a host CSR transformation) or a sort window beyond the device
+    // builder's 4096 asks for the host layout.
+    const bool on_device = o.build_on_gpu && o.sigma <= 4096 && split_ratio_of(o) <= 0.0;
+    std::vector<double> diag;
+    if (!on_device) {
+        validate_csr(n, row_ptr, col_idx, row_ptr[n]);
+        diag.resize(static_cast<size_t>(n));
+        jacobi_diag(n, row_ptr, col_idx, values, diag.data());
+        for (int i = 0; i < n; ++i)
+            require(std::fabs(diag[static_cast<size_t>(i)]) > 1.0e-30, XPLUS_ERR_DATA,
+                    "zero diagonal entry while building Jacobi inverse");
+    }
+    require_device(o.device);
+    cuda_check(cudaSetDevice(o.device), "cudaSetDevice");
 
     auto* h = new xplus_pcg();
     h->device = o.device;
@@ -307,79 +547,19 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         h->opts = o;
         h->key = KernelKey{o.value_type, o.vector_type, o.chunk, split ? 1 : 0, 0, 0};
         h->n = n;
-        h->n_pad = S.n_pad;
-        h->n_slices = S.n_slices;
         h->nnz = row_ptr[n];
-        h->slots = S.slots;
-        h->perm = S.perm;
         cuda_check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaEventCreate(&h->ev0), "cudaEventCreate");
         cuda_check(cudaEventCreate(&h->ev1), "cudaEventCreate");
-        const size_t np = static_cast<size_t>(S.n_pad);
+        // SM-resident kernel candidate: one block per SM, windows computed with the layout
+        int sms = 0;
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device), "attr");
+        const int res_grid = o.resident && resident_supported(h->key) ? sms : 0;
+        std::vector<int2> win;
+        if (on_device) create_layout_device(h, o, split, n, row_ptr, col_idx, values, res_grid, win);
+        else create_layout_host(h, o, split, n, row_ptr, col_idx, values, diag, res_grid, win);
+        const size_t np = static_cast<size_t>(h->n_pad);
         const size_t xs = elem_size(o.vector_type);
-        h->d_slice_ptr = dalloc<long long>(h, S.slice_ptr.size());
-        // int16 offsets from the row when the ordered bandwidth allows (lossless)
-        bool idx16 = o.index16 != 0;
-        std::vector<short> col16;
-        if (idx16) {
-            col16.resize(static_cast<size_t>(S.slots));
-            // slot (j/chunk) 32 chunk + lane chunk + j%chunk of slice sl belongs to row 32 sl + lane
-            std::vector<unsigned char> far(static_cast<size_t>(S.n_slices), 0);
-            const int ch = o.chunk;
-            parallel_for(S.n_slices, [&](int64_t b, int64_t e) {
-                for (int64_t sl = b; sl < e; ++sl) {
-                    const int64_t base = S.slice_ptr[static_cast<size_t>(sl)];
-                    const int64_t groups = (S.slice_ptr[static_cast<size_t>(sl) + 1] - base) / (32 * ch);
-                    for (int64_t jg = 0; jg < groups; ++jg)
-                        for (int lane = 0; lane < 32; ++lane) {
-                            const int row = static_cast<int>(sl) * 32 + lane;
-                            const int64_t p0 = base + jg * 32 * ch + lane * ch;
-                            for (int q = 0; q < ch; ++q) {
-                                const int d = S.col[static_cast<size_t>(p0 + q)] - row;
-                                if (d < -32768 || d > 32767) far[static_cast<size_t>(sl)] = 1;
-                                col16[static_cast<size_t>(p0 + q)] = static_cast<short>(d);
-                            }
-                        }
-                }
-            });
-            for (unsigned char f : far)
-                if (f) idx16 = false;
-        }
-        h->key.idx16 = idx16 ? 1 : 0;
-        // columns and values in one allocation, so one L2 access-policy window covers both
-        const size_t col_bytes = (static_cast<size_t>(S.slots) * (idx16 ? 2 : 4) + 255) / 256 * 256;
-        const size_t val_bytes = static_cast<size_t>(S.slots) * elem_size(o.value_type);
-        unsigned char* mat = dalloc<unsigned char>(h, col_bytes + val_bytes);
-        h->d_col = mat;
-        h->d_val = mat + col_bytes;
-        if (o.l2_persist) {
-            int max_window = 0;
-            cudaDeviceProp prop;
-            cuda_check(cudaGetDeviceProperties(&prop, o.device), "props");
-            cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, o.device), "attr");
-            const size_t bytes = std::min(col_bytes + val_bytes, static_cast<size_t>(max_window));
-            size_t limit = 0;
-            const size_t want = std::min(bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
-            {
-                std::lock_guard<std::mutex> lk(g_l2_mutex);
-                cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
-                if (g_l2_wants.empty()) g_l2_limit_before = limit;
-                if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
-                g_l2_wants.insert(want);
-                h->l2_want = want;
-                h->l2_user = true;
-            }
-            cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
-            if (bytes > 0 && limit > 0) {
-                h->window.base_ptr = mat;
-                h->window.num_bytes = bytes;
-                h->window.hitRatio = std::min(1.0f, static_cast<float>(limit) / static_cast<float>(bytes));
-                h->window.hitProp = cudaAccessPropertyPersisting;
-                h->window.missProp = cudaAccessPropertyStreaming;
-            }
-        }
-        h->d_perm = dalloc<int>(h, static_cast<size_t>(n));
-        h->d_minv = dalloc<unsigned char>(h, np * xs);
         h->d_b64 = dalloc<double>(h, np);
         h->d_x64 = dalloc<double>(h, np);
         // {z, p} records, or for the one-barrier resident kernel {m r, m Ap, p} x 2 generations
@@ -394,73 +574,16 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
         h->d_err = dalloc<int>(h, 1);
         h->d_out = dalloc<PcgOut>(h, 1);
         cudaStream_t st = h->stream;
-        std::vector<long long> sp(S.slice_ptr.begin(), S.slice_ptr.end());
-        cuda_check(cudaMemcpyAsync(h->d_slice_ptr, sp.data(), sp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
-        if (h->key.idx16)
-            cuda_check(cudaMemcpyAsync(h->d_col, col16.data(), col16.size() * sizeof(short), cudaMemcpyHostToDevice, st), "H2D");
-        else
-            cuda_check(cudaMemcpyAsync(h->d_col, S.col.data(), S.col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
-        cuda_check(cudaMemcpyAsync(h->d_perm, S.perm.data(), S.perm.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
-        h->val_scale = o.value_type == XPLUS_F16 ? scale16 : 1.0;
-        std::vector<unsigned char> vbytes = convert(S.val, o.value_type, h->val_scale);
-        cuda_check(cudaMemcpyAsync(h->d_val, vbytes.data(), vbytes.size(), cudaMemcpyHostToDevice, st), "H2D");
-        const bool keep64 = o.keep_fp64 != 0 && o.value_type != XPLUS_F64;
-        if (keep64) {
-            h->d_val64 = dalloc<double>(h, static_cast<size_t>(S.slots));
-            cuda_check(cudaMemcpyAsync(h->d_val64, S.val.data(), S.val.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
-        } else if (o.value_type == XPLUS_F64) {
-            h->d_val64 = static_cast<double*>(h->d_val);
-        }
-        // Jacobi inverse in SELL order (host/pcg_common.hpp:42-54: m_inv = 1 / diag), from
-        // the exact FP64 diagonal.
-        std::vector<double> dsell(np, 0.0), minv(np, 0.0);
-        for (int i = 0; i < n; ++i) {
-            dsell[static_cast<size_t>(i)] = diag[static_cast<size_t>(S.perm[static_cast<size_t>(i)])];
-            minv[static_cast<size_t>(i)] = 1.0 / dsell[static_cast<size_t>(i)];
-        }
-        if (split) {
-            std::vector<double> rs(np, 0.0);
-            parallel_for(n, [&](int64_t b, int64_t e) {
-                for (int64_t i = b; i < e; ++i) {
-                    const int old = S.perm[static_cast<size_t>(i)];
-                    double acc = 0.0;
-                    for (int k = row_ptr[old]; k < row_ptr[old + 1]; ++k) acc += values[k];
-                    rs[static_cast<size_t>(i)] = acc;
-                }
-            });
-            std::vector<unsigned char> rb = convert(rs, o.vector_type);
-            h->d_rowsum = dalloc<unsigned char>(h, np * xs);
-            cuda_check(cudaMemcpyAsync(h->d_rowsum, rb.data(), rb.size(), cudaMemcpyHostToDevice, st), "H2D");
-            h->d_diag64 = dalloc<double>(h, np);
-            cuda_check(cudaMemcpyAsync(h->d_diag64, dsell.data(), np * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
-        }
-        std::vector<unsigned char> mb = convert(minv, o.vector_type);
-        cuda_check(cudaMemcpyAsync(h->d_minv, mb.data(), mb.size(), cudaMemcpyHostToDevice, st), "H2D");
         const int want_tpb = o.block_threads > 0 ? o.block_threads : 512;
         // SM-resident kernel when its shared-memory band + halo fits one CTA per SM
-        if (o.resident && resident_supported(h->key)) {
-            int sms = 0;
-            cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device), "attr");
-            const int grid = sms;
-            const int per_block = (S.n_slices + grid - 1) / grid;
+        if (res_grid > 0) {
+            const int per_block = (h->n_slices + res_grid - 1) / res_grid;
             if (per_block <= resident_max_slices()) {
-                std::vector<int2> win(static_cast<size_t>(grid));
                 int max_wn = 0, max_nb = 0;
-                for (int b = 0; b < grid; ++b) {
-                    const int sb = b * per_block, se = std::min(S.n_slices, sb + per_block);
-                    if (se <= sb) {
-                        win[static_cast<size_t>(b)] = make_int2(0, 0);
-                        continue;
-                    }
-                    int lo = sb * 32, hi = se * 32;
-                    for (int64_t pos = S.slice_ptr[static_cast<size_t>(sb)]; pos < S.slice_ptr[static_cast<size_t>(se)]; ++pos) {
-                        lo = std::min(lo, S.col[static_cast<size_t>(pos)]);
-                        hi = std::max(hi, S.col[static_cast<size_t>(pos)] + 1);
-                    }
-                    lo &= ~3;                                        // 16-byte aligned window
-                    hi = std::min(S.n_pad, (hi + 3) & ~3);
-                    win[static_cast<size_t>(b)] = make_int2(lo, hi - lo);
-                    max_wn = std::max(max_wn, hi - lo);
+                for (int b = 0; b < res_grid; ++b) {
+                    const int sb = b * per_block, se = std::min(h->n_slices, sb + per_block);
+                    if (se <= sb) continue;
+                    max_wn = std::max(max_wn, win[static_cast<size_t>(b)].y);
                     max_nb = std::max(max_nb, (se - sb) * 32);
                 }
                 const size_t smem = sizeof(float) * (static_cast<size_t>(max_wn) + 5 * static_cast<size_t>(max_nb));
@@ -470,7 +593,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
                 if (fits) {
                     h->resident = true;
                     h->smem_bytes = smem;
-                    h->grid = grid;
+                    h->grid = res_grid;
                     h->tpb = want_tpb;
                     h->d_win = dalloc<int2>(h, win.size());
                     cuda_check(cudaMemcpyAsync(h->d_win, win.data(), win.size() * sizeof(int2), cudaMemcpyHostToDevice, st), "H2D");
@@ -478,7 +601,7 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
             }
         }
         if (!h->resident)
-            cuda_check(pcg_grid(h->key, o.device, S.n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
+            cuda_check(pcg_grid(h->key, o.device, h->n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
         h->d_partial = dalloc<double>(h, static_cast<size_t>(16) * h->grid);
         h->d_block_clk = dalloc<long long>(h, static_cast<size_t>(4) * h->grid);
         cuda_check(cudaMemsetAsync(h->d_x64, 0, np * sizeof(double), st), "memset");

@@ -71,6 +71,36 @@ def rcm(row_ptr, col_idx) -> np.ndarray:
     return perm
 
 
+def rcm_device(row_ptr, col_idx, device=0):
+    """xplus_rcm_device on the GPU: (perm as a numpy array, whether the GPU ordering ran)."""
+    import torch
+    dev = torch.device("cuda", device)
+    rp = torch.as_tensor(np.ascontiguousarray(row_ptr, np.int32), device=dev)
+    ci = torch.as_tensor(np.ascontiguousarray(col_idx, np.int32), device=dev)
+    n = len(row_ptr) - 1
+    perm = torch.empty(n, dtype=torch.int32, device=dev)
+    used = C.c_int()
+    torch.cuda.synchronize(dev)
+    check(lib.xplus_rcm_device(n, rp.data_ptr(), ci.data_ptr(), perm.data_ptr(), C.byref(used), None))
+    return perm.cpu().numpy(), bool(used.value)
+
+
+def permute_symmetric_device(row_ptr, col_idx, values, perm, device=0):
+    """xplus_permute_symmetric_device on the GPU; returns numpy arrays."""
+    import torch
+    dev = torch.device("cuda", device)
+    t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a, dt), device=dev)  # noqa: E731
+    rp, ci, v, pm = t(row_ptr, np.int32), t(col_idx, np.int32), t(values, np.float64), t(perm, np.int32)
+    n = len(row_ptr) - 1
+    orp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    oci = torch.empty(len(col_idx), dtype=torch.int32, device=dev)
+    ov = torch.empty(len(col_idx), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    check(lib.xplus_permute_symmetric_device(n, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), pm.data_ptr(),
+                                             orp.data_ptr(), oci.data_ptr(), ov.data_ptr(), None))
+    return orp.cpu().numpy(), oci.cpu().numpy(), ov.cpu().numpy()
+
+
 def permute_symmetric(row_ptr, col_idx, values, perm):
     n = len(row_ptr) - 1
     rp = np.ascontiguousarray(row_ptr, np.int32)

@@ -34,6 +34,17 @@ def _params(seed=3):
     return p.astype(np.float32)
 
 
+def assert_close_bf16(got, ref, rtol=2e-4, frac=0.995):
+    """The network's node products take their activations rounded to BF16.  The oracle rounds
+    its FP64 activations, the GPU its FP32 ones, so a value within ~1e-7 of a BF16 rounding
+    boundary can round to neighbouring BF16 values on the two sides (one BF16 step is 2^-8
+    relative): nearly every entry agrees to rtol, and every entry to 1e-2."""
+    scale = np.abs(ref).max()
+    tight = np.abs(got - ref) <= rtol * np.abs(ref) + 0.1 * rtol * scale
+    assert tight.mean() >= frac, (tight.mean(), np.abs(got - ref).max())
+    np.testing.assert_allclose(got, ref, rtol=1e-2, atol=1e-3 * scale)
+
+
 def _glow_from_oracle(d, go, gd):
     g = O.graph(d.row_ptr, d.col_idx, d.values)
     G = O.g_matrix(g, go, gd).tocsr()
@@ -62,7 +73,7 @@ def test_forward_matches_oracle(trainer):
         ref = _glow_from_oracle(d, go, gd)
         got = t.predict(k)
         assert got.shape == ref.shape
-        np.testing.assert_allclose(got, ref, rtol=2e-4, atol=2e-5 * np.abs(ref).max())
+        assert_close_bf16(got, ref)
 
 
 def test_loss_and_gradient_match_oracle(trainer):
@@ -275,7 +286,7 @@ def test_solver_inference_matches_trainer(trainer):
         s.set_gnn(theta, refine_sweeps=0)
         got = s.get_gtg()
         ref = _glow_from_oracle(d, *O.normalize_rows(g, go, gd))
-        np.testing.assert_allclose(got, ref, rtol=5e-4, atol=5e-5 * np.abs(ref).max())
+        assert_close_bf16(got, ref, rtol=5e-4)
         G = _gmat(d, got)
         np.testing.assert_allclose((G @ A_of(d) @ G.T).diagonal(), 1.0, rtol=2e-5)
         raw = _gmat(d, t.predict(k))  # the trainer's output has the same row directions
@@ -285,7 +296,7 @@ def test_solver_inference_matches_trainer(trainer):
         s.set_gnn(theta)
         got1 = s.get_gtg()
         ref1 = _glow_from_oracle(d, *O.normalize_rows(g, O.refine_rows(g, go, gd, 1), gd))
-        np.testing.assert_allclose(got1, ref1, rtol=1e-3, atol=1e-4 * np.abs(ref1).max())
+        assert_close_bf16(got1, ref1, rtol=1e-3)
         G1 = _gmat(d, got1)
         np.testing.assert_allclose((G1 @ A_of(d) @ G1.T).diagonal(), 1.0, rtol=2e-5)
         s.close()

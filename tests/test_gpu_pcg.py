@@ -512,19 +512,42 @@ def test_max_iters_one_and_exact_start(gpu, sys0):
     assert r0.converged and r0.iterations == 0
 
 
-def test_create_with_gpu_and_host_builders_agree(gpu):
-    """xplus_pcg_create builds the layout on the GPU by default; the host builder gives the
-    same handle: identical solves, bit for bit."""
-    d, _ = g.fem2d(90, sigma=2.0, perm_seed=2, rcm=True)
-    out = []
-    for gpu_build in (True, False):
-        s = xp.PcgSolver.from_dataset(d, build_on_gpu=gpu_build)
-        r = s.solve(d.b, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE, trace=True)
-        out.append((r.iterations, r.solution.copy(), [t.residual for t in r.iteration_trace]))
-        s.close()
-    assert out[0][0] == out[1][0]
-    np.testing.assert_array_equal(out[0][1], out[1][1])
-    np.testing.assert_array_equal(out[0][2], out[1][2])
+@pytest.mark.parametrize("kw", [dict(), dict(values_dtype="f64", vector_dtype="f64", chunk=2),
+                                dict(values_dtype="f32", vector_dtype="f64"), dict(index16=False),
+                                dict(row_sum_form=False, chunk=1), dict(resident=False, sigma=1),
+                                dict(values_dtype="f16", split_ratio=0.0), dict(barriers_per_iter=2)])
+def test_create_with_gpu_and_host_builders_agree(gpu, kw):
+    """xplus_pcg_create derives every array on the GPU from one device copy of the CSR by
+    default (checks, Jacobi diagonal, SELL image, int16 offsets, value conversion, FP64 copy,
+    row sums, resident windows); the host builder gives the same handle: identical solves, bit
+    for bit, and the same layout sizes, on a 2D and a 3D system."""
+    for d in (g.fem2d(90, sigma=2.0, perm_seed=2, rcm=True)[0], g.fem3d(14, sigma=1.5, perm_seed=3, rcm=True)[0]):
+        out = []
+        for gpu_build in (True, False):
+            s = xp.PcgSolver.from_dataset(d, build_on_gpu=gpu_build, **kw)
+            r = s.solve(d.b, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE, trace=True)
+            out.append((r.iterations, r.solution.copy(), [t.residual for t in r.iteration_trace], s.info(),
+                        r.metrics["kernel"]))
+            s.close()
+        assert out[0][0] == out[1][0] and out[0][3] == out[1][3] and out[0][4] == out[1][4]
+        np.testing.assert_array_equal(out[0][1], out[1][1])
+        np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("gpu_build", [True, False])
+def test_create_rejects_bad_systems_with_the_reference_messages(gpu, gpu_build):
+    """Both create paths refuse a CSR or diagonal the reference refuses, with its messages."""
+    from project_xplus_b200 import XplusError
+    d, _ = g.fem2d(6, sigma=1.0)
+    ci = d.col_idx.copy()
+    ci[3] = d.n + 5
+    with pytest.raises(XplusError, match="col_idx out of range"):
+        xp.PcgSolver(d.row_ptr, ci, d.values, build_on_gpu=gpu_build)
+    v = d.values.copy()
+    rows = np.repeat(np.arange(d.n), np.diff(d.row_ptr))
+    v[(d.col_idx == rows) & (rows == 7)] = 0.0
+    with pytest.raises(XplusError, match="zero diagonal entry at row 7"):
+        xp.PcgSolver(d.row_ptr, d.col_idx, v, build_on_gpu=gpu_build)
 
 
 def test_gpu_builder_rejects_bad_csr(gpu):
@@ -591,3 +614,54 @@ def test_control_kernel_abi_matches_golden(gpu, oracle, sys0):
     assert status.cpu().tolist() == [2, 0] and metrics.cpu().tolist() == [0.0, 0.0, 0.0, 0.0]
     assert float(x2.abs().max()) == 0.0
     s.close()
+
+
+def _block_diag(*systems):
+    """Several CSR systems as one disconnected graph (components in the given order)."""
+    rps, cis, vs, off, nnz = [np.zeros(1, np.int32)], [], [], 0, 0
+    for d in systems:
+        rps.append(d.row_ptr[1:] + nnz)
+        cis.append(d.col_idx + off)
+        vs.append(d.values)
+        off += d.n
+        nnz += d.nnz
+    return np.concatenate(rps).astype(np.int32), np.concatenate(cis).astype(np.int32), np.concatenate(vs)
+
+
+def test_rcm_on_the_gpu_is_bit_identical_to_the_host(gpu):
+    """xplus_rcm_device gives xplus_rcm's permutation exactly: randomly permuted 2D and 3D
+    meshes, a graph of several components (taken in order of their lowest node), a star whose
+    centre has more children in one level than the GPU path takes (the host ordering then runs,
+    same result), and the symmetric permutation on the device matches the host's too."""
+    cases = [g.fem2d(60, sigma=2.0, perm_seed=4)[0], g.fem3d(12, sigma=1.5, perm_seed=5)[0], g.fem2d(1, perm_seed=1)[0]]
+    a, b = g.fem2d(20, perm_seed=7)[0], g.fem3d(6, perm_seed=8)[0]
+    rp, ci, v = _block_diag(b, a, g.fem2d(3)[0])
+    n_star = 200  # node 0 joined to all others, plus a path: 199 children of the root at once
+    star = [[0] + list(range(1, n_star))] + [[0, i] + ([i + 1] if i + 1 < n_star else []) + ([i - 1] if i > 1 else [])
+                                             for i in range(1, n_star)]
+    srp = np.concatenate([[0], np.cumsum([len(r) for r in star])]).astype(np.int32)
+    sci = np.concatenate([sorted(r) for r in star]).astype(np.int32)
+    for k, (r_, c_, vv, expect_gpu) in enumerate([(d.row_ptr, d.col_idx, d.values, True) for d in cases] +
+                                                 [(rp, ci, v, True), (srp, sci, np.ones(len(sci)), False)]):
+        host = g.rcm(r_, c_)
+        dev, used = g.rcm_device(r_, c_)
+        assert used == expect_gpu, k
+        np.testing.assert_array_equal(dev, host, err_msg=str(k))
+        out_h = g.permute_symmetric(r_, c_, vv, host)
+        out_d = g.permute_symmetric_device(r_, c_, vv, host)
+        for x, y in zip(out_h, out_d):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_rcm_gpu_on_the_config1_system(gpu):
+    """The 1108x1108 system randomly permuted (seed 1): the GPU ordering equals the host's, and
+    the reordered matrix equals what the generator produces with RCM on the host."""
+    d, _ = g.fem2d(1108, sigma=2.0, seed=0, perm_seed=1, rcm=False)
+    dev, used = g.rcm_device(d.row_ptr, d.col_idx)
+    assert used
+    np.testing.assert_array_equal(dev, g.rcm(d.row_ptr, d.col_idx))
+    rp, ci, v = g.permute_symmetric_device(d.row_ptr, d.col_idx, d.values, dev)
+    ref = g.system_2d_large()[0]
+    np.testing.assert_array_equal(rp, ref.row_ptr)
+    np.testing.assert_array_equal(ci, ref.col_idx)
+    np.testing.assert_array_equal(v, ref.values)

@@ -24,6 +24,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -903,6 +905,194 @@ void* Arena::raw(size_t bytes) {
 void Arena::release() {
     for (void* p : ptrs) cudaFree(p);
     ptrs.clear();
+}
+
+// ---------------------------------------------------------------------------------------
+// The same graph built on the GPU for inference (forward, refinement, normalization and the
+// g_low map): HostGraph::build's arrays, each CSR entry placed by its rank within its row
+// (column order, CSR order between equal columns), so no row needs a sort buffer.  The only
+// difference is the order of the FP64 sum behind the centring of log a_ii.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+// per row: diagonal (sum of its entries), |a| row sum, entry counts; bad: 1 no positive
+// diagonal, 2 more than one diagonal entry
+__global__ void k_gg_rows(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v, int n,
+                          double* __restrict__ d, double* __restrict__ rowabs, double* __restrict__ logd,
+                          int* __restrict__ n_adj, int* __restrict__ n_low, int* __restrict__ n_glow, int* __restrict__ bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double di = 0.0, ra = 0.0;
+    int seen = 0, a = 0, l = 0, gl = 0;
+    for (int q = rp[i]; q < rp[i + 1]; ++q) {
+        const int j = ci[q];
+        ra += fabs(v[q]);
+        if (j == i) {
+            di += v[q];
+            ++seen;
+        } else {
+            ++a;
+            if (j < i) ++l;
+        }
+        if (j <= i) ++gl;
+    }
+    d[i] = di;
+    rowabs[i] = ra;
+    logd[i] = di > 0.0 ? log(di) : 0.0;
+    n_adj[i] = a;
+    n_low[i] = l;
+    n_glow[i] = gl;
+    if (!(di > 0.0)) atomicOr(bad, 1);
+    if (seen > 1) atomicOr(bad, 2);
+}
+
+__global__ void k_gg_fill(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v, int n,
+                          const double* __restrict__ d, const double* __restrict__ rowabs, const double* __restrict__ logd,
+                          const double* __restrict__ mean, const int* __restrict__ adj_ptr, const int* __restrict__ low_ptr,
+                          const int* __restrict__ glow_ptr, int* __restrict__ adj_col, float* __restrict__ adj_e,
+                          int* __restrict__ low_col, float* __restrict__ low_e, int* __restrict__ pos_low,
+                          int* __restrict__ pos_diag, float* __restrict__ x, float* __restrict__ isq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double di = d[i];
+    x[2 * i] = static_cast<float>(logd[i] - *mean);
+    x[2 * i + 1] = static_cast<float>(rowabs[i] / di - 1.0);
+    isq[i] = static_cast<float>(1.0 / sqrt(di));
+    const int q0 = rp[i], q1 = rp[i + 1];
+    int g = glow_ptr[i];
+    for (int q = q0; q < q1; ++q) {
+        const int j = ci[q];
+        if (j != i) {
+            int ra = 0, rl = 0;  // rank among the row's off-diagonal / lower entries
+            for (int p = q0; p < q1; ++p) {
+                const int c = ci[p];
+                if (c == i) continue;
+                const bool ahead = c < j || (c == j && p < q);
+                ra += ahead;
+                rl += ahead && c < i;
+            }
+            const float ev = static_cast<float>(v[q] / sqrt(di * d[j]));
+            adj_col[adj_ptr[i] + ra] = j;
+            adj_e[adj_ptr[i] + ra] = ev;
+            if (j < i) {
+                low_col[low_ptr[i] + rl] = j;
+                low_e[low_ptr[i] + rl] = ev;
+                pos_low[low_ptr[i] + rl] = g++;
+            }
+        } else {
+            pos_diag[i] = g++;
+        }
+    }
+}
+
+// f_ij over the lower edges of row i (after the adjacency is complete)
+__global__ void k_gg_f(const int* __restrict__ adj_ptr, const int* __restrict__ adj_col, const float* __restrict__ adj_e,
+                       const int* __restrict__ low_ptr, const int* __restrict__ low_col, const float* __restrict__ low_e,
+                       int n, float* __restrict__ low_f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int l0 = low_ptr[i], l1 = low_ptr[i + 1];
+    for (int k = l0; k < l1; ++k) {
+        const int j = low_col[k];
+        const int a0 = adj_ptr[j], a1 = adj_ptr[j + 1];
+        double f = 0.0;
+        for (int q = l0; q < l1; ++q) {
+            if (q == k) continue;
+            const int m = low_col[q];
+            int lo = a0, hi = a1;  // first adjacency entry >= m
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (adj_col[mid] < m) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < a1 && adj_col[lo] == m) f += static_cast<double>(adj_e[lo]) * static_cast<double>(low_e[q]);
+        }
+        low_f[k] = static_cast<float>(f);
+    }
+}
+
+void gg_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+}  // namespace
+
+void DevGraph::build_on_device(int n_, const int* d_rp, const int* d_ci, const double* d_v, const int* row_ptr,
+                               const int* col_idx, const double* values, Arena& ar, cudaStream_t st) {
+    n = n_;
+    const int tb = 256;
+    Arena tmp;
+    try {
+        double* d = tmp.get<double>(static_cast<size_t>(n));
+        double* rowabs = tmp.get<double>(static_cast<size_t>(n));
+        double* logd = tmp.get<double>(static_cast<size_t>(n));
+        int* cnt = tmp.get<int>(3 * (static_cast<size_t>(n) + 1));
+        int* bad = tmp.get<int>(1);
+        double* mean = tmp.get<double>(1);
+        gg_check(cudaMemsetAsync(cnt, 0, 3 * (static_cast<size_t>(n) + 1) * sizeof(int), st), "memset");
+        gg_check(cudaMemsetAsync(bad, 0, sizeof(int), st), "memset");
+        int* c_adj = cnt;
+        int* c_low = cnt + (n + 1);
+        int* c_glow = cnt + 2 * (n + 1);
+        k_gg_rows<<<(n + tb - 1) / tb, tb, 0, st>>>(d_rp, d_ci, d_v, n, d, rowabs, logd, c_adj, c_low, c_glow, bad);
+        gg_check(cudaGetLastError(), "graph rows");
+        int h_bad = 0;
+        gg_check(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        gg_check(cudaStreamSynchronize(st), "sync");
+        if (h_bad) {
+            HostGraph hg;  // the host builder throws the message of the first failing row
+            hg.build(n, row_ptr, col_idx, values);
+            throw Error(XPLUS_ERR_DATA, "learned preconditioner needs a positive, single diagonal entry per row");
+        }
+        adj_ptr = ar.get<int>(static_cast<size_t>(n) + 1);
+        low_ptr = ar.get<int>(static_cast<size_t>(n) + 1);
+        int* glow_ptr = tmp.get<int>(static_cast<size_t>(n) + 1);
+        size_t bytes = 0;
+        gg_check(cub::DeviceScan::ExclusiveSum(nullptr, bytes, c_adj, adj_ptr, n + 1, st), "scan size");
+        void* ws = tmp.raw(std::max<size_t>(bytes, 1));
+        gg_check(cub::DeviceScan::ExclusiveSum(ws, bytes, c_adj, adj_ptr, n + 1, st), "scan");
+        gg_check(cub::DeviceScan::ExclusiveSum(ws, bytes, c_low, low_ptr, n + 1, st), "scan");
+        gg_check(cub::DeviceScan::ExclusiveSum(ws, bytes, c_glow, glow_ptr, n + 1, st), "scan");
+        size_t rbytes = 0;
+        gg_check(cub::DeviceReduce::Sum(nullptr, rbytes, logd, mean, n, st), "reduce size");
+        void* rws = tmp.raw(std::max<size_t>(rbytes, 1));
+        gg_check(cub::DeviceReduce::Sum(rws, rbytes, logd, mean, n, st), "reduce");
+        int sizes[3];
+        gg_check(cudaMemcpyAsync(&sizes[0], adj_ptr + n, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        gg_check(cudaMemcpyAsync(&sizes[1], low_ptr + n, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        gg_check(cudaMemcpyAsync(&sizes[2], glow_ptr + n, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        double h_sum = 0.0;
+        gg_check(cudaMemcpyAsync(&h_sum, mean, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        gg_check(cudaStreamSynchronize(st), "sync");
+        n_adj = sizes[0];
+        n_low = sizes[1];
+        n_glow = sizes[2];
+        const double h_mean = h_sum / static_cast<double>(n);  // the host builder's mean
+        gg_check(cudaMemcpyAsync(mean, &h_mean, sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+        adj_col = ar.get<int>(std::max(1, n_adj));
+        adj_e = ar.get<float>(std::max(1, n_adj));
+        low_col = ar.get<int>(std::max(1, n_low));
+        low_e = ar.get<float>(std::max(1, n_low));
+        low_f = ar.get<float>(std::max(1, n_low));
+        pos_low = ar.get<int>(std::max(1, n_low));
+        pos_diag = ar.get<int>(static_cast<size_t>(n));
+        x = ar.get<float>(2 * static_cast<size_t>(n));
+        isq = ar.get<float>(static_cast<size_t>(n));
+        k_gg_fill<<<(n + tb - 1) / tb, tb, 0, st>>>(d_rp, d_ci, d_v, n, d, rowabs, logd, mean, adj_ptr, low_ptr, glow_ptr,
+                                                    adj_col, adj_e, low_col, low_e, pos_low, pos_diag, x, isq);
+        gg_check(cudaGetLastError(), "graph fill");
+        k_gg_f<<<(n + tb - 1) / tb, tb, 0, st>>>(adj_ptr, adj_col, adj_e, low_ptr, low_col, low_e, n, low_f);
+        gg_check(cudaGetLastError(), "graph two-step paths");
+        gg_check(cudaStreamSynchronize(st), "sync");
+    } catch (...) {
+        cudaStreamSynchronize(st);
+        tmp.release();
+        throw;
+    }
+    tmp.release();
 }
 
 void DevGraph::upload(const HostGraph& g, Arena& ar, cudaStream_t st) {

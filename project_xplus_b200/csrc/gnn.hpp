@@ -52,6 +52,11 @@ struct DevGraph {
     int *pos_low = nullptr, *pos_diag = nullptr;
     float *adj_e = nullptr, *low_e = nullptr, *low_f = nullptr, *a_val = nullptr, *x = nullptr, *isq = nullptr;
     void upload(const HostGraph& g, Arena& ar, cudaStream_t st);
+    // The arrays inference needs (adjacency, lower edges with e and f, node inputs, 1/sqrt(a_ii),
+    // g_low positions), built on the GPU from a device CSR; the host CSR only supplies the host
+    // builder's error message when the diagonal is not positive or repeated.
+    void build_on_device(int n, const int* d_rp, const int* d_ci, const double* d_v, const int* row_ptr,
+                         const int* col_idx, const double* values, Arena& ar, cudaStream_t st);
 };
 
 // Activations and temporaries, sized for the largest system.

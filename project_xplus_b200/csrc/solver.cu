@@ -20,6 +20,7 @@
 
 #include "common.hpp"
 #include "gnn.hpp"
+#include "gtg_layout_gpu.hpp"
 #include "layout_gpu.hpp"
 #include "pcg_kernels.cuh"
 
@@ -762,14 +763,9 @@ void gtg_sell(const std::vector<std::vector<std::pair<int, int>>>& rows, int n_p
 }
 
 // Builds the G / G^T SELL images for the pattern of the CSR given to xplus_pcg_create (once).
-void gtg_layout(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
-    require(h->opts.vector_type == XPLUS_F32 && h->key.diag && h->opts.value_type != XPLUS_F64,
-            XPLUS_ERR_ARG, "G^T G preconditioning needs FP32 vectors, FP32, BF16 or FP16 values and row_sum_form");
-    require(h->d_val64 != nullptr, XPLUS_ERR_ARG, "G^T G preconditioning needs keep_fp64");
-    if (h->d_g_slice_ptr) return;
+// The host construction of the G / G^T images (the reference for gtg_layout_device).
+void gtg_layout_host(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
     const int n = h->n;
-    require(row_ptr && col_idx && row_ptr[0] == 0 && row_ptr[n] == h->nnz, XPLUS_ERR_ARG,
-            "pattern differs from the matrix of the handle");
     std::vector<int> iperm(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) iperm[static_cast<size_t>(h->perm[static_cast<size_t>(i)])] = i;
     std::vector<std::vector<std::pair<int, int>>> g(static_cast<size_t>(h->n_pad)), gt(static_cast<size_t>(h->n_pad));
@@ -799,17 +795,47 @@ void gtg_layout(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
     h->d_gt_col = dalloc<int>(h, tcol.size());
     h->d_g_map = dalloc<int>(h, map.size());
     h->d_gt_map = dalloc<int>(h, tmap.size());
-    h->d_g_val = dalloc<float>(h, col.size());
-    h->d_gt_val = dalloc<float>(h, tcol.size());
-    h->d_t = dalloc<float>(h, static_cast<size_t>(h->n_pad));
-    h->d_r2 = dalloc<float>(h, static_cast<size_t>(h->n_pad));
-    h->d_glow = dalloc<double>(h, static_cast<size_t>(gl));
     cuda_check(cudaMemcpyAsync(h->d_g_slice_ptr, sp.data(), sp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
     cuda_check(cudaMemcpyAsync(h->d_gt_slice_ptr, tsp.data(), tsp.size() * sizeof(long long), cudaMemcpyHostToDevice, st), "H2D");
     cuda_check(cudaMemcpyAsync(h->d_g_col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
     cuda_check(cudaMemcpyAsync(h->d_gt_col, tcol.data(), tcol.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
     cuda_check(cudaMemcpyAsync(h->d_g_map, map.data(), map.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
     cuda_check(cudaMemcpyAsync(h->d_gt_map, tmap.data(), tmap.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+    cuda_check(cudaStreamSynchronize(st), "sync");  // the host images go next
+}
+
+// The G / G^T images and the vectors of the G^T G kernel for the pattern of the CSR given to
+// xplus_pcg_create (once per handle): on the GPU unless the handle was built on the host.
+void gtg_layout(xplus_pcg* h, const int* row_ptr, const int* col_idx) {
+    require(h->opts.vector_type == XPLUS_F32 && h->key.diag && h->opts.value_type != XPLUS_F64,
+            XPLUS_ERR_ARG, "G^T G preconditioning needs FP32 vectors, FP32, BF16 or FP16 values and row_sum_form");
+    require(h->d_val64 != nullptr, XPLUS_ERR_ARG, "G^T G preconditioning needs keep_fp64");
+    if (h->d_g_slice_ptr) return;
+    const int n = h->n;
+    require(row_ptr && col_idx && row_ptr[0] == 0 && row_ptr[n] == h->nnz, XPLUS_ERR_ARG,
+            "pattern differs from the matrix of the handle");
+    if (h->opts.build_on_gpu) {
+        const GtgImages im = gtg_layout_device(n, h->n_pad, row_ptr, col_idx, h->d_perm,
+                                               [h](size_t bytes) { return static_cast<void*>(dalloc<unsigned char>(h, bytes)); },
+                                               h->stream);
+        h->n_glow = im.n_glow;
+        h->g_slots = im.g_slots;
+        h->gt_slots = im.gt_slots;
+        h->d_g_slice_ptr = im.g_slice_ptr;
+        h->d_gt_slice_ptr = im.gt_slice_ptr;
+        h->d_g_col = im.g_col;
+        h->d_g_map = im.g_map;
+        h->d_gt_col = im.gt_col;
+        h->d_gt_map = im.gt_map;
+    } else {
+        gtg_layout_host(h, row_ptr, col_idx);
+    }
+    cudaStream_t st = h->stream;
+    h->d_g_val = dalloc<float>(h, static_cast<size_t>(h->g_slots));
+    h->d_gt_val = dalloc<float>(h, static_cast<size_t>(h->gt_slots));
+    h->d_t = dalloc<float>(h, static_cast<size_t>(h->n_pad));
+    h->d_r2 = dalloc<float>(h, static_cast<size_t>(h->n_pad));
+    h->d_glow = dalloc<double>(h, static_cast<size_t>(h->n_glow));
     cuda_check(cudaMemsetAsync(h->d_r2, 0, static_cast<size_t>(h->n_pad) * sizeof(float), st), "memset");
     cuda_check(cudaMemsetAsync(h->d_t, 0, static_cast<size_t>(h->n_pad) * sizeof(float), st), "memset");
     int gtg_tpb = 0;
@@ -1114,16 +1140,22 @@ int xplus_pcg_set_gnn_ex(xplus_pcg* h, const int* row_ptr, const int* col_idx, c
         cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
         gtg_layout(h, row_ptr, col_idx);
         const auto t0 = std::chrono::steady_clock::now();
-        gnn::HostGraph hg;
-        hg.build(h->n, row_ptr, col_idx, values);
-        require(hg.n_glow == h->n_glow, XPLUS_ERR_DATA, "matrix pattern needs every diagonal entry");
         gnn::Arena ar;
         try {
             cudaStream_t st = h->stream;
             gnn::DevGraph dg;
-            dg.upload(hg, ar, st);
+            if (h->opts.build_on_gpu) {
+                DeviceCsr csr;
+                upload_csr(h->n, row_ptr, col_idx, values, csr, st);
+                dg.build_on_device(h->n, csr.rp, csr.ci, csr.v, row_ptr, col_idx, values, ar, st);
+            } else {
+                gnn::HostGraph hg;
+                hg.build(h->n, row_ptr, col_idx, values);
+                dg.upload(hg, ar, st);
+            }
+            require(dg.n_glow == h->n_glow, XPLUS_ERR_DATA, "matrix pattern needs every diagonal entry");
             gnn::Work w;
-            w.alloc(ar, hg.n, std::max(1, hg.n_low), 1, false);
+            w.alloc(ar, dg.n, std::max(1, dg.n_low), 1, false);
             const int P = gnn::param_offsets().total;
             float* master = ar.get<float>(static_cast<size_t>(P));
             float* wr = ar.get<float>(static_cast<size_t>(P));

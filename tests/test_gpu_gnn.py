@@ -377,3 +377,38 @@ def test_scale_gtg_normalizes_rows(gpu):
     s.scale_gtg()
     np.testing.assert_allclose(s.get_gtg(), f, rtol=1e-12)
     s.close()
+
+
+def test_inference_graph_on_gpu_matches_host(gpu):
+    """The network's input graph built on the GPU (the default) and on the host give the same G:
+    every array but the centring of log a_ii is bit-identical, and that one differs only in the
+    order of its FP64 sum, so G agrees to the BF16 activation rounding; the solves agree too."""
+    from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
+    from project_xplus_b200 import generators as gen
+    from project_xplus_b200.learned import load_weights
+    params, _ = load_weights()
+    for d in (gen.fem2d(120, sigma=2.0, seed=5, perm_seed=5, rcm=True)[0], gen.fem3d(18, sigma=1.5, seed=6, perm_seed=6, rcm=True)[0]):
+        out = []
+        for gpu_build in (True, False):
+            s = PcgSolver(d.row_ptr, d.col_idx, d.values, build_on_gpu=gpu_build)
+            s.set_gnn(params)
+            r = s.solve(d.b, tau=1e-8, tau_mode=XPLUS_TAU_REL_TRUE)
+            assert r.converged and r.residual_rel <= 1e-8
+            out.append((s.get_gtg(), r.iterations))
+            s.close()
+        assert_close_bf16(out[0][0], out[1][0], rtol=1e-5)
+        assert abs(out[0][1] - out[1][1]) <= max(2, 0.02 * out[1][1])
+    # a non-positive diagonal is refused with the host builder's message
+    from project_xplus_b200 import XplusError
+    d = gen.fem2d(8, sigma=1.0)[0]
+    s = PcgSolver(d.row_ptr, d.col_idx, d.values)
+    v = d.values.copy()
+    rows = np.repeat(np.arange(d.n), np.diff(d.row_ptr))
+    v[(d.col_idx == rows) & (rows == 3)] *= -1.0
+    import ctypes as C
+    from project_xplus_b200 import _lib
+    p = np.ascontiguousarray(params, np.float32)
+    rc = _lib.lib.xplus_pcg_set_gnn(s.handle, d.row_ptr.ctypes.data, d.col_idx.ctypes.data, v.ctypes.data,
+                                    p.ctypes.data, 0, None)
+    assert rc == _lib.XPLUS_ERR_DATA and "positive diagonal" in _lib.last_error()
+    s.close()

@@ -665,3 +665,31 @@ def test_rcm_gpu_on_the_config1_system(gpu):
     np.testing.assert_array_equal(rp, ref.row_ptr)
     np.testing.assert_array_equal(ci, ref.col_idx)
     np.testing.assert_array_equal(v, ref.values)
+
+
+def test_gtg_layouts_on_gpu_and_host_agree(gpu):
+    """The G and G^T SELL images of the factorized preconditioner, built on the GPU (stable
+    radix sort for the transpose) or on the host, give bit-identical solves with the same G,
+    and the layout refuses a pattern with an out-of-range column without indexing it."""
+    from project_xplus_b200 import XplusError
+    from project_xplus_b200.learned import fsai_lower
+    for d in (g.fem2d(70, sigma=2.0, perm_seed=2, rcm=True)[0], g.fem3d(11, sigma=1.5, perm_seed=6, rcm=True)[0]):
+        f = fsai_lower(d.row_ptr, d.col_idx, d.values)
+        out = []
+        for gpu_build in (True, False):
+            s = xp.PcgSolver.from_dataset(d, build_on_gpu=gpu_build)
+            s.set_gtg(f)
+            r = s.solve(d.b, tau=1e-8, tau_mode=xp.XPLUS_TAU_REL_TRUE, trace=True)
+            assert r.metrics["kernel"] == "pcg_gtg_kernel"
+            out.append((r.iterations, r.solution.copy(), [t.residual for t in r.iteration_trace]))
+            s.close()
+        assert out[0][0] == out[1][0]
+        np.testing.assert_array_equal(out[0][1], out[1][1])
+        np.testing.assert_array_equal(out[0][2], out[1][2])
+    s = xp.PcgSolver.from_dataset(d)
+    ci = d.col_idx.copy()
+    ci[5] = d.n + 3
+    with pytest.raises(XplusError, match="column index out of range"):
+        lib_ok = xp._lib.lib.xplus_pcg_set_gtg(s.handle, d.row_ptr.ctypes.data, ci.ctypes.data, f.ctypes.data, 0)
+        xp._lib.check(lib_ok)
+    s.close()

@@ -68,3 +68,72 @@ def test_batch_fails_loudly_without_gpu():
     with pytest.raises(XplusError) as e:
         BatchSolver([(d.row_ptr, d.col_idx, d.values)])
     assert e.value.code == 11  # XPLUS_ERR_CUDA
+
+
+def _solve_rank(rank, world, port, q):
+    """One rank of the sharded batch as bench.py runs it: every rank builds the same system
+    list, solves only its shard (here with the oracle's FP64 golden standing in for the GPU
+    batch kernel, which needs a GPU), times it, and the job's time is the max over ranks."""
+    import time
+
+    import torch
+    import torch.distributed as dist
+
+    from oracle import oracle as O
+    from project_xplus_b200 import generators as g
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sides, sigmas = g.batch_sides(12, 6, 24, seed=5)
+    works = [system_work(int(s) ** 2, 7 * int(s) ** 2) for s in sides]
+    mine = shard_systems(works, world, rank)
+    t0 = time.perf_counter()
+    xs = {}
+    for k in mine:
+        d, _ = g.fem2d(int(sides[k]), sigma=float(sigmas[k]), seed=1000 + k, x_seed=1000 + k)
+        tau_rr = (1e-8 * float(np.linalg.norm(d.b))) ** 2
+        xs[k] = O.golden(d, tau_rr)["x"]
+    dt = torch.tensor([time.perf_counter() - t0], dtype=torch.float64)
+    dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, xs)
+    dist.destroy_process_group()
+    q.put((rank, float(dt.item()), gathered))
+
+
+def test_two_ranks_solve_their_shards():
+    """Two gloo ranks each solve their shard of a batch; the gathered solutions cover every
+    system once and equal a one-process solve of the whole batch bit for bit, every solution
+    meets the FP64 true-residual tolerance, and both ranks report the same max-over-ranks time."""
+    import multiprocessing as mp
+    import socket
+
+    from oracle import oracle as O
+    from project_xplus_b200 import generators as g
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_solve_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in procs:
+        rank, t, gathered = q.get(timeout=300)
+        out[rank] = (t, gathered)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out[0][0] == out[1][0] > 0.0
+    merged = {}
+    for part in out[0][1]:
+        assert not set(part) & set(merged)
+        merged.update(part)
+    sides, sigmas = g.batch_sides(12, 6, 24, seed=5)
+    assert sorted(merged) == list(range(len(sides)))
+    for k in range(len(sides)):
+        d, _ = g.fem2d(int(sides[k]), sigma=float(sigmas[k]), seed=1000 + k, x_seed=1000 + k)
+        ref = O.golden(d, (1e-8 * float(np.linalg.norm(d.b))) ** 2)["x"]
+        np.testing.assert_array_equal(merged[k], ref)
+        assert O.residual_norm(d, merged[k]) <= 1e-8 * np.linalg.norm(d.b)

@@ -122,8 +122,11 @@ __device__ __forceinline__ double batch_row64(const BatchArgs& a, int s, int lan
     return acc + a.diag64[row] * __ldcg(a.x64 + row);
 }
 
-template <typename VT, int CHUNK, typename IT>
-__global__ void __launch_bounds__(512, 1) pcg_batch_kernel(BatchArgs a) {
+// MAXT / MINB: the 512-thread form for launches of 256 and 512 threads (126 registers), and a
+// 128-thread form held to 80 registers so that six CTAs share an SM (24 warps instead of 16;
+// no spills) for launches of 128 threads
+template <typename VT, int CHUNK, typename IT, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) pcg_batch_kernel(BatchArgs a) {
     constexpr int NS = 2;  // slices of one warp in flight together
     cg::cluster_group cl = cg::this_cluster();
     __shared__ double s_red[32 * 4];
@@ -408,26 +411,28 @@ __global__ void batch_scatter_kernel(const double* __restrict__ src, double* __r
 
 using BatchKernel = void (*)(BatchArgs);
 
-template <typename VT, typename IT>
+template <typename VT, typename IT, int MAXT, int MINB>
 BatchKernel pick_chunk(int chunk) {
     switch (chunk) {
-        case 1: return pcg_batch_kernel<VT, 1, IT>;
-        case 2: return pcg_batch_kernel<VT, 2, IT>;
-        case 4: return pcg_batch_kernel<VT, 4, IT>;
+        case 1: return pcg_batch_kernel<VT, 1, IT, MAXT, MINB>;
+        case 2: return pcg_batch_kernel<VT, 2, IT, MAXT, MINB>;
+        case 4: return pcg_batch_kernel<VT, 4, IT, MAXT, MINB>;
     }
     return nullptr;
 }
-template <typename IT>
+template <typename IT, int MAXT, int MINB>
 BatchKernel pick_vt(int vt, int chunk) {
     switch (vt) {
-        case XPLUS_F32: return pick_chunk<float, IT>(chunk);
-        case XPLUS_BF16: return pick_chunk<__nv_bfloat16, IT>(chunk);
-        case XPLUS_F16: return pick_chunk<__half, IT>(chunk);
+        case XPLUS_F32: return pick_chunk<float, IT, MAXT, MINB>(chunk);
+        case XPLUS_BF16: return pick_chunk<__nv_bfloat16, IT, MAXT, MINB>(chunk);
+        case XPLUS_F16: return pick_chunk<__half, IT, MAXT, MINB>(chunk);
     }
     return nullptr;
 }
-BatchKernel pick_kernel(int vt, int chunk, bool idx16) {
-    return idx16 ? pick_vt<short>(vt, chunk) : pick_vt<int>(vt, chunk);
+// small: the 128-thread form
+BatchKernel pick_kernel(int vt, int chunk, bool idx16, bool small) {
+    if (small) return idx16 ? pick_vt<short, 128, 6>(vt, chunk) : pick_vt<int, 128, 6>(vt, chunk);
+    return idx16 ? pick_vt<short, 512, 1>(vt, chunk) : pick_vt<int, 512, 1>(vt, chunk);
 }
 
 }  // namespace
@@ -442,7 +447,8 @@ struct xplus_batch {
     int n_slices = 0;
     int64_t total_n = 0, total_nnz = 0, slots = 0;
     bool idx16 = true;
-    xplus::BatchKernel kernel = nullptr;
+    xplus::BatchKernel kernel = nullptr;        // launches of 256 or 512 threads
+    xplus::BatchKernel kernel_small = nullptr;  // launches of 128 threads
     int cluster = 4, tpb = 512, grid = 0;
     // the `split` largest systems in a launch of their own (clusters of cluster2 CTAs of tpb2
     // threads, one cluster per system) on a second stream, beside the launch of the rest
@@ -534,6 +540,8 @@ void batch_destroy(xplus_batch* h) {
     delete h;
 }
 
+BatchKernel kernel_for(const xplus_batch* h, int tpb) { return tpb <= 128 ? h->kernel_small : h->kernel; }
+
 // Clusters of `cluster` CTAs of `tpb` threads that the device holds at once (0: not launchable).
 int active_clusters(xplus_batch* h, int cluster, int tpb) {
     cudaLaunchConfig_t cfg = {};
@@ -547,7 +555,7 @@ int active_clusters(xplus_batch* h, int cluster, int tpb) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int num = 0;
-    if (cudaOccupancyMaxActiveClusters(&num, h->kernel, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&num, kernel_for(h, tpb), &cfg) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -715,12 +723,14 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
                 if (f) idx16 = false;
         }
         h->idx16 = idx16;
-        h->kernel = pick_kernel(o.value_type, o.chunk, idx16);
-        require(h->kernel != nullptr, XPLUS_ERR_ARG, "no batch kernel for these options");
+        h->kernel = pick_kernel(o.value_type, o.chunk, idx16, false);
+        h->kernel_small = pick_kernel(o.value_type, o.chunk, idx16, true);
+        require(h->kernel != nullptr && h->kernel_small != nullptr, XPLUS_ERR_ARG, "no batch kernel for these options");
         // clusters of 16 CTAs (beyond the portable 8) for the lane of the largest systems
-        if (cudaFuncSetAttribute(reinterpret_cast<const void*>(h->kernel),
-                                 cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-            cudaGetLastError();  // then 16 is simply not launchable (active_clusters returns 0)
+        for (BatchKernel k : {h->kernel, h->kernel_small})
+            if (cudaFuncSetAttribute(reinterpret_cast<const void*>(k), cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess)
+                cudaGetLastError();  // then 16 is simply not launchable (active_clusters returns 0)
 
         // concatenated host image
         const size_t R = static_cast<size_t>(h->rows);
@@ -872,20 +882,24 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     a.out_true_rel = h->d_true_rel;
     a.out_ns = h->d_ns;
     bcheck(cudaMemsetAsync(h->d_head, 0, 2 * sizeof(int), st), "memset");
-    auto launch = [&](const BatchArgs& args, int c, int t, int g, cudaStream_t s, const char* what) {
+    auto launch = [&](const BatchArgs& args, int c, int t, int g, cudaStream_t s, int priority, const char* what) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(g);
         cfg.blockDim = dim3(t);
         cfg.stream = s;
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = c;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
+        attr[1].id = cudaLaunchAttributePriority;
+        attr[1].val.priority = priority;
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        bcheck(cudaLaunchKernelEx(&cfg, h->kernel, args), what);
+        cfg.numAttrs = 2;
+        bcheck(cudaLaunchKernelEx(&cfg, kernel_for(h, t), args), what);
     };
+    int prio_low = 0, prio_high = 0;  // numerically lower is higher priority
+    bcheck(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high), "priority range");
     const int split = std::min(h->split, h->nsys);
     if (split > 0) {
         // the largest systems first, on the second stream (fork / join through events, which
@@ -896,12 +910,14 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
         big.head = h->d_head + 1;
         bcheck(cudaEventRecord(h->ev_fork, st), "event");
         bcheck(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0), "wait");
-        launch(big, h->cluster2, h->tpb2, h->grid2, h->stream2, "batch PCG launch (largest systems)");
+        // the highest priority: when SMs free up, the CTA scheduler places this launch's
+        // clusters before the main launch's, so the largest systems get SMs of their own early
+        launch(big, h->cluster2, h->tpb2, h->grid2, h->stream2, prio_high, "batch PCG launch (largest systems)");
         bcheck(cudaEventRecord(h->ev_join, h->stream2), "event");
     }
     a.q_begin = split;
     a.q_end = h->nsys;
-    launch(a, cluster, tpb, grid, st, "batch PCG launch");
+    launch(a, cluster, tpb, grid, st, prio_low, "batch PCG launch");
     if (split > 0) bcheck(cudaStreamWaitEvent(st, h->ev_join, 0), "wait");
 }
 

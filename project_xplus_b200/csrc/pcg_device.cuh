@@ -171,6 +171,53 @@ __device__ __forceinline__ void publish(double (&v)[NV], double* s_red, double* 
         for (int q = 0; q < NV; ++q) partial[static_cast<size_t>(q) * gridDim.x + blockIdx.x] = v[q];
 }
 
+// The warp sums of eight values with 9 double shuffles instead of 40: three levels of
+// reduce-scatter (partners swap the half of the values that the other keeps, each adding
+// what it receives to what it keeps), then two plain levels.  Lane l returns the total of
+// value 4*bit4(l) + 2*bit3(l) + bit2(l); the four lanes that share those bits return the
+// same bits (a + b == b + a in floating point).
+__device__ __forceinline__ double warp_sum8_scatter(const double (&v)[8], int lane) {
+    const bool b = (lane >> 4) & 1, c = (lane >> 3) & 1, d = (lane >> 2) & 1;
+    double w[4], u[2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double keep = b ? v[4 + j] : v[j];
+        const double give = b ? v[j] : v[4 + j];
+        w[j] = keep + __shfl_xor_sync(0xffffffffu, give, 16);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const double keep = c ? w[2 + j] : w[j];
+        const double give = c ? w[j] : w[2 + j];
+        u[j] = keep + __shfl_xor_sync(0xffffffffu, give, 8);
+    }
+    double t = (d ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, d ? u[0] : u[1], 4);
+    t += __shfl_xor_sync(0xffffffffu, t, 2);
+    t += __shfl_xor_sync(0xffffffffu, t, 1);
+    return t;
+}
+
+// publish() for up to eight values at a fraction of the shuffles: warp sums by
+// warp_sum8_scatter, then warp q sums value q over the warps and writes its partial.  Every
+// call must be separated from the previous user of s_red by a __syncthreads (in the
+// persistent kernels a grid barrier always is).  Fixed combination order, as publish().
+template <int NV>
+__device__ __forceinline__ void publish_scatter(const double (&v)[NV], double* s_red, double* partial) {
+    static_assert(NV <= 8, "publish_scatter sums at most eight values");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double v8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v8[q] = q < NV ? v[q] : 0.0;
+    const double t = warp_sum8_scatter(v8, lane);
+    const int q = (((lane >> 4) & 1) << 2) | (((lane >> 3) & 1) << 1) | ((lane >> 2) & 1);
+    if ((lane & 3) == 0 && q < NV) s_red[q * 32 + warp] = t;
+    __syncthreads();
+    if (warp < NV) {
+        const double x = warp_sum(lane < nwarps ? s_red[warp * 32 + lane] : 0.0);
+        if (lane == 0) partial[static_cast<size_t>(warp) * gridDim.x + blockIdx.x] = x;
+    }
+}
+
 inline __device__ bool bad(double v) { return v != v; }
 
 // What the SpMV needs from a neighbour j: z_j = M^-1 r_j and the previous search direction

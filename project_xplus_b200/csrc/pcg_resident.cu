@@ -375,12 +375,16 @@ constexpr int kPartials1 = 7;
 template <typename VT, int CHUNK, typename IT>
 __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
     constexpr int NS = kResNS;
+    // halo float4 groups per thread loaded ahead, per record array: as many as fit the
+    // 128-register budget without spills (-Xptxas -v)
+    constexpr int kHaloU = std::is_same<VT, float>::value ? 3 : 2;
     extern __shared__ float smem[];
     __shared__ double s_red[32 * kPartials1];
     __shared__ double s_tot[kPartials1 + 1];
     __shared__ int s_flag;
     __shared__ int2 s_slice[kResSlices];
     __shared__ long long s_clk[6];
+    __shared__ int s_exp[2];
     GridBarrier bar{a.bar, a.err, a.timeout_ns, 0u, a.debug_skip_block};
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -421,12 +425,34 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
     }
     // the band's p' is rebuilt from its own previous value (beta = 0 the first time)
     for (int t = threadIdx.x; t < wn; t += blockDim.x) pw[t] = 0.0f;
+    // The rows of this band that another CTA's window covers: [r0, s_exp[0]) for the CTAs
+    // below, [s_exp[1], r0 + nb) for those above.  Only these rows' records are ever read by
+    // anyone but their owner, so the hot loop writes no others.
+    if (warp == 0) {
+        int lo = r0, hi = r0 + nb;
+        for (int c = lane; c < static_cast<int>(gridDim.x); c += 32) {
+            const int2 wc = a.win[c];
+            if (wc.y <= 0) continue;
+            if (c < static_cast<int>(blockIdx.x)) lo = max(lo, wc.x + wc.y);
+            else if (c > static_cast<int>(blockIdx.x)) hi = min(hi, wc.x);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = max(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = min(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            s_exp[0] = min(lo, r0 + nb);
+            s_exp[1] = max(hi, r0);
+        }
+    }
     if (threadIdx.x == 0) {
         for (int k = 0; k < 5; ++k) s_clk[k] = 0;
         s_clk[5] = globaltimer_ns();
         if (lead) a.out->t_start_ns = s_clk[5];
     }
     __syncthreads();
+    const int exp_lo = s_exp[0], exp_hi = s_exp[1];
     auto clock = [&](int slot) {
         if (threadIdx.x == 0) {
             const long long t = globaltimer_ns();
@@ -478,9 +504,39 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
         }
     };
 
+    // The halo's records, in float4 groups of the window [w0, w0 + wn) without the own band
+    // (w0, r0, nb and wn are multiples of 4): group u < nlo lies below the band, the others
+    // above it.  The first kHaloU groups of each thread are loaded into registers as soon as
+    // the grid barrier has made the records final (issue_halo), so the loads overlap the
+    // dot-product totals, the scalar updates and the own band's update.
+    const int nlo = (r0 - w0) >> 2;
+    const int hi0 = (r0 + nb - w0) >> 2;
+    const int nh = nlo + (wn >> 2) - hi0;
+    const int hbd = static_cast<int>(blockDim.x);
+    auto qof = [&](int u) { return u < nlo ? u : hi0 + (u - nlo); };
+    float4 hz[kHaloU], hq[kHaloU], hp[kHaloU];
+    auto issue_halo = [&](int g) {
+        const float4* zr4 = reinterpret_cast<const float4*>(rec_zr(g) + w0);
+        const float4* za4 = reinterpret_cast<const float4*>(rec_za(g) + w0);
+        const float4* p4 = reinterpret_cast<const float4*>(rec_p(g) + w0);
+#pragma unroll
+        for (int v = 0; v < kHaloU; ++v) {
+            const int u = threadIdx.x + v * hbd;
+            if (u < nh) {
+                const int qq = qof(u);
+                hz[v] = zr4[qq];
+                hq[v] = za4[qq];
+                hp[v] = p4[qq];
+            }
+        }
+    };
+    bool halo_ready = false;  // hz, hq, hp hold generation gen's halo records
+
     int gen = 0;
     residual_phase(true, gen);
     if (!bar.sync(&s_flag)) return;
+    issue_halo(gen);
+    halo_ready = true;
     grid_totals(cur_bank, 4, s_tot);
     double rz = s_tot[0], rr = s_tot[1], true_rr = s_tot[2];
     const double tau_true_rr = a.tau2_rel > 0.0 ? a.tau2_rel * s_tot[3] : a.tau_true_rr;
@@ -507,6 +563,8 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             // {m r, m Ap', p'} of these very values, so p'_new = fma(beta, p', fma(-alpha, m Ap',
             // m r)) here is bit-identical to what the neighbours rebuild from the records; then
             // the pending update dx += alpha p', r -= alpha Ap'.  Only the halo reads records.
+            if (!halo_ready) issue_halo(gen);
+            halo_ready = false;
             const float al_prev = static_cast<float>(pend);
             const bool upd = pend != 0.0;
             const bool flush = upd && it % flush_every == 0;
@@ -531,15 +589,13 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
             }
             pend = 0.0;
             {
-                // halo [w0, r0) and [r0 + nb, w0 + wn) from the records, in float4 groups
+                // halo [w0, r0) and [r0 + nb, w0 + wn) from the records, in float4 groups:
+                // the first U groups of each thread were loaded right after the grid barrier
+                // (issue_halo), the rest (halos above U * 4 * blockDim.x rows) load here
                 const float4* zr4 = reinterpret_cast<const float4*>(rec_zr(gen) + w0);
                 const float4* za4 = reinterpret_cast<const float4*>(rec_za(gen) + w0);
                 const float4* p4 = reinterpret_cast<const float4*>(rec_p(gen) + w0);
                 float4* pw4 = reinterpret_cast<float4*>(pw);
-                const int nlo = (r0 - w0) >> 2;
-                const int hi0 = (r0 + nb - w0) >> 2;
-                const int nh = nlo + (wn >> 2) - hi0;
-                auto qof = [&](int u) { return u < nlo ? u : hi0 + (u - nlo); };
                 auto fill = [&](const float4& z, const float4& q, const float4& p) {
                     float4 o;
                     o.x = __fmaf_rn(be, p.x, __fmaf_rn(-al_prev, q.x, z.x));
@@ -548,10 +604,14 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                     o.w = __fmaf_rn(be, p.w, __fmaf_rn(-al_prev, q.w, z.w));
                     return o;
                 };
-                // four float4 groups per thread in flight: all twelve loads before any store
-                constexpr int U = 4;
-                const int bd = static_cast<int>(blockDim.x);
-                int u = threadIdx.x;
+#pragma unroll
+                for (int v = 0; v < kHaloU; ++v) {
+                    const int u = threadIdx.x + v * hbd;
+                    if (u < nh) pw4[qof(u)] = fill(hz[v], hq[v], hp[v]);
+                }
+                constexpr int U = kHaloU;
+                const int bd = hbd;
+                int u = threadIdx.x + U * bd;
                 for (; u + (U - 1) * bd < nh; u += U * bd) {
                     float4 z[U], q[U], p[U];
 #pragma unroll
@@ -599,9 +659,11 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                         const float ap_ = y[k] * a.val_scale + rsv[t] * pi[k];
                         apv[t] = ap_;
                         const float r_ = rv[t], m = mi[t];
-                        zr1[row[k]] = m * r_;
-                        za1[row[k]] = m * ap_;
-                        p1[row[k]] = pi[k];
+                        if (row[k] < exp_lo || row[k] >= exp_hi) {
+                            zr1[row[k]] = m * r_;
+                            za1[row[k]] = m * ap_;
+                            p1[row[k]] = pi[k];
+                        }
                         const double dr = r_, da = ap_, dm = m;
                         acc[0] += static_cast<double>(pi[k]) * da;
                         acc[1] += dm * dr * dr;
@@ -614,10 +676,12 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 }
                 clock(3);
                 cur_bank = next_bank();
-                publish<kPartials1>(acc, s_red, cur_bank);
+                publish_scatter<kPartials1>(acc, s_red, cur_bank);
             }
             clock(0);
             if (!bar.sync(&s_flag)) return;
+            issue_halo(gen ^ 1);  // the generation just published
+            halo_ready = true;
             grid_totals(cur_bank, kPartials1, s_tot);
             clock(1);
             gen ^= 1;
@@ -650,6 +714,7 @@ __global__ void __launch_bounds__(512, 1) pcg_resident1_kernel(PcgArgs a) {
                 if (a.replace_drop > 0.0 && rr_new <= a.replace_drop * rr_at_replace) do_replace = drop_replace = true;
             }
             if (do_replace) {
+                halo_ready = false;  // the residual phase rewrites this generation's records
                 apply_update(static_cast<float>(pend));
                 pend = 0.0;
                 __syncthreads();

@@ -718,12 +718,14 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
         raise SystemExit(f"batch: {int((r['status'] != 0).sum())} systems did not converge")
     tot = max_over_ranks(pg, sum(ms), dev)
     s.close()
-    # the same batch with BF16 values (the other value type of the batched workload), on the
-    # launch shape tuned for FP32
+    # the same batch with BF16 values (the other value type of the batched workload), with its
+    # own tuned kernel and launch shapes
     s16 = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems], values_dtype="bf16")
-    s16.set_launch(info["cluster"], info["block_threads"])
-    lane = info["split_lane"]
-    s16.set_split_lane(lane["count"], lane["cluster"], lane["block_threads"])
+    x.zero_()
+    s16.solve_device(b, x, tau=args.tol, stream=stream)
+    stream.synchronize()
+    tune16 = s16.autotune(iters=0, tau=args.tol)
+    info16 = s16.info()
     for _ in range(args.warmup):
         x.zero_()
         s16.solve_device(b, x, tau=args.tol, stream=stream)
@@ -746,7 +748,11 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
     s16.close()
     bf16 = {"value": len(sides) * args.steps / (tot16 / 1e3), "unit": "systems/s", "ms_per_step": tot16 / args.steps,
             "converged": int((r16["status"] == 0).sum()), "iterations_total": int(r16["iterations"].sum()),
-            "max_true_rel_residual": float(r16["true_rel"].max())}
+            "max_true_rel_residual": float(r16["true_rel"].max()),
+            "system_ms_max": float(r16["system_ms"].max()),
+            "launch": {"cluster": info16["cluster"], "block_threads": info16["block_threads"],
+                       "grid": info16["grid"], "autotune_ms": tune16["ms"],
+                       "largest_systems_lane": info16["split_lane"], "resident": info16["resident"]}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = batch_cpu_baseline(systems, [works[k] for k in mine], args.tol)
@@ -758,7 +764,8 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
             "system_ms": {"max": float(r["system_ms"].max()), "median": float(np.median(r["system_ms"])),
                           "sum": float(r["system_ms"].sum())},
             "launch": {"cluster": info["cluster"], "block_threads": info["block_threads"], "grid": info["grid"],
-                       "autotune_ms": tune["ms"], "largest_systems_lane": info["split_lane"]},
+                       "autotune_ms": tune["ms"], "largest_systems_lane": info["split_lane"],
+                       "resident": info["resident"]},
             "graph": True, "bf16_values": bf16}
 
 

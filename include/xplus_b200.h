@@ -364,10 +364,24 @@ int xplus_batch_set_launch(xplus_batch* h, int cluster, int block_threads);
 int xplus_batch_set_split(xplus_batch* h, int count, int cluster, int block_threads);
 /* The current split: count (0: none), cluster, block_threads and grid of its launch. */
 int xplus_batch_split_info(xplus_batch* h, int* count, int* cluster, int* block_threads, int* grid);
+/* on != 0: both launches run the cluster-resident kernel.  Each CTA of a cluster keeps, for the
+ * whole solve of its system, its band's r, Ap', dx, M^-1 and row sums and the window of the
+ * search direction that its columns reach in shared memory (the single-system SM-resident
+ * iteration with one cluster barrier per iteration); each launch is given the dynamic shared
+ * memory of the largest band among the systems it takes.  XPLUS_ERR_ARG when a system does not
+ * fit at its launch's cluster size (split the largest systems off into bigger clusters first);
+ * 0: the global-memory kernel (two cluster barriers per iteration, no shared-memory limit). */
+int xplus_batch_set_resident(xplus_batch* h, int on);
+/* Whether the resident kernel is on, and the dynamic shared memory (bytes per CTA) of the main
+ * and the split launch (0 when off or no split). */
+int xplus_batch_resident_info(xplus_batch* h, int* on, int* smem, int* smem_split);
 /* The launch-shape autotuner: times every cluster x block_threads shape that launches and keeps
  * the fastest, with x0 = 0 for every system; then, on that shape, splits off the 1, 2, 4, 8 or
- * 16 largest systems (at most a quarter of them) into clusters of 16 x 512, 8 x 512 or 16 x 256
- * and keeps a split when it is faster (xplus_batch_split_info reports it).  iters > 0: that many
+ * 16 largest systems (at most a quarter of them) into clusters of 16 x 512, 8 x 512 or 16 x 256;
+ * then the resident kernel, with main launches of 2, 4 or 8 CTAs x 256 or 512 threads and the
+ * systems that do not fit the main launch's shared memory (or half an SM's, so that two CTAs
+ * share one) in a split launch of 16-CTA clusters.  It keeps the fastest of all
+ * (xplus_batch_split_info and xplus_batch_resident_info report it).  iters > 0: that many
  * PCG iterations per system on b = 1; iters <= 0: every system solved to FP64 true relative
  * residual tau (0 < tau < 1) on the right-hand side of the last solve (b = 1 before any solve),
  * so the queue's makespan on the caller's workload is what is timed.  Returns the main shape

@@ -90,7 +90,18 @@ class BatchSolver:
         check(lib.xplus_batch_info(self._h, C.byref(n), C.byref(nnz), C.byref(cl), C.byref(tpb), C.byref(grid),
                                    C.byref(sp)))
         return dict(total_n=n.value, total_nnz=nnz.value, cluster=cl.value, block_threads=tpb.value,
-                    grid=grid.value, spmv_bytes=sp.value, split_lane=self.split_lane())
+                    grid=grid.value, spmv_bytes=sp.value, split_lane=self.split_lane(), resident=self.resident())
+
+    def set_resident(self, on: bool = True) -> None:
+        """Both launches on the cluster-resident kernel (vectors and the search direction's
+        window in shared memory, one cluster barrier per iteration), or back to the
+        global-memory kernel.  Raises when a system does not fit its launch's cluster size."""
+        check(lib.xplus_batch_set_resident(self._h, 1 if on else 0))
+
+    def resident(self) -> dict:
+        on, sm, sm2 = C.c_int(), C.c_int(), C.c_int()
+        check(lib.xplus_batch_resident_info(self._h, C.byref(on), C.byref(sm), C.byref(sm2)))
+        return dict(on=bool(on.value), smem=sm.value, smem_split=sm2.value)
 
     def set_split_lane(self, count: int, cluster: int = 16, block_threads: int = 512) -> None:
         """The `count` largest systems in a concurrent launch of their own (0: none)."""
@@ -105,11 +116,12 @@ class BatchSolver:
         check(lib.xplus_batch_set_launch(self._h, int(cluster), int(block_threads)))
 
     def autotune(self, iters: int = 0, tau: float = 1e-8) -> dict:
-        """Launch shape, then the lane of the largest systems: fixed `iters` iterations per
-        system, or (iters=0) full solves to tau."""
+        """Kernel (global-memory or cluster-resident), launch shape and the lane of the largest
+        systems: fixed `iters` iterations per system, or (iters=0) full solves to tau."""
         cl, tpb, ms = C.c_int(), C.c_int(), C.c_double()
         check(lib.xplus_batch_autotune(self._h, int(iters), float(tau), C.byref(cl), C.byref(tpb), C.byref(ms)))
-        return dict(cluster=cl.value, block_threads=tpb.value, ms=ms.value, split_lane=self.split_lane())
+        return dict(cluster=cl.value, block_threads=tpb.value, ms=ms.value, split_lane=self.split_lane(),
+                    resident=self.resident())
 
     def split(self, x) -> list[np.ndarray]:
         return [x[self.offsets[k]:self.offsets[k + 1]] for k in range(self.nsys)]

@@ -24,103 +24,15 @@
 #include <type_traits>
 #include <vector>
 
+#include "batch_common.cuh"
 #include "common.hpp"
 #include "device_common.cuh"
 #include "pcg_device.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace xplus {
 namespace {
 
 using namespace dev;
-
-struct BatchArgs {
-    int nsys;
-    int q_begin, q_end;       // this launch takes queue positions [q_begin, q_end)
-    const int* order;         // queue: system ids in the order they are taken
-    int* head;                // this launch's queue head (atomic), zero at launch
-    const int* sys_slice0;    // [nsys + 1] first global slice of each system
-    const int* sys_n;         // rows of each system
-    const float* sys_scale;   // stored off-diagonal value = a_ij / scale (FP16), else 1
-    const long long* slice_ptr;
-    const void* col;          // int32 global rows or int16 offsets from the row
-    const void* val;          // off-diagonal weights (row-sum form), VT
-    const double* val64;      // FP64 copy of the off-diagonals, same layout
-    const double* diag64;     // FP64 diagonal
-    const float* rowsum;      // s_i = sum_j a_ij
-    const float* minv;        // 1 / a_ii
-    const double* b64;
-    double* x64;
-    NodeRec<float>* rec;      // {z, p} per row
-    float* r;
-    float* ap;
-    double tau;
-    int tau_mode;             // XPLUS_TAU_ABS_RR | XPLUS_TAU_REL_TRUE
-    int max_iters;            // <= 0: max(4n, 1000) per system
-    int replace_every;
-    double replace_drop2;     // squared ||r|| drop that triggers a replacement (0: off)
-    int restart_on_replace;   // ReplacePolicy: 0 keep p, 1 / 2 restart, 3 / 4 adaptive
-    double stag_factor;
-    int stag_window;
-    int* out_status;
-    int* out_iters;
-    int* out_repl;
-    double* out_true_rel;
-    long long* out_ns;        // device time of each system (first pop to exit residual)
-};
-
-__device__ __forceinline__ NodeRec<float> ldcg_rec(const NodeRec<float>* q) {
-    const float2 v = __ldcg(reinterpret_cast<const float2*>(q));
-    return NodeRec<float>{v.x, v.y};
-}
-
-// Sum of NV per-thread values over the cluster: block tree, then the per-CTA partials read
-// through distributed shared memory in rank order (same result in every CTA).  Two banks of
-// partials: a CTA that runs ahead writes the other bank, and a bank is rewritten only after
-// the next cluster barrier, by which time every reader has finished with it.
-template <int NV>
-__device__ __forceinline__ void cluster_sum(cg::cluster_group& cl, double (&v)[NV], double* s_red,
-                                            double (*s_part)[4], double* s_tot, int& pbank) {
-    block_sum<NV>(v, s_red);
-    if (threadIdx.x == 0)
-#pragma unroll
-        for (int q = 0; q < NV; ++q) s_part[pbank][q] = v[q];
-    cl.sync();
-    if (threadIdx.x < NV) {
-        const int cs = static_cast<int>(cl.num_blocks());
-        double t = 0.0;
-        for (int rk = 0; rk < cs; ++rk) t += *cl.map_shared_rank(&s_part[pbank][threadIdx.x], rk);
-        s_tot[threadIdx.x] = t;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < NV; ++q) v[q] = s_tot[q];
-    pbank ^= 1;
-}
-
-// FP64 row of A times x: stored off-diagonals (FP64 copy) plus the exact diagonal.  x of
-// neighbouring rows is read through L2 (another CTA of the cluster wrote it).
-template <int CHUNK, typename IT>
-__device__ __forceinline__ double batch_row64(const BatchArgs& a, int s, int lane) {
-    const long long base = a.slice_ptr[s];
-    const int w = static_cast<int>((a.slice_ptr[s + 1] - base) >> 5);
-    const int row = s * 32 + lane;
-    const double* vp = a.val64 + base + lane * CHUNK;
-    const IT* cp = static_cast<const IT*>(a.col) + base + lane * CHUNK;
-    double acc = 0.0;
-    for (int c = 0; c < w; c += CHUNK) {
-        double v[CHUNK];
-        int cc[CHUNK];
-        ChunkLoad<double, CHUNK, true>::run(vp, v);
-        ColLoad<CHUNK, IT, true>::run(cp, row, cc);
-#pragma unroll
-        for (int q = 0; q < CHUNK; ++q) acc += v[q] * __ldcg(a.x64 + cc[q]);
-        vp += 32 * CHUNK;
-        cp += 32 * CHUNK;
-    }
-    return acc + a.diag64[row] * __ldcg(a.x64 + row);
-}
 
 // MAXT / MINB: the 512-thread form for launches of 256 and 512 threads (126 registers), and a
 // 128-thread form held to 80 registers so that six CTAs share an SM (24 warps instead of 16;
@@ -409,8 +321,6 @@ __global__ void batch_scatter_kernel(const double* __restrict__ src, double* __r
     }
 }
 
-using BatchKernel = void (*)(BatchArgs);
-
 template <typename VT, typename IT, int MAXT, int MINB>
 BatchKernel pick_chunk(int chunk) {
     switch (chunk) {
@@ -453,6 +363,15 @@ struct xplus_batch {
     // the `split` largest systems in a launch of their own (clusters of cluster2 CTAs of tpb2
     // threads, one cluster per system) on a second stream, beside the launch of the rest
     int split = 0, cluster2 = 16, tpb2 = 512, grid2 = 0;
+    // the cluster-resident kernel (both lanes): vectors and the p' window in shared memory,
+    // each launch sized for the largest need of the systems it takes
+    xplus::BatchKernel res_kernel = nullptr;
+    bool resident = false;
+    int res_max_dyn = 0;             // dynamic shared memory a CTA may have (bytes)
+    int res_smem = 0, res_smem2 = 0; // the main and the split launch's dynamic shared memory
+    std::vector<int> order;          // host copy of the queue (system ids, largest first)
+    std::vector<int> need[5];        // [log2 cluster][system]: resident bytes per CTA
+    float* d_rec3 = nullptr;
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<int> sys_n;
@@ -490,6 +409,7 @@ struct xplus_batch {
     double* g_x = nullptr;
     double g_tau = 0.0;
     int g_mode = -1, g_iters = 0, g_cluster = 0, g_tpb = 0, g_split = -1, g_cluster2 = 0, g_tpb2 = 0;
+    bool g_resident = false;
     bool pending = false;
     bool have_b = false;   // d_b64 holds the (gathered) right-hand side of a solve
     double last_ms = 0.0;
@@ -540,13 +460,29 @@ void batch_destroy(xplus_batch* h) {
     delete h;
 }
 
-BatchKernel kernel_for(const xplus_batch* h, int tpb) { return tpb <= 128 ? h->kernel_small : h->kernel; }
+int log2_cluster(int c) { return c <= 1 ? 0 : c == 2 ? 1 : c == 4 ? 2 : c == 8 ? 3 : 4; }
 
-// Clusters of `cluster` CTAs of `tpb` threads that the device holds at once (0: not launchable).
-int active_clusters(xplus_batch* h, int cluster, int tpb) {
+BatchKernel kernel_for(const xplus_batch* h, int tpb) {
+    if (h->resident) return h->res_kernel;
+    return tpb <= 128 ? h->kernel_small : h->kernel;
+}
+
+// Largest resident-kernel need (bytes of dynamic shared memory per CTA) of the systems at queue
+// positions [q0, q1) on clusters of `cluster` CTAs.
+int lane_need(const xplus_batch* h, int q0, int q1, int cluster) {
+    const std::vector<int>& nd = h->need[log2_cluster(cluster)];
+    int m = 0;
+    for (int q = q0; q < q1; ++q) m = std::max(m, nd[static_cast<size_t>(h->order[static_cast<size_t>(q)])]);
+    return m;
+}
+
+// Clusters of `cluster` CTAs of `tpb` threads (and `smem` bytes of dynamic shared memory) that
+// the device holds at once (0: not launchable).
+int active_clusters(xplus_batch* h, int cluster, int tpb, int smem = 0) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cluster);
     cfg.blockDim = dim3(tpb);
+    cfg.dynamicSmemBytes = static_cast<size_t>(smem);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cluster;
@@ -562,31 +498,102 @@ int active_clusters(xplus_batch* h, int cluster, int tpb) {
     return num;
 }
 
+// Grids of the two launches (and, for the resident kernel, their dynamic shared memory) for
+// the handle's current kernel and shapes; throws when a shape cannot launch or a system does
+// not fit the resident kernel's shared memory at its lane's cluster size.
+void plan(xplus_batch* h) {
+    const int split = std::min(h->split, h->nsys);
+    if (h->resident) {
+        h->res_smem = lane_need(h, split, h->nsys, h->cluster);
+        require(h->res_smem <= h->res_max_dyn, XPLUS_ERR_ARG,
+                "a system of the main launch does not fit the resident kernel's shared memory at cluster " +
+                    std::to_string(h->cluster) + " (" + std::to_string(h->res_smem) + " bytes per CTA)");
+        h->res_smem2 = split > 0 ? lane_need(h, 0, split, h->cluster2) : 0;
+        require(h->res_smem2 <= h->res_max_dyn, XPLUS_ERR_ARG,
+                "a system of the split launch does not fit the resident kernel's shared memory at cluster " +
+                    std::to_string(h->cluster2) + " (" + std::to_string(h->res_smem2) + " bytes per CTA)");
+    }
+    if (split < h->nsys) {
+        const int num = active_clusters(h, h->cluster, h->tpb, h->resident ? h->res_smem : 0);
+        require(num > 0, XPLUS_ERR_CUDA, "cluster shape not launchable on this device");
+        h->grid = num * h->cluster;
+    } else {
+        h->grid = 0;
+    }
+    if (split > 0) {
+        const int num2 = active_clusters(h, h->cluster2, h->tpb2, h->resident ? h->res_smem2 : 0);
+        require(num2 > 0, XPLUS_ERR_CUDA, "split cluster shape not launchable on this device");
+        h->grid2 = std::min(num2, split) * h->cluster2;
+    } else {
+        h->grid2 = 0;
+    }
+}
+
+// Runs `change` on the handle's launch settings and plans them; restores the previous
+// settings when the new ones cannot launch.
+template <typename F>
+void replan(xplus_batch* h, F&& change) {
+    const bool res0 = h->resident;
+    const int c0 = h->cluster, t0 = h->tpb, s0 = h->split, c20 = h->cluster2, t20 = h->tpb2;
+    change();
+    try {
+        plan(h);
+    } catch (...) {
+        h->resident = res0;
+        h->cluster = c0;
+        h->tpb = t0;
+        h->split = s0;
+        h->cluster2 = c20;
+        h->tpb2 = t20;
+        try {
+            plan(h);
+        } catch (...) {
+        }
+        throw;
+    }
+}
+
 void set_split(xplus_batch* h, int count, int cluster, int tpb) {
     require(count >= 0 && count <= h->nsys, XPLUS_ERR_ARG, "split count must be in [0, nsys]");
     require(cluster == 4 || cluster == 8 || cluster == 16, XPLUS_ERR_ARG, "split cluster must be 4, 8 or 16");
     require(tpb == 128 || tpb == 256 || tpb == 512, XPLUS_ERR_ARG, "block_threads must be 128, 256 or 512");
-    if (count == 0) {
-        h->split = 0;
-        return;
-    }
-    const int num = active_clusters(h, cluster, tpb);
-    require(num > 0, XPLUS_ERR_CUDA, "split cluster shape not launchable on this device");
-    h->split = count;
-    h->cluster2 = cluster;
-    h->tpb2 = tpb;
-    h->grid2 = std::min(num, count) * cluster;
+    replan(h, [&] {
+        h->split = count;
+        if (count > 0) {
+            h->cluster2 = cluster;
+            h->tpb2 = tpb;
+        }
+    });
 }
 
 void set_launch(xplus_batch* h, int cluster, int tpb) {
     require(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8, XPLUS_ERR_ARG,
             "cluster must be 1, 2, 4 or 8");
     require(tpb == 128 || tpb == 256 || tpb == 512, XPLUS_ERR_ARG, "block_threads must be 128, 256 or 512");
-    const int num = active_clusters(h, cluster, tpb);
-    require(num > 0, XPLUS_ERR_CUDA, "cluster shape not launchable on this device");
-    h->cluster = cluster;
-    h->tpb = tpb;
-    h->grid = num * cluster;
+    replan(h, [&] {
+        h->cluster = cluster;
+        h->tpb = tpb;
+    });
+}
+
+// The resident kernel's records: [generation][{M r, M Ap', p'}][rows], allocated on first use.
+void ensure_rec3(xplus_batch* h) {
+    if (h->d_rec3) return;
+    void* p = nullptr;
+    const size_t bytes = 6 * sizeof(float) * static_cast<size_t>(h->rows);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(XPLUS_ERR_NOMEM, "cudaMalloc (resident records)");
+    }
+    h->allocations.push_back(p);
+    h->d_rec3 = static_cast<float*>(p);
+    bcheck(cudaMemset(h->d_rec3, 0, bytes), "memset");
+}
+
+void set_resident(xplus_batch* h, bool on) {
+    require(!on || h->res_kernel, XPLUS_ERR_ARG, "no resident batch kernel for these options");
+    if (on) ensure_rec3(h);
+    replan(h, [&] { h->resident = on; });
 }
 
 // f(k) for every system k, on the host's threads (system k on thread k mod T, which balances
@@ -731,6 +738,59 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
             if (cudaFuncSetAttribute(reinterpret_cast<const void*>(k), cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
                 cudaSuccess)
                 cudaGetLastError();  // then 16 is simply not launchable (active_clusters returns 0)
+        // the cluster-resident kernel: as much dynamic shared memory as a CTA may have
+        h->res_kernel = batch_resident_kernel(o.value_type, o.chunk, idx16);
+        if (h->res_kernel) {
+            int optin = 0;
+            const int st = batch_resident_static_smem(h->res_kernel);
+            const void* fk = reinterpret_cast<const void*>(h->res_kernel);
+            if (st < 0 || cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, o.device) != cudaSuccess ||
+                cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - st) != cudaSuccess) {
+                cudaGetLastError();
+                h->res_kernel = nullptr;
+            } else {
+                h->res_max_dyn = optin - st;
+                if (cudaFuncSetAttribute(fk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+                    cudaGetLastError();
+            }
+        }
+        // the resident kernel's shared memory per CTA for every system and cluster size of 1 to
+        // 16: the band split and the column window (every slot's column, padding included,
+        // widened to float4 groups) that the kernel itself computes
+        for (auto& v : h->need) v.assign(static_cast<size_t>(nsys), 0);
+        for_each_system(nsys, [&](int k) {
+            const SellHost& s = S[static_cast<size_t>(k)];
+            const int nsl_all = s.n_slices;
+            std::vector<int> smin(static_cast<size_t>(nsl_all)), smax(static_cast<size_t>(nsl_all));
+            for (int sl = 0; sl < nsl_all; ++sl) {
+                int lo = sl * 32, hi = sl * 32 + 32;
+                for (int64_t pos = s.slice_ptr[static_cast<size_t>(sl)]; pos < s.slice_ptr[static_cast<size_t>(sl) + 1]; ++pos) {
+                    lo = std::min(lo, s.col[static_cast<size_t>(pos)]);
+                    hi = std::max(hi, s.col[static_cast<size_t>(pos)] + 1);
+                }
+                smin[static_cast<size_t>(sl)] = lo;
+                smax[static_cast<size_t>(sl)] = hi;
+            }
+            for (int li = 0; li < 5; ++li) {
+                const int cs = 1 << li;
+                const int per = (nsl_all + cs - 1) / cs;
+                long long worst = 0;
+                for (int rk = 0; rk < cs; ++rk) {
+                    const int sb = std::min(nsl_all, rk * per), se = std::min(nsl_all, (rk + 1) * per);
+                    const int nsl = se - sb, r0 = sb * 32, nb = nsl * 32;
+                    int cmin = r0, cmax = r0 + nb;
+                    for (int sl = sb; sl < se; ++sl) {
+                        cmin = std::min(cmin, smin[static_cast<size_t>(sl)]);
+                        cmax = std::max(cmax, smax[static_cast<size_t>(sl)]);
+                    }
+                    const int w0 = std::max(0, cmin & ~3);
+                    const int wend = std::min(nsl_all * 32, (cmax + 3) & ~3);
+                    const long long need = ((nsl * 8LL + 15) & ~15LL) + 4LL * ((wend - w0) + 5LL * nb);
+                    worst = std::max(worst, need);
+                }
+                h->need[li][static_cast<size_t>(k)] = static_cast<int>(std::min<long long>(worst, 1LL << 30));
+            }
+        });
 
         // concatenated host image
         const size_t R = static_cast<size_t>(h->rows);
@@ -789,6 +849,7 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
             return wa > wb;
         });
 
+        h->order = order;
         bcheck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         bcheck(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking), "cudaStreamCreate");
         bcheck(cudaEventCreate(&h->ev0), "cudaEventCreate");
@@ -868,6 +929,8 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     a.rec = static_cast<NodeRec<float>*>(h->d_rec);
     a.r = h->d_r;
     a.ap = h->d_ap;
+    a.rec3 = h->d_rec3;
+    a.rows = h->rows;
     a.tau = tau;
     a.tau_mode = tau_mode;
     a.max_iters = max_iters;
@@ -886,6 +949,7 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(g);
         cfg.blockDim = dim3(t);
+        cfg.dynamicSmemBytes = h->resident ? static_cast<size_t>(args.res_smem) : 0;
         cfg.stream = s;
         cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -908,6 +972,7 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
         big.q_begin = 0;
         big.q_end = split;
         big.head = h->d_head + 1;
+        big.res_smem = h->res_smem2;
         bcheck(cudaEventRecord(h->ev_fork, st), "event");
         bcheck(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0), "wait");
         // the highest priority: when SMs free up, the CTA scheduler places this launch's
@@ -917,7 +982,8 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     }
     a.q_begin = split;
     a.q_end = h->nsys;
-    launch(a, cluster, tpb, grid, st, prio_low, "batch PCG launch");
+    a.res_smem = h->res_smem;
+    if (split < h->nsys) launch(a, cluster, tpb, grid, st, prio_low, "batch PCG launch");
     if (split > 0) bcheck(cudaStreamWaitEvent(st, h->ev_join, 0), "wait");
 }
 
@@ -1014,7 +1080,8 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
         const bool same = h->gexec && h->g_b == d_b && h->g_x == d_x && h->g_tau == tau && h->g_mode == tau_mode &&
                           h->g_iters == max_iters && h->g_cluster == h->cluster && h->g_tpb == h->tpb &&
-                          h->g_split == h->split && h->g_cluster2 == h->cluster2 && h->g_tpb2 == h->tpb2;
+                          h->g_split == h->split && h->g_cluster2 == h->cluster2 && h->g_tpb2 == h->tpb2 &&
+                          h->g_resident == h->resident;
         if (!same) {
             if (h->gexec) {
                 bcheck(cudaGraphExecDestroy(h->gexec), "graph destroy");
@@ -1045,6 +1112,7 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
             h->g_split = h->split;
             h->g_cluster2 = h->cluster2;
             h->g_tpb2 = h->tpb2;
+            h->g_resident = h->resident;
         }
         bcheck(cudaEventRecord(h->ev0, st), "event");
         bcheck(cudaGraphLaunch(h->gexec, st), "graph launch");
@@ -1061,8 +1129,13 @@ int xplus_batch_results(xplus_batch* h, int* status, int* iterations, int* repla
         bcheck(cudaSetDevice(h->device), "cudaSetDevice");
         collect(h);
         const size_t K = static_cast<size_t>(h->nsys);
+        std::vector<int> its(K);
+        bcheck(cudaMemcpy(its.data(), h->d_iters, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        for (size_t k = 0; k < K; ++k)
+            require(its[k] >= 0, XPLUS_ERR_CUDA,
+                    "system " + std::to_string(k) + " did not fit the resident launch's shared memory (not solved)");
         if (status) bcheck(cudaMemcpy(status, h->d_status, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
-        if (iterations) bcheck(cudaMemcpy(iterations, h->d_iters, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+        if (iterations) std::copy(its.begin(), its.end(), iterations);
         if (replacements) bcheck(cudaMemcpy(replacements, h->d_repl, K * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
         if (true_rel) bcheck(cudaMemcpy(true_rel, h->d_true_rel, K * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
         if (system_ms) {
@@ -1095,15 +1168,15 @@ int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, in
             bcheck(cudaStreamSynchronize(st), "sync");
             bcheck(cudaMemcpy(ones.data(), h->d_b64, ones.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
         }
-        // best of two launches of the current split with main shape (c, t)
-        auto time_shape = [&](int c, int t, int num) {
+        // best of two launches with the handle's current settings
+        auto time_current = [&]() {
             double ms_min = 1e300;
             for (int rep = 0; rep < 2; ++rep) {
                 bcheck(cudaMemcpyAsync(h->d_b64, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
                 bcheck(cudaMemsetAsync(h->d_x64, 0, ones.size() * sizeof(double), st), "memset");
                 bcheck(cudaEventRecord(h->ev0, st), "event");
-                if (fixed) enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, c, t, num * c, st);
-                else enqueue_kernel(h, tau, XPLUS_TAU_REL_TRUE, 0, c, t, num * c, st);
+                if (fixed) enqueue_kernel(h, 1e-300, XPLUS_TAU_ABS_RR, iters, h->cluster, h->tpb, h->grid, st);
+                else enqueue_kernel(h, tau, XPLUS_TAU_REL_TRUE, 0, h->cluster, h->tpb, h->grid, st);
                 bcheck(cudaEventRecord(h->ev1, st), "event");
                 bcheck(cudaEventSynchronize(h->ev1), "sync");
                 float ms = 0.0f;
@@ -1112,52 +1185,103 @@ int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, in
             }
             return ms_min;
         };
-        // stage 1: the main launch's shape, every system in it
-        const int split0 = h->split, c20 = h->cluster2, t20 = h->tpb2;
-        h->split = 0;
-        double best = 1e300;
-        int bc = h->cluster, bt = h->tpb;
-        const int clusters[4] = {1, 2, 4, 8};
-        const int threads[3] = {128, 256, 512};
-        for (int c : clusters)
-            for (int t : threads) {
-                const int num = active_clusters(h, c, t);
-                if (num <= 0) continue;
-                const double ms = time_shape(c, t, num);
-                if (ms < best) {
-                    best = ms;
-                    bc = c;
-                    bt = t;
-                }
+        struct Cfg {
+            bool res;
+            int c, t, k, c2, t2;
+        };
+        auto apply = [&](const Cfg& q) {
+            try {
+                replan(h, [&] {
+                    h->resident = q.res;
+                    h->cluster = q.c;
+                    h->tpb = q.t;
+                    h->split = q.k;
+                    if (q.k > 0) {
+                        h->cluster2 = q.c2;
+                        h->tpb2 = q.t2;
+                    }
+                });
+                return true;
+            } catch (const Error&) {
+                return false;  // not launchable, or a system does not fit: not a candidate
             }
+        };
+        double best = 1e300;
+        Cfg bestc{false, h->cluster, h->tpb, 0, h->cluster2, h->tpb2};
+        auto trial = [&](const Cfg& q) {
+            if (!apply(q)) return;
+            const double ms = time_current();
+            if (ms < best) {
+                best = ms;
+                bestc = q;
+            }
+        };
+        // stage 1: the global-memory kernel's main shape, every system in the main launch
+        for (int c : {1, 2, 4, 8})
+            for (int t : {128, 256, 512}) trial(Cfg{false, c, t, 0, 16, 512});
         require(best < 1e300, XPLUS_ERR_CUDA, "no launchable cluster shape");
-        set_launch(h, bc, bt);
-        // stage 2: the largest systems in a lane of their own with bigger clusters, beside the
-        // rest on that shape (the largest system otherwise sets the makespan on its own)
-        int bs = 0, bc2 = c20, bt2 = t20;
-        (void)split0;
+        // stage 2: on that shape, the largest systems in a lane of their own with bigger clusters
+        // (the largest system otherwise sets the makespan on its own)
         {
-            const int counts[5] = {1, 2, 4, 8, 16};
-            const int shapes2[3][2] = {{16, 512}, {8, 512}, {16, 256}};
-            for (int k : counts) {
+            const Cfg g = bestc;
+            for (int k : {1, 2, 4, 8, 16}) {
                 if (k > h->nsys / 4) break;
-                for (const auto& sh : shapes2) {
-                    if (active_clusters(h, sh[0], sh[1]) <= 0) continue;
-                    set_split(h, k, sh[0], sh[1]);
-                    const double ms = time_shape(h->cluster, h->tpb, h->grid / h->cluster);
-                    if (ms < best) {
-                        best = ms;
-                        bs = k;
-                        bc2 = sh[0];
-                        bt2 = sh[1];
+                for (const auto& sh : {std::make_pair(16, 512), std::make_pair(8, 512), std::make_pair(16, 256)})
+                    trial(Cfg{false, g.c, g.t, k, sh.first, sh.second});
+            }
+        }
+        // stage 3: the cluster-resident kernel.  Main launches of 2, 4 or 8 CTAs; the systems
+        // whose bands do not fit the main launch's shared-memory budget (all a CTA may have, or
+        // what lets two CTAs share an SM) go to a split launch of 16-CTA clusters, largest first
+        if (h->res_kernel) {
+            ensure_rec3(h);
+            int per_sm = 0;
+            bcheck(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device), "attribute");
+            const int st_bytes = batch_resident_static_smem(h->res_kernel);
+            const int half = per_sm / 2 - st_bytes - 1024;  // 1 KB per CTA is the system's
+            for (int c : {2, 4, 8}) {
+                // suffix maxima of the needs in queue order: the main launch takes [k, nsys)
+                const std::vector<int>& nd = h->need[log2_cluster(c)];
+                std::vector<int> suf(static_cast<size_t>(h->nsys) + 1, 0);
+                for (int q = h->nsys - 1; q >= 0; --q)
+                    suf[static_cast<size_t>(q)] = std::max(suf[static_cast<size_t>(q) + 1],
+                                                           nd[static_cast<size_t>(h->order[static_cast<size_t>(q)])]);
+                int last_k = -1;
+                for (int budget : {h->res_max_dyn, half}) {
+                    int k = 0;
+                    while (k < h->nsys && suf[static_cast<size_t>(k)] > budget) ++k;
+                    if (k == last_k || k >= h->nsys) continue;
+                    last_k = k;
+                    for (int t : {256, 512}) {
+                        if (k == 0) trial(Cfg{true, c, t, 0, 16, 512});
+                        else
+                            for (int t2 : {256, 512}) trial(Cfg{true, c, t, k, 16, t2});
                     }
                 }
             }
         }
-        set_split(h, bs, bc2, bt2);
+        require(apply(bestc), XPLUS_ERR_CUDA, "the autotuner's best shape no longer launches");
+        const int bc = bestc.c, bt = bestc.t;
         if (cluster) *cluster = bc;
         if (block_threads) *block_threads = bt;
         if (best_ms) *best_ms = best;
+    });
+}
+
+int xplus_batch_set_resident(xplus_batch* h, int on) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        set_resident(h, on != 0);
+    });
+}
+
+int xplus_batch_resident_info(xplus_batch* h, int* on, int* smem, int* smem_split) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        if (on) *on = h->resident ? 1 : 0;
+        if (smem) *smem = h->resident ? h->res_smem : 0;
+        if (smem_split) *smem_split = h->resident && h->split > 0 ? h->res_smem2 : 0;
     });
 }
 

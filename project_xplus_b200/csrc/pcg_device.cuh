@@ -197,13 +197,14 @@ __device__ __forceinline__ double warp_sum8_scatter(const double (&v)[8], int la
     return t;
 }
 
-// publish() for up to eight values at a fraction of the shuffles: warp sums by
-// warp_sum8_scatter, then warp q sums value q over the warps and writes its partial.  Every
-// call must be separated from the previous user of s_red by a __syncthreads (in the
-// persistent kernels a grid barrier always is).  Fixed combination order, as publish().
-template <int NV>
-__device__ __forceinline__ void publish_scatter(const double (&v)[NV], double* s_red, double* partial) {
-    static_assert(NV <= 8, "publish_scatter sums at most eight values");
+// Block sums of up to eight values at a fraction of block_sum's shuffles: warp sums by
+// warp_sum8_scatter, then warp q sums value q over the warps and lane 0 of warp q calls
+// store(q, total).  Every call must be separated from the previous user of s_red by a
+// __syncthreads (in the persistent kernels a grid or cluster barrier always is).  Fixed
+// combination order.
+template <int NV, typename Store>
+__device__ __forceinline__ void block_sum_scatter(const double (&v)[NV], double* s_red, Store&& store) {
+    static_assert(NV <= 8, "block_sum_scatter sums at most eight values");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double v8[8];
 #pragma unroll
@@ -214,8 +215,16 @@ __device__ __forceinline__ void publish_scatter(const double (&v)[NV], double* s
     __syncthreads();
     if (warp < NV) {
         const double x = warp_sum(lane < nwarps ? s_red[warp * 32 + lane] : 0.0);
-        if (lane == 0) partial[static_cast<size_t>(warp) * gridDim.x + blockIdx.x] = x;
+        if (lane == 0) store(warp, x);
     }
+}
+
+// publish() for up to eight values through block_sum_scatter.
+template <int NV>
+__device__ __forceinline__ void publish_scatter(const double (&v)[NV], double* s_red, double* partial) {
+    block_sum_scatter<NV>(v, s_red, [&](int q, double x) {
+        partial[static_cast<size_t>(q) * gridDim.x + blockIdx.x] = x;
+    });
 }
 
 inline __device__ bool bad(double v) { return v != v; }
@@ -304,6 +313,47 @@ __device__ __forceinline__ void sell_rows_pnew(const int2 (&sl)[NS], const int (
     }
 }
 
+
+// NS slices of one warp: all value/column loads of the group first (the only global traffic),
+// then the products with p' gathered from the shared-memory window.  y_k excludes s_i p'_i.
+template <typename VT, int CHUNK, typename IT, int NS>
+__device__ __forceinline__ void sell_rows_smem(const int2 (&sl)[NS], const int (&row)[NS], int lane,
+                                               const IT* __restrict__ col, const VT* __restrict__ val,
+                                               const float* pw, int w0, const float (&pi)[NS],
+                                               float (&y)[NS]) {
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        y[k] = 0.0f;
+        wmax = max(wmax, sl[k].y);
+    }
+    for (int c = 0; c < wmax; c += 2 * CHUNK) {
+        float v[NS][2][CHUNK];
+        int cc[NS][2][CHUNK];
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (c + h * CHUNK < sl[k].y) {
+                    const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
+                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
+                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < CHUNK; ++q) {
+                        v[k][h][q] = 0.0f;
+                        cc[k][h][q] = row[k] >= 0 ? row[k] : w0;
+                    }
+                }
+            }
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q) y[k] += v[k][h][q] * (pw[cc[k][h][q] - w0] - pi[k]);
+    }
+}
 
 }  // namespace dev
 }  // namespace xplus

@@ -31,47 +31,6 @@ using namespace dev;
 constexpr int kResSlices = 1024;  // slice table capacity per CTA
 constexpr int kResNS = 4;         // slices of one warp in flight together in phase A
 
-// NS slices of one warp: all value/column loads of the group first (the only global traffic),
-// then the products with p' gathered from the shared-memory window.  y_k excludes s_i p'_i.
-template <typename VT, int CHUNK, typename IT, int NS>
-__device__ __forceinline__ void sell_rows_smem(const int2 (&sl)[NS], const int (&row)[NS], int lane,
-                                               const IT* __restrict__ col, const VT* __restrict__ val,
-                                               const float* pw, int w0, const float (&pi)[NS],
-                                               float (&y)[NS]) {
-    int wmax = 0;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-        y[k] = 0.0f;
-        wmax = max(wmax, sl[k].y);
-    }
-    for (int c = 0; c < wmax; c += 2 * CHUNK) {
-        float v[NS][2][CHUNK];
-        int cc[NS][2][CHUNK];
-#pragma unroll
-        for (int k = 0; k < NS; ++k)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (c + h * CHUNK < sl[k].y) {
-                    const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
-                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
-                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < CHUNK; ++q) {
-                        v[k][h][q] = 0.0f;
-                        cc[k][h][q] = row[k] >= 0 ? row[k] : w0;
-                    }
-                }
-            }
-#pragma unroll
-        for (int k = 0; k < NS; ++k)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int q = 0; q < CHUNK; ++q) y[k] += v[k][h][q] * (pw[cc[k][h][q] - w0] - pi[k]);
-    }
-}
-
 template <typename VT, int CHUNK, typename IT>
 __global__ void __launch_bounds__(512, 1) pcg_resident_kernel(PcgArgs a) {
     constexpr int NS = kResNS;

@@ -164,6 +164,77 @@ def test_lane_of_the_largest_systems(gpu, batch_systems, count, cluster, tpb):
     s.close()
 
 
+@pytest.mark.parametrize("vt", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("cluster,tpb,split", [(1, 512, 0), (2, 256, 0), (4, 256, 2), (8, 512, 0)])
+def test_resident_kernel(gpu, batch_systems, vt, cluster, tpb, split):
+    """The cluster-resident kernel (vectors and the search direction's window in shared
+    memory, one cluster barrier per iteration): every system reaches the tolerance, its
+    iteration count stays within the dot-product rounding of the global-memory kernel's, the
+    two solutions are equally close to the direct solve (two solutions at residual 1e-8 may
+    differ by up to cond(A) x 1e-8), repeated solves are bit-identical, and the graph-captured
+    device path gives the host path's x bit for bit."""
+    import torch
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.linalg import spsolve
+    s = _make(batch_systems, values_dtype=vt)
+    b = _b(batch_systems)
+    s.set_launch(cluster, tpb)
+    if split:
+        s.set_split_lane(split, 16, 256)
+    ref = s.solve(b, tau=1e-8)
+    s.set_resident(True)
+    info = s.resident()
+    assert info["on"] and 0 < info["smem"] <= 232448 and (info["smem_split"] > 0) == bool(split)
+    r = s.solve(b, tau=1e-8)
+    assert list(r["status"]) == [0] * len(SPECS), r["status_names"]
+    assert np.all(r["true_rel"] <= 1e-8)
+    for k, ((d, _), x, x_ref) in enumerate(zip(batch_systems, s.split(r["x"]), s.split(ref["x"]))):
+        it, it_ref = int(r["iterations"][k]), int(ref["iterations"][k])
+        assert abs(it - it_ref) <= max(4, 0.06 * it_ref), (k, it, it_ref)
+        assert np.linalg.norm(d.b - _spmv(d, x)) / np.linalg.norm(d.b) <= 1.5e-8
+        x64 = spsolve(csr_matrix((d.values, d.col_idx, d.row_ptr), shape=(d.n, d.n)).tocsc(), d.b)
+        err, err_ref = (np.linalg.norm(v - x64) / np.linalg.norm(x64) for v in (x, x_ref))
+        assert err <= 10 * max(err_ref, 1e-7), (k, err, err_ref)
+    again = s.solve(b, tau=1e-8)
+    np.testing.assert_array_equal(again["x"], r["x"])
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros_like(d_b)
+    st = torch.cuda.Stream()
+    for _ in range(2):
+        d_x.zero_()
+        torch.cuda.synchronize()
+        s.solve_device(d_b, d_x, tau=1e-8, stream=st)
+        st.synchronize()
+        np.testing.assert_array_equal(d_x.cpu().numpy(), r["x"])
+    s.set_resident(False)
+    assert not s.resident()["on"]
+    np.testing.assert_array_equal(s.solve(b, tau=1e-8)["x"], ref["x"])
+    s.close()
+
+
+def test_resident_kernel_refuses_systems_that_do_not_fit(gpu):
+    """A 128x128 system's band does not fit one CTA's shared memory at cluster size 1: the
+    resident kernel is refused with XPLUS_ERR_ARG before any launch and the handle keeps its
+    kernel; at clusters of 4 it fits and solves."""
+    from project_xplus_b200 import XplusError
+    from project_xplus_b200.batch import BatchSolver
+    sys2 = _systems([(128, 1.0, 8), (20, 1.0, 9)])
+    s = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d, _ in sys2])
+    s.set_launch(1, 512)
+    with pytest.raises(XplusError) as e:
+        s.set_resident(True)
+    assert e.value.code == 10 and "does not fit" in str(e.value)
+    assert not s.resident()["on"]
+    s.set_launch(4, 256)
+    s.set_resident(True)
+    r = s.solve(np.concatenate([d.b for d, _ in sys2]), tau=1e-8)
+    assert list(r["status"]) == [0, 0] and np.all(r["true_rel"] <= 1e-8)
+    with pytest.raises(XplusError):
+        s.set_launch(1, 512)  # refused: the 128x128 band no longer fits
+    assert s.info()["cluster"] == 4 and s.resident()["on"]
+    s.close()
+
+
 def test_launch_shapes_and_autotune(gpu, batch_systems):
     from project_xplus_b200 import XplusError
     from project_xplus_b200.batch import autotune_build

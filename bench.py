@@ -252,9 +252,16 @@ def run_b200(args):
     t_setup = time.perf_counter()
     xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=4, device=local).close()
     setup_first_ms = (time.perf_counter() - t_setup) * 1e3
-    t_setup = time.perf_counter()
-    solver = xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=4, device=local)
-    setup_ms = (time.perf_counter() - t_setup) * 1e3  # checks, SELL build and every device array, on the GPU
+    # checks, SELL build and every device array, on the GPU: three creates, the fastest reported
+    # (one create has read far above the others in a process now and then; all three are listed)
+    setup_warm = []
+    for k in range(3):
+        t_setup = time.perf_counter()
+        solver = xp.PcgSolver.from_dataset(d, values_dtype="f32", vector_dtype="f32", chunk=4, device=local)
+        setup_warm.append((time.perf_counter() - t_setup) * 1e3)
+        if k < 2:
+            solver.close()
+    setup_ms = min(setup_warm)
     info = solver.info()
     # a real (non-default) stream: the library enqueues on exactly the stream the events see
     stream = torch.cuda.Stream(dev)
@@ -471,7 +478,7 @@ def run_b200(args):
                 s3.set_gnn(params)  # inference, one refinement sweep, rows normalized: on the GPU
             else:
                 s3.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))
-            setup_ms = (time.perf_counter() - t0) * 1e3
+            pre_ms = (time.perf_counter() - t0) * 1e3  # preconditioner set-up on this handle
             runs = []
             for _ in range(2):
                 flush.fill_(1.0)
@@ -479,8 +486,8 @@ def run_b200(args):
                 runs.append(s3.solve(d.b, None, tau=args.tol, tau_mode=_lib.XPLUS_TAU_REL_TRUE, max_iters=40000))
             r3 = runs[-1]
             compare[name] = {"time_to_tol_ms": r3.kernel_ms, "iterations": r3.iterations, "status": r3.status,
-                             "true_rel_residual": r3.residual_rel, "setup_ms": setup_ms,
-                             "time_to_tol_incl_setup_ms": r3.kernel_ms + setup_ms,
+                             "true_rel_residual": r3.residual_rel, "setup_ms": pre_ms,
+                             "time_to_tol_incl_setup_ms": r3.kernel_ms + pre_ms,
                              "jacobi_fallback_at": r3.metrics["jacobi_fallback_at"]}
             s3.close()
         compare["speedup_vs_plain_fp32"] = compare["plain_fp32"]["time_to_tol_ms"] / kern_mean
@@ -496,12 +503,14 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         per_it, setup, kind = cpu_reference_sample(d, args.cpu_sample_iters)
-        ref_iters = fp64_iters or it_mean
+        # the golden's own iteration count on this system (one full run, recorded beside
+        # GOLDEN_ITERATIONS_1108), else the FP64 GPU solve's as a stand-in
+        ref_iters = GOLDEN_ITERATIONS_1108 if args.grid == 1108 else (fp64_iters or it_mean)
         t_cpu = per_it * ref_iters + setup
         cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": kind,
                "sample": f"{args.cpu_sample_iters} iterations of the reference run_jacobi_pcg (FP64, 1 thread) on "
-                         f"the full system, extrapolated to {ref_iters:.0f} iterations (the FP64 CG iteration "
-                         f"count to 1e-8); {per_it * 1e3:.1f} ms/iteration"}
+                         f"the full system, extrapolated to {ref_iters:.0f} iterations (the golden's own "
+                         f"iteration count to 1e-8 on this system); {per_it * 1e3:.1f} ms/iteration"}
 
     config0 = run_config0(args, local) if rank == 0 and not args.no_config0 else None
 
@@ -519,7 +528,7 @@ def run_b200(args):
             "config": workload_config(args, {"nnz": nnz}),
             "time_to_tol_ms": ms_per_step,
             "setup_ms": setup_ms, "time_to_tol_incl_setup_ms": ms_per_step + setup_ms,
-            "first_call_ms": first_call_ms, "setup_first_ms": setup_first_ms,
+            "first_call_ms": first_call_ms, "setup_first_ms": setup_first_ms, "setup_warm_ms_all": setup_warm,
             "iterations": it_mean, "replacements": rp_mean, "true_rel_residual": max(relres),
             "spmv": {"cold_gbs": spmv_cold_gbs, "warm_gbs": spmv_warm_gbs, "cold_ms": cold_ms, "warm_ms": warm_ms,
                      "bytes": spmv_bytes, "frac_cold": spmv_cold_gbs / hbm, "peak_kind": hbm_kind,

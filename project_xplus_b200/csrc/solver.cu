@@ -74,6 +74,7 @@ struct xplus_pcg {
     std::vector<void*> allocations;
     std::vector<int> perm;     // SELL row -> original row
     bool l2_user = false;      // holds a persisting-L2 request (l2_want bytes) in g_l2_wants
+    size_t mat_bytes = 0;      // matrix columns + values (one allocation at d_col)
     size_t l2_want = 0;
     // M^-1 = G^T G: G on A's lower pattern (original order), SELL images of G and G^T in the
     // matrix's SELL order, and the map from each SELL slot to its entry of g_low
@@ -261,36 +262,45 @@ void destroy(xplus_pcg* h) {
 
 // Columns and values in one allocation, so one L2 access-policy window covers both.
 unsigned char* alloc_matrix(xplus_pcg* h, const xplus_opts& o, size_t col_bytes, size_t val_bytes) {
+    (void)o;
     unsigned char* mat = dalloc<unsigned char>(h, col_bytes + val_bytes);
     h->d_col = mat;
     h->d_val = mat + col_bytes;
-    if (o.l2_persist) {
-        int max_window = 0;
-        cudaDeviceProp prop;
-        cuda_check(cudaGetDeviceProperties(&prop, o.device), "props");
-        cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, o.device), "attr");
-        const size_t bytes = std::min(col_bytes + val_bytes, static_cast<size_t>(max_window));
-        size_t limit = 0;
-        const size_t want = std::min(bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
-        {
-            std::lock_guard<std::mutex> lk(g_l2_mutex);
-            cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
-            if (g_l2_wants.empty()) g_l2_limit_before = limit;
-            if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
-            g_l2_wants.insert(want);
-            h->l2_want = want;
-            h->l2_user = true;
-        }
-        cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
-        if (bytes > 0 && limit > 0) {
-            h->window.base_ptr = mat;
-            h->window.num_bytes = bytes;
-            h->window.hitRatio = std::min(1.0f, static_cast<float>(limit) / static_cast<float>(bytes));
-            h->window.hitProp = cudaAccessPropertyPersisting;
-            h->window.missProp = cudaAccessPropertyStreaming;
-        }
-    }
+    h->mat_bytes = col_bytes + val_bytes;
     return mat;
+}
+
+// The persisting-L2 set-aside and access-policy window over the matrix, for the kernels whose
+// working set can exceed L2 (the global-memory and the G^T G kernel); requested once per
+// handle when such a kernel is first chosen.  The SM-resident kernel does without: its matrix
+// stays in L2 anyway, and changing the device's persisting limit at create and destroy took
+// from 30 ms up to 2.7 s per call on a shared B200 (1108^2 system, creates without it: 28-29 ms).
+void request_l2(xplus_pcg* h) {
+    if (h->l2_user || !h->opts.l2_persist || h->mat_bytes == 0) return;
+    int max_window = 0;
+    cudaDeviceProp prop;
+    cuda_check(cudaGetDeviceProperties(&prop, h->device), "props");
+    cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, h->device), "attr");
+    const size_t bytes = std::min(h->mat_bytes, static_cast<size_t>(max_window));
+    size_t limit = 0;
+    const size_t want = std::min(bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
+    {
+        std::lock_guard<std::mutex> lk(g_l2_mutex);
+        cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+        if (g_l2_wants.empty()) g_l2_limit_before = limit;
+        if (limit < want) cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "set L2 limit");
+        g_l2_wants.insert(want);
+        h->l2_want = want;
+        h->l2_user = true;
+    }
+    cuda_check(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "limit");
+    if (bytes > 0 && limit > 0) {
+        h->window.base_ptr = h->d_col;
+        h->window.num_bytes = bytes;
+        h->window.hitRatio = std::min(1.0f, static_cast<float>(limit) / static_cast<float>(bytes));
+        h->window.hitProp = cudaAccessPropertyPersisting;
+        h->window.missProp = cudaAccessPropertyStreaming;
+    }
 }
 
 // Device temporaries of one create call, freed when it returns.
@@ -601,8 +611,10 @@ void create(const int* row_ptr, const int* col_idx, const double* values, int n,
                 }
             }
         }
-        if (!h->resident)
+        if (!h->resident) {
             cuda_check(pcg_grid(h->key, o.device, h->n_slices, want_tpb, o.blocks_per_sm, &h->grid, &h->tpb), "pcg_grid");
+            request_l2(h);
+        }
         h->d_partial = dalloc<double>(h, static_cast<size_t>(16) * h->grid);
         h->d_block_clk = dalloc<long long>(h, static_cast<size_t>(4) * h->grid);
         cuda_check(cudaMemsetAsync(h->d_x64, 0, np * sizeof(double), st), "memset");
@@ -690,7 +702,11 @@ void enqueue_solve(xplus_pcg* h, double tau, int tau_mode, int max_iters_in, int
         a.g_fallback_iters = h->g_fallback_iters;
         cuda_check(gtg_launch(h->key, a, h->gtg_grid, 512, st, h->window), "GTG PCG launch");
     } else if (h->resident)
-        cuda_check(resident_launch(h->key, a, h->grid, h->tpb, h->smem_bytes, h->one_sync, st, h->window),
+        // no access-policy window: the resident kernel's only global stream is a matrix that L2
+        // holds anyway, and the launch attribute cost time (1108^2 system: 97.1 ms with it,
+        // 95.9 ms without, and ~3 ms more on the host per solve call)
+        cuda_check(resident_launch(h->key, a, h->grid, h->tpb, h->smem_bytes, h->one_sync, st,
+                                   cudaAccessPolicyWindow{}),
                    "resident PCG launch");
     else
         cuda_check(pcg_launch(h->key, a, h->grid, h->tpb, st, h->window), "persistent PCG launch");
@@ -856,6 +872,7 @@ void gtg_enable(xplus_pcg* h, int fallback_iters) {
     cuda_check(cudaStreamSynchronize(st), "sync");
     h->g_fallback_iters = fallback_iters;
     h->gtg = true;
+    request_l2(h);
 }
 
 }  // namespace

@@ -4,7 +4,7 @@ then a few standalone SELL SpMV launches.  Every kernel here is a product kernel
 
   python -m project_xplus_b200.profile_case --grid 1108 --iters 100 --spmv 5
   python -m project_xplus_b200.profile_case --grid 1108 --iters 50 --spmv 0 --gtg fsai
-  python -m project_xplus_b200.profile_case --batch 64 --iters 200
+  python -m project_xplus_b200.profile_case --batch 64 --iters 200 [--resident]
 """
 from __future__ import annotations
 
@@ -18,15 +18,20 @@ from . import generators as g
 from .solver import PcgSolver
 
 
-def batch_case(count: int, iters: int) -> None:
-    """`count` systems of the batched workload's distribution, clusters of 8 x 512 threads,
-    at most `iters` iterations per system, two launches."""
+def batch_case(count: int, iters: int, resident: bool) -> None:
+    """`count` systems of the batched workload's distribution, clusters of 8 x 512 threads
+    (8 x 256 for the cluster-resident kernel), at most `iters` iterations per system, two
+    launches."""
     from .batch import BatchSolver
     sides, sigmas = g.batch_sides(count, 45, 256, seed=3)
     systems = [g.fem2d(int(sd), sigma=float(sg), seed=1000 + k, x_seed=1000 + k)[0]
                for k, (sd, sg) in enumerate(zip(sides, sigmas))]
     s = BatchSolver([(d.row_ptr, d.col_idx, d.values) for d in systems])
-    s.set_launch(8, 512)
+    if resident:
+        s.set_launch(8, 256)
+        s.set_resident(True)
+    else:
+        s.set_launch(8, 512)
     b = np.concatenate([d.b for d in systems])
     for _ in range(2):
         r = s.solve(b, tau=1e-8, max_iters=iters)
@@ -48,9 +53,10 @@ def main() -> None:
                     help="plain layout: values with the diagonal, int32 columns (no row-sum form)")
     ap.add_argument("--gtg", choices=["fsai", "learned"], help="solve with M^-1 = G^T G (FSAI or learned G)")
     ap.add_argument("--batch", type=int, default=0, help="run the batched solver on this many systems instead")
+    ap.add_argument("--resident", action="store_true", help="batched solver: the cluster-resident kernel")
     a = ap.parse_args()
     if a.batch:
-        batch_case(a.batch, a.iters)
+        batch_case(a.batch, a.iters, a.resident)
         return
     d, _ = g.system_3d(a.dim3) if a.dim3 else g.system_2d_large(a.grid)
     extra = dict(row_sum_form=False, index16=False) if a.plain else {}

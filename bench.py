@@ -178,6 +178,34 @@ def barrier(pg, device=None):
 # --------------------------------------------------------------------------------------
 # reference arm: the reference's own CPU code (oracle/_ref, built from its sources)
 # --------------------------------------------------------------------------------------
+def cpu_model():
+    """The host CPU's model name (for the CPU baselines' tables)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cuper_reference_sample(d, iters):
+    """Times the reference's own FP32-SpMV software PCG (run_cuper_pcg_solver,
+    host/cuper_pcg_solver.hpp:311, oracle/_ref) on this host, one thread: `iters` and
+    iters / 4 iterations, the per-iteration cost as the slope.  Returns (seconds per iteration,
+    plan build in ms) or None without the reference build."""
+    from oracle import oracle as O
+    if O.reflib() is None:
+        return None
+    t0 = time.perf_counter()
+    r = O.cuper_pcg_ref(d, 1e-300, iters)
+    dt = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    O.cuper_pcg_ref(d, 1e-300, max(1, iters // 4))
+    dt2 = time.perf_counter() - t1
+    return (dt - dt2) / (iters - max(1, iters // 4)), r["plan_ms"]
+
+
 def cpu_reference_sample(d, iters):
     """Times `iters` iterations of the reference's run_jacobi_pcg on this host (1 thread: the
     reference has no threading).  Returns (seconds per iteration, kind, label)."""
@@ -215,8 +243,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args, {"solver": "reference run_jacobi_pcg (FP64 CSR, 1 thread)"}),
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": kind,
+            "config": workload_config(args), "solver": "reference run_jacobi_pcg (FP64 CSR, 1 thread)",
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": kind, "cpu_model": cpu_model(),
                              "sample": f"{args.cpu_sample_iters} iterations of run_jacobi_pcg per step on the full "
                                        f"system, extrapolated to {iters_needed} iterations"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -421,6 +449,16 @@ def run_b200(args):
                               "stagnated": r3.metrics["stagnated"], "kernel": r3.metrics["kernel"],
                               "slots": s3.info()["slots"]}
             s3.close()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            # the reference's golden on this system, sampled on one core and extrapolated to the
+            # FP64 GPU solve's iteration count (the golden's own count here was not measured)
+            per_it3, setup3, kind3 = cpu_reference_sample(d3, 10)
+            it3 = mixed_3d["fp64"]["iterations"]
+            mixed_3d["cpu_reference"] = {
+                "value_ms": (per_it3 * it3 + setup3) * 1e3, "cores": 1, "kind": kind3, "cpu_model": cpu_model(),
+                "sample": f"10 iterations of run_jacobi_pcg (FP64, 1 thread) on the full system, "
+                          f"{per_it3 * 1e3:.1f} ms/iteration, extrapolated to {it3} iterations (the FP64 GPU "
+                          f"solve's count to 1e-10)"}
     if not args.no_spmv3d:
         del d3
 
@@ -523,7 +561,12 @@ def run_b200(args):
         # GOLDEN_ITERATIONS_1108), else the FP64 GPU solve's as a stand-in
         ref_iters = GOLDEN_ITERATIONS_1108 if args.grid == 1108 else (fp64_iters or it_mean)
         t_cpu = per_it * ref_iters + setup
-        cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": kind,
+        cup = cuper_reference_sample(d, 8)
+        cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": kind, "cpu_model": cpu_model(),
+               "cuper_pcg": None if cup is None else {
+                   "ms_per_iteration": cup[0] * 1e3, "plan_ms": cup[1],
+                   "note": "the reference's FP32-SpMV software PCG (run_cuper_pcg_solver), 8- and 2-iteration "
+                           "samples on one core; per iteration only (its iteration count to 1e-8 not measured)"},
                "sample": f"{args.cpu_sample_iters} iterations of the reference run_jacobi_pcg (FP64, 1 thread) on "
                          f"the full system, extrapolated to {ref_iters:.0f} iterations (the golden's own "
                          f"iteration count to 1e-8 on this system); {per_it * 1e3:.1f} ms/iteration"}
@@ -659,7 +702,7 @@ def run_config0(args, device):
         out["cpu_reference"] = {"multi_kernel": {"solves_per_s": 1.0 / dt, "ms_per_solve": dt * 1e3, "iterations": it,
                                                  "max_abs_diff_vs_golden": float(np.abs(xo - gold["x"]).max())},
                                 "golden": {"solves_per_s": 1.0 / dt_g, "ms_per_solve": dt_g * 1e3},
-                                "cores": 1, "kind": "reference"}
+                                "cores": 1, "kind": "reference", "cpu_model": cpu_model()}
     return out
 
 
@@ -693,6 +736,7 @@ def batch_cpu_baseline(systems, works, tol, sample=24):
     total_cpu_s = per_work * sum(works)
     est_wall = total_cpu_s / cores
     return {"value": len(systems) / est_wall, "unit": "systems/s", "cores": cores, "kind": "reference",
+            "cpu_model": cpu_model(),
             "sample": f"{len(pick)} of {len(systems)} systems (spread over the work range) solved by the reference "
                       f"run_jacobi_pcg, one process per core; total CPU time {total_cpu_s:.1f} s extrapolated by "
                       f"nnz*sqrt(n), divided over {cores} cores (sample wall {wall:.1f} s)"}

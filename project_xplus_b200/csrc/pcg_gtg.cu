@@ -53,35 +53,44 @@ __device__ __forceinline__ void g_rows(const int2* __restrict__ st, int s_first,
         w[k] = e.y;
         wmax = max(wmax, w[k]);
     }
-    for (int c = 0; c < wmax; c += kGChunk) {
-        float2 v[NB];
-        int2 cc[NB];
+    // two chunk steps per pass: every slot load of both steps before any gather, so a row of
+    // up to 2 * kGChunk entries costs one load-then-gather round trip instead of two (the
+    // products still add in slot order, as one step at a time would)
+    for (int c = 0; c < wmax; c += 2 * kGChunk) {
+        float2 v[NB][2];
+        int2 cc[NB][2];
 #pragma unroll
-        for (int k = 0; k < NB; ++k) {
-            if (c < w[k]) {
-                const int off = base[k] + c * 32 + lane * kGChunk;
-                v[k] = __ldg(reinterpret_cast<const float2*>(val + off));
-                cc[k] = __ldg(reinterpret_cast<const int2*>(col + off));
-            } else {
-                v[k] = make_float2(0.0f, 0.0f);
-                cc[k] = make_int2(-1, -1);
+        for (int k = 0; k < NB; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (c + h * kGChunk < w[k]) {
+                    const int off = base[k] + (c + h * kGChunk) * 32 + lane * kGChunk;
+                    v[k][h] = __ldg(reinterpret_cast<const float2*>(val + off));
+                    cc[k][h] = __ldg(reinterpret_cast<const int2*>(col + off));
+                } else {
+                    v[k][h] = make_float2(0.0f, 0.0f);
+                    cc[k][h] = make_int2(-1, -1);
+                }
             }
-        }
-        float x0[NB], x1[NB];
+        float x0[NB][2], x1[NB][2];
 #pragma unroll
-        for (int k = 0; k < NB; ++k) {
-            x0[k] = cc[k].x >= 0 ? x[cc[k].x] : 0.0f;
-            x1[k] = cc[k].y >= 0 ? x[cc[k].y] : 0.0f;
-            if (RECOMP) {
-                if (cc[k].x >= 0) x0[k] = __fmaf_rn(nal, ap[cc[k].x], x0[k]);
-                if (cc[k].y >= 0) x1[k] = __fmaf_rn(nal, ap[cc[k].y], x1[k]);
+        for (int k = 0; k < NB; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                x0[k][h] = cc[k][h].x >= 0 ? x[cc[k][h].x] : 0.0f;
+                x1[k][h] = cc[k][h].y >= 0 ? x[cc[k][h].y] : 0.0f;
+                if (RECOMP) {
+                    if (cc[k][h].x >= 0) x0[k][h] = __fmaf_rn(nal, ap[cc[k][h].x], x0[k][h]);
+                    if (cc[k][h].y >= 0) x1[k][h] = __fmaf_rn(nal, ap[cc[k][h].y], x1[k][h]);
+                }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < NB; ++k) {
-            out[k] = fmaf(v[k].x, x0[k], out[k]);
-            out[k] = fmaf(v[k].y, x1[k], out[k]);
-        }
+        for (int k = 0; k < NB; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                out[k] = fmaf(v[k][h].x, x0[k][h], out[k]);
+                out[k] = fmaf(v[k][h].y, x1[k][h], out[k]);
+            }
     }
 }
 

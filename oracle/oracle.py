@@ -22,20 +22,16 @@ RELINKED_HOST = HERE / "_ref" / "xplus_host_b200"
 REFERENCE_HOST = HERE / "_ref" / "xplus_host_ref"
 
 
-# Where the reference checkout lies in the build container; XPLUS_REFERENCE_TREE overrides it.
-# Only this build step reads the tree: tests and benchmarks load the prebuilt _ref library.
-_REFERENCE_CHECKOUT = "/root/reference"
-
-
 def reference_tree() -> Path | None:
-    """The reference tree to compile from: $XPLUS_REFERENCE_TREE when set (it must then hold
-    the reference's src/), else the build container's checkout when present, else None."""
+    """The reference tree to compile from: $XPLUS_REFERENCE_TREE (it must hold the reference's
+    src/), or None when the variable is unset (then no _ref build).  Only the build step reads
+    the tree: tests and benchmarks load the prebuilt _ref library."""
     env = os.environ.get("XPLUS_REFERENCE_TREE")
-    if env:
-        if not (Path(env) / "src").is_dir():
-            raise FileNotFoundError(f"XPLUS_REFERENCE_TREE={env} does not hold the reference's src/")
-        return Path(env)
-    return Path(_REFERENCE_CHECKOUT) if (Path(_REFERENCE_CHECKOUT) / "src").is_dir() else None
+    if not env:
+        return None
+    if not (Path(env) / "src").is_dir():
+        raise FileNotFoundError(f"XPLUS_REFERENCE_TREE={env} does not hold the reference's src/")
+    return Path(env)
 
 
 def build(ref: bool = True) -> None:

@@ -252,6 +252,11 @@ struct GridBarrier {
     int skip_block;  // test-only: this block withholds its arrival at the first barrier (-1: none)
 
     __device__ __forceinline__ bool sync(int* s_flag) {
+        if (gridDim.x == 1 && skip_block < 0) {
+            // one CTA: the CTA barrier orders its global-memory accesses as well
+            __syncthreads();
+            return true;
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             ++epoch;

@@ -786,6 +786,24 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
     if not np.all(r["status"] == 0):
         raise SystemExit(f"batch: {int((r['status'] != 0).sum())} systems did not converge")
     tot = max_over_ranks(pg, sum(ms), dev)
+    staged = s.staged()
+    # the same launch shape with every band's matrix read from global memory (one step; the
+    # same x bit for bit)
+    unstaged_ms = None
+    if info["resident"]["on"]:
+        s.set_stage_matrix(False)
+        x.zero_()
+        s.solve_device(b, x, tau=args.tol, stream=stream)
+        stream.synchronize()
+        flush.fill_(1.0)
+        x.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.solve_device(b, x, tau=args.tol, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        unstaged_ms = max_over_ranks(pg, e0.elapsed_time(e1), dev)
     s.close()
     # the same batch with BF16 values (the other value type of the batched workload), with its
     # own tuned kernel and launch shapes
@@ -814,6 +832,7 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
     clk.__exit__(None, None, None)
     r16 = s16.results()
     tot16 = max_over_ranks(pg, sum(ms16), dev)
+    staged16 = s16.staged()
     s16.close()
     bf16 = {"value": len(sides) * args.steps / (tot16 / 1e3), "unit": "systems/s", "ms_per_step": tot16 / args.steps,
             "converged": int((r16["status"] == 0).sum()), "iterations_total": int(r16["iterations"].sum()),
@@ -821,7 +840,8 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
             "system_ms_max": float(r16["system_ms"].max()),
             "launch": {"cluster": info16["cluster"], "block_threads": info16["block_threads"],
                        "grid": info16["grid"], "autotune_ms": tune16["ms"],
-                       "largest_systems_lane": info16["split_lane"], "resident": info16["resident"]}}
+                       "largest_systems_lane": info16["split_lane"], "resident": info16["resident"],
+                       "matrix_staged_systems": staged16["all"], "matrix_staged_partly": staged16["some"]}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = batch_cpu_baseline(systems, [works[k] for k in mine], args.tol)
@@ -834,7 +854,8 @@ def run_batch(args, world, rank, pg, dev, stream, flush):
                           "sum": float(r["system_ms"].sum())},
             "launch": {"cluster": info["cluster"], "block_threads": info["block_threads"], "grid": info["grid"],
                        "autotune_ms": tune["ms"], "largest_systems_lane": info["split_lane"],
-                       "resident": info["resident"]},
+                       "resident": info["resident"], "matrix_staged_systems": staged["all"],
+                       "matrix_staged_partly": staged["some"], "ms_matrix_not_staged": unstaged_ms},
             "graph": True, "bf16_values": bf16}
 
 

@@ -375,6 +375,17 @@ int xplus_batch_set_resident(xplus_batch* h, int on);
 /* Whether the resident kernel is on, and the dynamic shared memory (bytes per CTA) of the main
  * and the split launch (0 when off or no split). */
 int xplus_batch_resident_info(xplus_batch* h, int* on, int* smem, int* smem_split);
+/* on != 0 (the default): each resident launch is given the most dynamic shared memory that
+ * keeps its occupancy (all a CTA may have, or half an SM's when two CTAs share one), and a CTA
+ * whose band's matrix (values and columns) fits beside its vectors copies it there once per
+ * system; its SpMV then reads no global memory.  Same products in the same order, so the
+ * results are the same bit for bit.  0: every launch sized to its largest band, the matrix
+ * read from global memory. */
+int xplus_batch_set_stage_matrix(xplus_batch* h, int on);
+/* Whether matrix staging is on, and over the last resident solve the systems whose every CTA
+ * staged its band's matrix (systems_all) and those where only some did (systems_some); both 0
+ * with the global-memory kernel. */
+int xplus_batch_staged_info(xplus_batch* h, int* on, int* systems_all, int* systems_some);
 /* The launch-shape autotuner: times every cluster x block_threads shape that launches and keeps
  * the fastest, with x0 = 0 for every system; then, on that shape, splits off the 1, 2, 4, 8 or
  * 16 largest systems (at most a quarter of them) into clusters of 16 x 512, 8 x 512 or 16 x 256;

@@ -127,6 +127,8 @@ _SIGS = {
     "xplus_batch_split_info": (_i, [_p, _ip, _ip, _ip, _ip]),
     "xplus_batch_set_resident": (_i, [_p, _i]),
     "xplus_batch_resident_info": (_i, [_p, _ip, _ip, _ip]),
+    "xplus_batch_set_stage_matrix": (_i, [_p, _i]),
+    "xplus_batch_staged_info": (_i, [_p, _ip, _ip, _ip]),
     "xplus_batch_autotune": (_i, [_p, _i, _d, _ip, _ip, _dp]),
     "xplus_batch_solve": (_i, [_p, _p, _p, _d, _i, _i, _p]),
     "xplus_batch_solve_device": (_i, [_p, _p, _p, _d, _i, _i, _p]),

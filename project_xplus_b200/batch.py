@@ -103,6 +103,19 @@ class BatchSolver:
         check(lib.xplus_batch_resident_info(self._h, C.byref(on), C.byref(sm), C.byref(sm2)))
         return dict(on=bool(on.value), smem=sm.value, smem_split=sm2.value)
 
+    def set_stage_matrix(self, on: bool = True) -> None:
+        """Resident launches widened to the most shared memory that keeps their occupancy, and
+        each band's matrix copied there when it fits (on by default; results are the same bit
+        for bit either way)."""
+        check(lib.xplus_batch_set_stage_matrix(self._h, 1 if on else 0))
+
+    def staged(self) -> dict:
+        """Matrix staging: on, and over the last resident solve the systems whose every CTA
+        staged its band's matrix (all) or only some CTAs did (some)."""
+        on, al, so = C.c_int(), C.c_int(), C.c_int()
+        check(lib.xplus_batch_staged_info(self._h, C.byref(on), C.byref(al), C.byref(so)))
+        return dict(on=bool(on.value), all=al.value, some=so.value)
+
     def set_split_lane(self, count: int, cluster: int = 16, block_threads: int = 512) -> None:
         """The `count` largest systems in a concurrent launch of their own (0: none)."""
         check(lib.xplus_batch_set_split(self._h, int(count), int(cluster), int(block_threads)))

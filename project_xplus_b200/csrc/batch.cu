@@ -151,8 +151,8 @@ __global__ void __launch_bounds__(MAXT, MINB) pcg_batch_kernel(BatchArgs a) {
                                         const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
                                         // slots bypass L1 (streamed once per iteration), so L1 keeps
                                         // the records gathered below (measured 8% faster batch)
-                                        ChunkLoad<VT, CHUNK, true>::run(val + off, v[k][h]);
-                                        ColLoad<CHUNK, IT, true>::run(col + off, row[k], cc[k][h]);
+                                        ChunkLoad<VT, CHUNK, kLdNoAlloc>::run(val + off, v[k][h]);
+                                        ColLoad<CHUNK, IT, kLdNoAlloc>::run(col + off, row[k], cc[k][h]);
                                     } else {
 #pragma unroll
                                         for (int q = 0; q < CHUNK; ++q) {
@@ -368,7 +368,11 @@ struct xplus_batch {
     xplus::BatchKernel res_kernel = nullptr;
     bool resident = false;
     int res_max_dyn = 0;             // dynamic shared memory a CTA may have (bytes)
+    int res_half = 0;                // dynamic shared memory at which two CTAs share an SM
     int res_smem = 0, res_smem2 = 0; // the main and the split launch's dynamic shared memory
+    // stage each band's matrix in the shared memory a launch has beyond its vectors (each
+    // launch widened to the most that keeps its occupancy)
+    bool stage_matrix = true;
     std::vector<int> order;          // host copy of the queue (system ids, largest first)
     std::vector<int> need[5];        // [log2 cluster][system]: resident bytes per CTA
     float* d_rec3 = nullptr;
@@ -402,6 +406,7 @@ struct xplus_batch {
     int* d_repl = nullptr;
     double* d_true_rel = nullptr;
     long long* d_ns = nullptr;
+    int* d_staged = nullptr;        // resident kernel: CTAs per system that staged their matrix
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // CUDA graph of the last device solve, replayed while its arguments stay the same
     cudaGraphExec_t gexec = nullptr;
@@ -409,7 +414,7 @@ struct xplus_batch {
     double* g_x = nullptr;
     double g_tau = 0.0;
     int g_mode = -1, g_iters = 0, g_cluster = 0, g_tpb = 0, g_split = -1, g_cluster2 = 0, g_tpb2 = 0;
-    bool g_resident = false;
+    bool g_resident = false, g_stage = false;
     bool pending = false;
     bool have_b = false;   // d_b64 holds the (gathered) right-hand side of a solve
     double last_ms = 0.0;
@@ -498,6 +503,17 @@ int active_clusters(xplus_batch* h, int cluster, int tpb, int smem = 0) {
     return num;
 }
 
+// The dynamic shared memory of a resident launch whose systems need `need` bytes per CTA: with
+// matrix staging, the most (all a CTA may have, or what lets two CTAs share an SM) at which
+// clusters of `cluster` CTAs of `tpb` threads are as many on the device as at `need`.
+int widen_budget(xplus_batch* h, int cluster, int tpb, int need) {
+    if (!h->stage_matrix) return need;
+    const int num = active_clusters(h, cluster, tpb, need);
+    for (int b : {h->res_max_dyn, h->res_half})
+        if (b >= need && active_clusters(h, cluster, tpb, b) == num) return b;
+    return need;
+}
+
 // Grids of the two launches (and, for the resident kernel, their dynamic shared memory) for
 // the handle's current kernel and shapes; throws when a shape cannot launch or a system does
 // not fit the resident kernel's shared memory at its lane's cluster size.
@@ -512,6 +528,8 @@ void plan(xplus_batch* h) {
         require(h->res_smem2 <= h->res_max_dyn, XPLUS_ERR_ARG,
                 "a system of the split launch does not fit the resident kernel's shared memory at cluster " +
                     std::to_string(h->cluster2) + " (" + std::to_string(h->res_smem2) + " bytes per CTA)");
+        if (split < h->nsys) h->res_smem = widen_budget(h, h->cluster, h->tpb, h->res_smem);
+        if (split > 0) h->res_smem2 = widen_budget(h, h->cluster2, h->tpb2, h->res_smem2);
     }
     if (split < h->nsys) {
         const int num = active_clusters(h, h->cluster, h->tpb, h->resident ? h->res_smem : 0);
@@ -750,6 +768,11 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
                 h->res_kernel = nullptr;
             } else {
                 h->res_max_dyn = optin - st;
+                int per_sm = 0;
+                if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, o.device) == cudaSuccess)
+                    h->res_half = std::max(0, per_sm / 2 - st - 1024);  // 1 KB per CTA is the system's
+                else
+                    cudaGetLastError();
                 if (cudaFuncSetAttribute(fk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
                     cudaGetLastError();
             }
@@ -883,6 +906,7 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
         h->d_repl = balloc<int>(h, static_cast<size_t>(nsys));
         h->d_true_rel = balloc<double>(h, static_cast<size_t>(nsys));
         h->d_ns = balloc<long long>(h, static_cast<size_t>(nsys));
+        h->d_staged = balloc<int>(h, static_cast<size_t>(nsys));
         upload(h, h->d_order, order);
         upload(h, h->d_slice0, slice0);
         upload(h, h->d_sysn, sysn);
@@ -898,6 +922,7 @@ void batch_create(int nsys, const int* const* row_ptrs, const int* const* col_id
         upload(h, h->d_map, map);
         bcheck(cudaMemsetAsync(h->d_x64, 0, R * sizeof(double), h->stream), "memset");
         bcheck(cudaMemsetAsync(h->d_rec, 0, R * sizeof(NodeRec<float>), h->stream), "memset");
+        bcheck(cudaMemsetAsync(h->d_staged, 0, static_cast<size_t>(nsys) * sizeof(int), h->stream), "memset");
         bcheck(cudaStreamSynchronize(h->stream), "sync");
         set_launch(h, 4, 512);
         *out = h;
@@ -944,6 +969,8 @@ void enqueue_kernel(xplus_batch* h, double tau, int tau_mode, int max_iters, int
     a.out_repl = h->d_repl;
     a.out_true_rel = h->d_true_rel;
     a.out_ns = h->d_ns;
+    a.stage_matrix = h->stage_matrix ? 1 : 0;
+    a.out_staged = h->d_staged;
     bcheck(cudaMemsetAsync(h->d_head, 0, 2 * sizeof(int), st), "memset");
     auto launch = [&](const BatchArgs& args, int c, int t, int g, cudaStream_t s, int priority, const char* what) {
         cudaLaunchConfig_t cfg = {};
@@ -1081,7 +1108,7 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
         const bool same = h->gexec && h->g_b == d_b && h->g_x == d_x && h->g_tau == tau && h->g_mode == tau_mode &&
                           h->g_iters == max_iters && h->g_cluster == h->cluster && h->g_tpb == h->tpb &&
                           h->g_split == h->split && h->g_cluster2 == h->cluster2 && h->g_tpb2 == h->tpb2 &&
-                          h->g_resident == h->resident;
+                          h->g_resident == h->resident && h->g_stage == h->stage_matrix;
         if (!same) {
             if (h->gexec) {
                 bcheck(cudaGraphExecDestroy(h->gexec), "graph destroy");
@@ -1113,6 +1140,7 @@ int xplus_batch_solve_device(xplus_batch* h, const double* d_b, double* d_x, dou
             h->g_cluster2 = h->cluster2;
             h->g_tpb2 = h->tpb2;
             h->g_resident = h->resident;
+            h->g_stage = h->stage_matrix;
         }
         bcheck(cudaEventRecord(h->ev0, st), "event");
         bcheck(cudaGraphLaunch(h->gexec, st), "graph launch");
@@ -1235,10 +1263,7 @@ int xplus_batch_autotune(xplus_batch* h, int iters, double tau, int* cluster, in
         // what lets two CTAs share an SM) go to a split launch of 16-CTA clusters, largest first
         if (h->res_kernel) {
             ensure_rec3(h);
-            int per_sm = 0;
-            bcheck(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device), "attribute");
-            const int st_bytes = batch_resident_static_smem(h->res_kernel);
-            const int half = per_sm / 2 - st_bytes - 1024;  // 1 KB per CTA is the system's
+            const int half = h->res_half;
             for (int c : {2, 4, 8}) {
                 // suffix maxima of the needs in queue order: the main launch takes [k, nsys)
                 const std::vector<int>& nd = h->need[log2_cluster(c)];
@@ -1273,6 +1298,43 @@ int xplus_batch_set_resident(xplus_batch* h, int on) {
         require(h, XPLUS_ERR_ARG, "null handle");
         bcheck(cudaSetDevice(h->device), "cudaSetDevice");
         set_resident(h, on != 0);
+    });
+}
+
+int xplus_batch_set_stage_matrix(xplus_batch* h, int on) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        const bool s0 = h->stage_matrix;
+        try {
+            replan(h, [&] { h->stage_matrix = on != 0; });
+        } catch (...) {
+            h->stage_matrix = s0;
+            throw;
+        }
+    });
+}
+
+int xplus_batch_staged_info(xplus_batch* h, int* on, int* systems_all, int* systems_some) {
+    return guarded([&] {
+        require(h, XPLUS_ERR_ARG, "null handle");
+        bcheck(cudaSetDevice(h->device), "cudaSetDevice");
+        if (on) *on = h->stage_matrix ? 1 : 0;
+        int all = 0, some = 0;
+        if (h->resident) {
+            collect(h);
+            std::vector<int> st(static_cast<size_t>(h->nsys));
+            bcheck(cudaMemcpy(st.data(), h->d_staged, st.size() * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+            const int split = std::min(h->split, h->nsys);
+            for (int q = 0; q < h->nsys; ++q) {
+                const int k = st[static_cast<size_t>(h->order[static_cast<size_t>(q)])];
+                const int cs = q < split ? h->cluster2 : h->cluster;
+                if (k >= cs) ++all;
+                else if (k > 0) ++some;
+            }
+        }
+        if (systems_all) *systems_all = all;
+        if (systems_some) *systems_some = some;
     });
 }
 

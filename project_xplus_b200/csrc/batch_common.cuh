@@ -38,6 +38,8 @@ struct BatchArgs {
     float* rec3;              // resident kernel: [generation][{M r, M Ap', p'}][rows]
     int rows;                 // concatenated SELL rows (padding included)
     int res_smem;             // resident kernel: dynamic shared memory of the launch (bytes)
+    int stage_matrix;         // resident kernel: copy a band's matrix into shared memory when it fits
+    int* out_staged;          // resident kernel: CTAs of the system's cluster that staged their band
     double tau;
     int tau_mode;             // XPLUS_TAU_ABS_RR | XPLUS_TAU_REL_TRUE
     int max_iters;            // <= 0: max(4n, 1000) per system
@@ -97,8 +99,8 @@ __device__ __forceinline__ double batch_row64(const BatchArgs& a, int s, int lan
     for (int c = 0; c < w; c += CHUNK) {
         double v[CHUNK];
         int cc[CHUNK];
-        dev::ChunkLoad<double, CHUNK, true>::run(vp, v);
-        dev::ColLoad<CHUNK, IT, true>::run(cp, row, cc);
+        dev::ChunkLoad<double, CHUNK, dev::kLdNoAlloc>::run(vp, v);
+        dev::ColLoad<CHUNK, IT, dev::kLdNoAlloc>::run(cp, row, cc);
 #pragma unroll
         for (int q = 0; q < CHUNK; ++q) acc += v[q] * __ldcg(a.x64 + cc[q]);
         vp += 32 * CHUNK;

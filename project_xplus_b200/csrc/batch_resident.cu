@@ -18,9 +18,13 @@
 // global-memory batch kernel (kernels/cuper_pcg_control_kernel.cpp:1069-1235).
 //
 // Dynamic shared memory per CTA (bytes): 16-aligned slice table (8 per slice) | p' window
-// (4 wn) | r | Ap' | dx | M^-1 | row sums (4 nb each).  The host sizes each launch for the
-// largest band among the systems it routes there; a system that would not fit is skipped
-// with iterations = -1, which the host reports as an error.
+// (4 wn) | r | Ap' | dx | M^-1 | row sums (4 nb each) | (when it fits the rest of the
+// launch's budget) the band's own matrix: values, then columns, slot for slot as in global
+// memory.  A CTA whose band's matrix is staged there reads no global memory in the SpMV; the
+// products are the same, in the same order.  The host sizes each launch for the largest band
+// among the systems it routes there (and widens it to the most that keeps the launch's
+// occupancy, so that matrices fit); a system that would not fit is skipped with
+// iterations = -1, which the host reports as an error.
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -51,8 +55,8 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
     __shared__ double s_tot[8];
     __shared__ int s_item[2];
     __shared__ int s_mm[2][32];
-    __shared__ int s_win[3];   // this CTA's w0, wn, fits (read by the other CTAs)
-    __shared__ int s_sys[3];   // exp_lo, exp_hi, every CTA fits
+    __shared__ int s_win[4];   // this CTA's w0, wn, fits, matrix staged (read by the other CTAs)
+    __shared__ int s_sys[4];   // exp_lo, exp_hi, every CTA fits, CTAs that staged their matrix
     cg::cluster_group cl = cg::this_cluster();
     const int crank = static_cast<int>(cl.block_rank());
     const int csize = static_cast<int>(cl.num_blocks());
@@ -142,19 +146,25 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
                 const int wend = min((S0 + ns) * 32, (cmax + 3) & ~3);
                 const long long need = ((static_cast<long long>(nsl) * 8 + 15) & ~15LL) +
                                        4LL * (static_cast<long long>(wend - w0) + 5LL * nb);
+                // the band's slots (a multiple of 32 per slice, so both arrays are whole
+                // 16-byte groups)
+                const long long ms = a.slice_ptr[se] - a.slice_ptr[sb];
+                const long long mat = ms * static_cast<long long>(sizeof(VT) + sizeof(IT));
                 s_win[0] = w0;
                 s_win[1] = wend - w0;
                 s_win[2] = need <= a.res_smem ? 1 : 0;
+                s_win[3] = a.stage_matrix && need + mat <= a.res_smem ? 1 : 0;
             }
         }
         // every CTA's window: the rows of this band that others read, and whether all fit
         cl.sync();
         if (threadIdx.x == 0) {
-            int lo = r0, hi = r0 + nb, fit = 1;
+            int lo = r0, hi = r0 + nb, fit = 1, staged = 0;
             for (int rk = 0; rk < csize; ++rk) {
                 const int* wk = cl.map_shared_rank(s_win, rk);
                 const int wx = wk[0], wy = wk[1];
                 fit &= wk[2];
+                staged += wk[3];
                 if (rk == crank || wy <= 0) continue;
                 if (rk < crank) lo = max(lo, wx + wy);
                 else hi = min(hi, wx);
@@ -162,6 +172,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
             s_sys[0] = min(lo, r0 + nb);
             s_sys[1] = max(hi, r0);
             s_sys[2] = fit;
+            s_sys[3] = staged;
         }
         __syncthreads();
         if (!s_sys[2]) {
@@ -173,10 +184,12 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
                 a.out_repl[sys] = 0;
                 a.out_true_rel[sys] = -1.0;
                 a.out_ns[sys] = 0;
+                if (a.out_staged) a.out_staged[sys] = 0;
             }
             continue;
         }
         const int w0 = s_win[0], wn = s_win[1];
+        const bool staged = s_win[3] != 0;
         const int exp_lo = s_sys[0], exp_hi = s_sys[1];
         int2* s_slice = reinterpret_cast<int2*>(smem_raw);
         float* pw = reinterpret_cast<float*>(smem_raw + ((static_cast<size_t>(nsl) * 8 + 15) & ~static_cast<size_t>(15)));
@@ -185,9 +198,26 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
         float* dxv = apv + nb;
         float* mi = dxv + nb;
         float* rsv = mi + nb;
+        // the staged matrix (16-aligned: the vectors end on a 16-byte boundary, wn being a
+        // multiple of 4 and nb of 32); slice offsets then count from the band's first slot
+        const long long m0 = a.slice_ptr[sb];
+        const long long ms = a.slice_ptr[se] - m0;
+        VT* mval = reinterpret_cast<VT*>(rsv + nb);
+        IT* mcol = reinterpret_cast<IT*>(mval + ms);
         for (int k = threadIdx.x; k < nsl; k += blockDim.x) {
             const long long b0 = a.slice_ptr[sb + k];
-            s_slice[k] = make_int2(static_cast<int>(b0), static_cast<int>((a.slice_ptr[sb + k + 1] - b0) >> 5));
+            s_slice[k] = make_int2(static_cast<int>(staged ? b0 - m0 : b0),
+                                   static_cast<int>((a.slice_ptr[sb + k + 1] - b0) >> 5));
+        }
+        if (staged) {
+            const uint4* gv = reinterpret_cast<const uint4*>(val + m0);
+            const uint4* gc = reinterpret_cast<const uint4*>(col + m0);
+            uint4* sv = reinterpret_cast<uint4*>(mval);
+            uint4* sc = reinterpret_cast<uint4*>(mcol);
+            const long long nv = ms * static_cast<long long>(sizeof(VT)) / 16;
+            const long long nc = ms * static_cast<long long>(sizeof(IT)) / 16;
+            for (long long i = threadIdx.x; i < nv; i += blockDim.x) sv[i] = __ldg(gv + i);
+            for (long long i = threadIdx.x; i < nc; i += blockDim.x) sc[i] = __ldg(gc + i);
         }
         for (int t = threadIdx.x; t < nb; t += blockDim.x) {
             mi[t] = a.minv[r0 + t];
@@ -356,7 +386,9 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
                             row[k] = on ? s * 32 + lane : -1;
                             pi[k] = on ? pw[row[k] - w0] : 0.0f;
                         }
-                        sell_rows_smem<VT, CHUNK, IT, NS>(sl, row, lane, col, val, pw, w0, pi, y);
+                        // one generic load path for both homes of the matrix
+                        sell_rows_smem<VT, CHUNK, IT, NS, kLdPlain>(sl, row, lane, staged ? mcol : col,
+                                                                    staged ? mval : val, pw, w0, pi, y);
 #pragma unroll
                         for (int k = 0; k < NS; ++k) {
                             if (row[k] < 0) continue;
@@ -486,6 +518,7 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
             a.out_repl[sys] = replacements;
             a.out_true_rel[sys] = bb > 0.0 ? sqrt(s_tot[0] / bb) : sqrt(s_tot[0]);
             a.out_ns[sys] = globaltimer_ns() - t_begin;
+            if (a.out_staged) a.out_staged[sys] = s_sys[3];
         }
     }
 }

@@ -45,48 +45,53 @@ __device__ __forceinline__ unsigned short ld_na(const unsigned short* p) {
     unsigned short v; asm volatile("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p)); return v; }
 __device__ __forceinline__ short ld_na(const short* p) {
     short v; asm volatile("ld.global.nc.L1::no_allocate.s16 %0, [%1];" : "=h"(v) : "l"(p)); return v; }
-template <bool NA, typename T>
+// Load flavours of the matrix streams: through the read-only path (kLdg), read-only without L1
+// allocation (kLdNoAlloc), or a plain load (kLdPlain: for arrays staged in shared memory, where
+// the read-only global forms would be wrong).
+constexpr int kLdg = 0, kLdNoAlloc = 1, kLdPlain = 2;
+template <int NA, typename T>
 __device__ __forceinline__ T ldro(const T* p) {
-    if constexpr (NA) return ld_na(p);
+    if constexpr (NA == kLdNoAlloc) return ld_na(p);
+    else if constexpr (NA == kLdPlain) return *p;
     else return __ldg(p);
 }
 
-// Matrix chunk loads: CHUNK consecutive slots of one row, as one vector load through the
-// read-only path (the matrix never changes inside a kernel).
+// Matrix chunk loads: CHUNK consecutive slots of one row, as one vector load in the flavour NA
+// (the matrix never changes inside a kernel).
 // ---------------------------------------------------------------------------------------
-template <typename VT, int CHUNK, bool NA = false>
+template <typename VT, int CHUNK, int NA = kLdg>
 struct ChunkLoad;
 
-template <bool NA>
+template <int NA>
 struct ChunkLoad<float, 1, NA> {
     static __device__ __forceinline__ void run(const float* p, float* o) { o[0] = ldro<NA>(p); }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<float, 2, NA> {
     static __device__ __forceinline__ void run(const float* p, float* o) {
         const float2 v = ldro<NA>(reinterpret_cast<const float2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<float, 4, NA> {
     static __device__ __forceinline__ void run(const float* p, float* o) {
         const float4 v = ldro<NA>(reinterpret_cast<const float4*>(p));
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<double, 1, NA> {
     static __device__ __forceinline__ void run(const double* p, double* o) { o[0] = ldro<NA>(p); }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<double, 2, NA> {
     static __device__ __forceinline__ void run(const double* p, double* o) {
         const double2 v = ldro<NA>(reinterpret_cast<const double2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<double, 4, NA> {
     static __device__ __forceinline__ void run(const double* p, double* o) {
         const double2 a = ldro<NA>(reinterpret_cast<const double2*>(p));
@@ -96,21 +101,21 @@ struct ChunkLoad<double, 4, NA> {
 };
 __device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
-template <bool NA>
+template <int NA>
 struct ChunkLoad<__nv_bfloat16, 1, NA> {
     static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
         const unsigned short v = ldro<NA>(reinterpret_cast<const unsigned short*>(p));
         o[0] = __uint_as_float(static_cast<uint32_t>(v) << 16);
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<__nv_bfloat16, 2, NA> {
     static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
         const uint32_t v = ldro<NA>(reinterpret_cast<const unsigned int*>(p));
         o[0] = bf16_lo(v); o[1] = bf16_hi(v);
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<__nv_bfloat16, 4, NA> {
     static __device__ __forceinline__ void run(const __nv_bfloat16* p, float* o) {
         const uint2 v = ldro<NA>(reinterpret_cast<const uint2*>(p));
@@ -124,20 +129,20 @@ __device__ __forceinline__ float f16_lo(uint32_t w) {
 __device__ __forceinline__ float f16_hi(uint32_t w) {
     return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
 }
-template <bool NA>
+template <int NA>
 struct ChunkLoad<__half, 1, NA> {
     static __device__ __forceinline__ void run(const __half* p, float* o) {
         o[0] = __half2float(__ushort_as_half(ldro<NA>(reinterpret_cast<const unsigned short*>(p))));
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<__half, 2, NA> {
     static __device__ __forceinline__ void run(const __half* p, float* o) {
         const uint32_t v = ldro<NA>(reinterpret_cast<const unsigned int*>(p));
         o[0] = f16_lo(v); o[1] = f16_hi(v);
     }
 };
-template <bool NA>
+template <int NA>
 struct ChunkLoad<__half, 4, NA> {
     static __device__ __forceinline__ void run(const __half* p, float* o) {
         const uint2 v = ldro<NA>(reinterpret_cast<const uint2*>(p));
@@ -147,20 +152,20 @@ struct ChunkLoad<__half, 4, NA> {
 
 // Column loads: absolute int32 columns, or int16 offsets from the row (lossless when the
 // bandwidth of the ordered matrix is below 32768) returned as absolute columns.
-template <int CHUNK, typename IT, bool NA = false>
+template <int CHUNK, typename IT, int NA = kLdg>
 struct ColLoad;
-template <bool NA>
+template <int NA>
 struct ColLoad<1, int, NA> {
     static __device__ __forceinline__ void run(const int* p, int, int* o) { o[0] = ldro<NA>(p); }
 };
-template <bool NA>
+template <int NA>
 struct ColLoad<2, int, NA> {
     static __device__ __forceinline__ void run(const int* p, int, int* o) {
         const int2 v = ldro<NA>(reinterpret_cast<const int2*>(p));
         o[0] = v.x; o[1] = v.y;
     }
 };
-template <bool NA>
+template <int NA>
 struct ColLoad<4, int, NA> {
     static __device__ __forceinline__ void run(const int* p, int, int* o) {
         const int4 v = ldro<NA>(reinterpret_cast<const int4*>(p));
@@ -169,18 +174,18 @@ struct ColLoad<4, int, NA> {
 };
 __device__ __forceinline__ int lo16(uint32_t w) { return static_cast<int>(static_cast<short>(w & 0xFFFFu)); }
 __device__ __forceinline__ int hi16(uint32_t w) { return static_cast<int>(static_cast<short>(w >> 16)); }
-template <bool NA>
+template <int NA>
 struct ColLoad<1, short, NA> {
     static __device__ __forceinline__ void run(const short* p, int row, int* o) { o[0] = row + ldro<NA>(p); }
 };
-template <bool NA>
+template <int NA>
 struct ColLoad<2, short, NA> {
     static __device__ __forceinline__ void run(const short* p, int row, int* o) {
         const uint32_t v = ldro<NA>(reinterpret_cast<const unsigned int*>(p));
         o[0] = row + lo16(v); o[1] = row + hi16(v);
     }
 };
-template <bool NA>
+template <int NA>
 struct ColLoad<4, short, NA> {
     static __device__ __forceinline__ void run(const short* p, int row, int* o) {
         const uint2 v = ldro<NA>(reinterpret_cast<const uint2*>(p));

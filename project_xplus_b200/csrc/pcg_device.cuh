@@ -314,9 +314,10 @@ __device__ __forceinline__ void sell_rows_pnew(const int2 (&sl)[NS], const int (
 }
 
 
-// NS slices of one warp: all value/column loads of the group first (the only global traffic),
-// then the products with p' gathered from the shared-memory window.  y_k excludes s_i p'_i.
-template <typename VT, int CHUNK, typename IT, int NS>
+// NS slices of one warp: all value/column loads of the group first (the only global traffic,
+// or shared-memory loads with LD = kLdPlain when the matrix itself is staged there), then the
+// products with p' gathered from the shared-memory window.  y_k excludes s_i p'_i.
+template <typename VT, int CHUNK, typename IT, int NS, int LD = kLdg>
 __device__ __forceinline__ void sell_rows_smem(const int2 (&sl)[NS], const int (&row)[NS], int lane,
                                                const IT* __restrict__ col, const VT* __restrict__ val,
                                                const float* pw, int w0, const float (&pi)[NS],
@@ -336,8 +337,8 @@ __device__ __forceinline__ void sell_rows_smem(const int2 (&sl)[NS], const int (
             for (int h = 0; h < 2; ++h) {
                 if (c + h * CHUNK < sl[k].y) {
                     const int off = sl[k].x + (c + h * CHUNK) * 32 + lane * CHUNK;
-                    ChunkLoad<VT, CHUNK>::run(val + off, v[k][h]);
-                    ColLoad<CHUNK, IT>::run(col + off, row[k], cc[k][h]);
+                    ChunkLoad<VT, CHUNK, LD>::run(val + off, v[k][h]);
+                    ColLoad<CHUNK, IT, LD>::run(col + off, row[k], cc[k][h]);
                 } else {
 #pragma unroll
                     for (int q = 0; q < CHUNK; ++q) {

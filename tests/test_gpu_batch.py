@@ -171,8 +171,9 @@ def test_resident_kernel(gpu, batch_systems, vt, cluster, tpb, split):
     memory, one cluster barrier per iteration): every system reaches the tolerance, its
     iteration count stays within the dot-product rounding of the global-memory kernel's, the
     two solutions are equally close to the direct solve (two solutions at residual 1e-8 may
-    differ by up to cond(A) x 1e-8), repeated solves are bit-identical, and the graph-captured
-    device path gives the host path's x bit for bit."""
+    differ by up to cond(A) x 1e-8), repeated solves are bit-identical, staging the bands'
+    matrices in shared memory changes no bit, and the graph-captured device path gives the host
+    path's x bit for bit."""
     import torch
     from scipy.sparse import csr_matrix
     from scipy.sparse.linalg import spsolve
@@ -197,6 +198,17 @@ def test_resident_kernel(gpu, batch_systems, vt, cluster, tpb, split):
         assert err <= 10 * max(err_ref, 1e-7), (k, err, err_ref)
     again = s.solve(b, tau=1e-8)
     np.testing.assert_array_equal(again["x"], r["x"])
+    # each band's matrix staged in shared memory (the default) or read from global memory:
+    # the same products in the same order, so the same x bit for bit
+    staged = s.staged()
+    assert staged["on"] and staged["all"] + staged["some"] > 0, staged
+    s.set_stage_matrix(False)
+    assert s.resident()["smem"] <= info["smem"]
+    unstaged = s.solve(b, tau=1e-8)
+    assert s.staged() == dict(on=False, all=0, some=0)
+    np.testing.assert_array_equal(unstaged["x"], r["x"])
+    np.testing.assert_array_equal(unstaged["iterations"], r["iterations"])
+    s.set_stage_matrix(True)
     d_b = torch.from_numpy(b).cuda()
     d_x = torch.zeros_like(d_b)
     st = torch.cuda.Stream()

@@ -324,16 +324,17 @@ def test_trained_network_beats_jacobi(gpu):
 def test_learned_beats_same_layout_jacobi_in_time(gpu):
     """Held-out systems (training systems use seeds from 110000 on): the learned G^T G solve
     reaches the 1e-8 FP64 true residual in fewer than half the iterations of the default Jacobi
-    solve of the same handle layout (the SM-resident one-barrier kernel) on 300x300 and 600x600
-    systems, and in less kernel time on the 600x600 one.  (On 300x300 the two take about the
-    same time: a G^T G iteration costs about three Jacobi iterations there, and Jacobi needs
-    only ~1500 iterations; the gain grows with the grid, to 2.1x on 1108x1108.)  Both timed on
-    their second solve."""
+    solve of the same handle layout (the SM-resident one-barrier kernel) on 300x300, 600x600
+    and 1000x1000 systems, and in at most 0.7x its kernel time on the 1000x1000 one.  A G^T G
+    iteration costs about three to five Jacobi iterations (three grid barriers, A, G and G^T
+    streamed), so the time gain grows with the grid as Jacobi's iteration count does: measured
+    learned / Jacobi kernel time 0.90-0.92 on 300x300 and 0.90-0.96 on 600x600 over several
+    machines, 0.44 on the 1108x1108 benchmark system.  Both timed on their second solve."""
     from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
     from project_xplus_b200 import generators as gen
     from project_xplus_b200.learned import load_weights
     params, _ = load_weights()
-    for side in (300, 600):
+    for side in (300, 600, 1000):
         d, _ = gen.fem2d(side, sigma=2.0, jitter=0.3, seed=91, perm_seed=91, rcm=True, x_seed=91)
         s = PcgSolver(d.row_ptr, d.col_idx, d.values)
         for _ in range(2):
@@ -345,8 +346,8 @@ def test_learned_beats_same_layout_jacobi_in_time(gpu):
         s.close()
         assert lrn.converged and lrn.residual_rel <= 1e-8 and lrn.metrics["jacobi_fallback_at"] == -1
         assert lrn.iterations < 0.5 * jac.iterations, (side, lrn.iterations, jac.iterations)
-        if side == 600:
-            assert lrn.kernel_ms < 0.9 * jac.kernel_ms, (lrn.kernel_ms, jac.kernel_ms, lrn.iterations, jac.iterations)
+        if side == 1000:
+            assert lrn.kernel_ms < 0.7 * jac.kernel_ms, (lrn.kernel_ms, jac.kernel_ms, lrn.iterations, jac.iterations)
 
 
 def test_gtg_with_fp16_values(gpu, sys64):

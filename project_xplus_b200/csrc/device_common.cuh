@@ -238,6 +238,15 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     return v;
 }
 
+// Arrival at a grid barrier: the add is a release (this thread's earlier writes, and those of
+// the CTA that a preceding __syncthreads ordered before it, are visible before it) and an
+// acquire (the block that arrives last, and sees the full count in the value returned, then
+// sees every other block's writes); the old value is returned.
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 __device__ __forceinline__ int ld_volatile_int(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
 }
@@ -266,9 +275,12 @@ struct GridBarrier {
         if (threadIdx.x == 0) {
             ++epoch;
             const unsigned target = epoch * gridDim.x;
-            __threadfence();
+            // ordering through the counter alone (no separate fences): the arrival is an
+            // acquire-release add and the polling loads are acquires; the counter's adds form
+            // one release sequence, so the load that sees the full count synchronizes with
+            // every block's arrival
             unsigned seen = target;  // a withheld arrival never completes the barrier
-            if (!(static_cast<int>(blockIdx.x) == skip_block && epoch == 1u)) seen = atomicAdd(counter, 1u) + 1u;
+            if (!(static_cast<int>(blockIdx.x) == skip_block && epoch == 1u)) seen = atom_add_acq_rel_gpu(counter, 1u) + 1u;
             else seen = 0u;
             int ok = 1;
             // the last block to arrive sees the full count in its own atomic: no polling
@@ -286,7 +298,6 @@ struct GridBarrier {
                     }
                 }
             }
-            __threadfence();
             *s_flag = ok;
         }
         __syncthreads();

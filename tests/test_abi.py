@@ -67,3 +67,13 @@ def test_argument_errors():
     h = C.c_void_p()
     rc = _lib.lib.xplus_pcg_create(None, None, None, 4, None, C.byref(h))
     assert rc == _lib.XPLUS_ERR_ARG
+
+
+def test_batch_entry_points_reject_a_null_handle():
+    """The batched solver's setters and queries check the handle before any CUDA call."""
+    for rc in (_lib.lib.xplus_batch_set_resident(None, 1),
+               _lib.lib.xplus_batch_set_stage_matrix(None, 1),
+               _lib.lib.xplus_batch_staged_info(None, None, None, None),
+               _lib.lib.xplus_batch_resident_info(None, None, None, None),
+               _lib.lib.xplus_batch_split_info(None, None, None, None, None)):
+        assert rc == _lib.XPLUS_ERR_ARG

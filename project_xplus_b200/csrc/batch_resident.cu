@@ -323,21 +323,46 @@ __global__ void __launch_bounds__(512, 1) pcg_batch_res_kernel(BatchArgs a) {
                 const bool upd = pend != 0.0;
                 const bool flush = upd && it % kFlushEvery == 0;
                 const float be = static_cast<float>(beta);
-                for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-                    float* pp = pw + (r0 + t - w0);
-                    const float pv = *pp;
-                    const float r_ = rv[t], ap_ = apv[t], m = mi[t];
-                    const float mr = m * r_;
-                    const float ma = upd ? m * ap_ : 0.0f;  // the records' m Ap' is 0 after a residual
-                    *pp = __fmaf_rn(be, pv, __fmaf_rn(-al_prev, ma, mr));
-                    if (upd) {
-                        const float d = __fmaf_rn(al_prev, pv, dxv[t]);
-                        rv[t] = r_ - al_prev * ap_;
-                        if (flush) {
-                            a.x64[r0 + t] += static_cast<double>(d);
-                            dxv[t] = 0.0f;
-                        } else {
-                            dxv[t] = d;
+                {
+                    // four rows per thread and step (float4: pw + r0 - w0 and the band's arrays
+                    // start on 16-byte boundaries, w0 being a multiple of 4 and nb of 32); each
+                    // row's arithmetic is the scalar form's
+                    float4* pw4o = reinterpret_cast<float4*>(pw + (r0 - w0));
+                    float4* rv4 = reinterpret_cast<float4*>(rv);
+                    const float4* ap4 = reinterpret_cast<const float4*>(apv);
+                    const float4* mi4 = reinterpret_cast<const float4*>(mi);
+                    float4* dx4 = reinterpret_cast<float4*>(dxv);
+                    auto row_update = [&](float& pv, float& r_, float ap_, float m, float& d) {
+                        const float mr = m * r_;
+                        const float ma = upd ? m * ap_ : 0.0f;  // the records' m Ap' is 0 after a residual
+                        const float pn = __fmaf_rn(be, pv, __fmaf_rn(-al_prev, ma, mr));
+                        if (upd) {
+                            d = __fmaf_rn(al_prev, pv, d);
+                            r_ = r_ - al_prev * ap_;
+                        }
+                        pv = pn;
+                    };
+                    for (int t4 = threadIdx.x; t4 < (nb >> 2); t4 += blockDim.x) {
+                        float4 pv = pw4o[t4];
+                        float4 r4 = rv4[t4];
+                        const float4 a4 = ap4[t4], m4 = mi4[t4];
+                        float4 d4 = upd ? dx4[t4] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        row_update(pv.x, r4.x, a4.x, m4.x, d4.x);
+                        row_update(pv.y, r4.y, a4.y, m4.y, d4.y);
+                        row_update(pv.z, r4.z, a4.z, m4.z, d4.z);
+                        row_update(pv.w, r4.w, a4.w, m4.w, d4.w);
+                        pw4o[t4] = pv;
+                        if (upd) {
+                            rv4[t4] = r4;
+                            if (flush) {
+                                double* xr = a.x64 + r0 + 4 * t4;
+                                xr[0] += static_cast<double>(d4.x);
+                                xr[1] += static_cast<double>(d4.y);
+                                xr[2] += static_cast<double>(d4.z);
+                                xr[3] += static_cast<double>(d4.w);
+                                d4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            }
+                            dx4[t4] = d4;
                         }
                     }
                 }

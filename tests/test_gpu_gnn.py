@@ -329,8 +329,8 @@ def test_learned_beats_same_layout_jacobi_in_time(gpu):
     iterations pay in time depends on the system: a G^T G iteration costs three Jacobi
     iterations at 300x300 and four to five at 1000x1000 (three grid barriers, A, G and G^T
     streamed, more than L2 holds as the grid grows).  Measured learned / Jacobi kernel time:
-    0.90-0.92 on 300x300 (475 against 1526 iterations) and 0.90-0.96 on 600x600 (817 against
-    2814) over several machines, 1.05 on 1000x1000 (794 against 3428), and 0.44 on the
+    0.90-0.93 on 300x300 (475 against 1526 iterations) and 0.90-0.96 on 600x600 (817 against
+    2814) over several machines, 1.05 on 1000x1000 (794 against 3428), and 0.47 on the
     1108x1108 benchmark system, where one very stiff element holds Jacobi to 5721 iterations.
     Both timed on their second solve."""
     from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE

@@ -38,9 +38,9 @@ FALLBACK_HBM_GBS = 6650.0
 # core (the reference arm times a bounded sample of it per step).
 GOLDEN_ITERATIONS_1108 = 5569
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the SM-resident kernel per
-# iteration on the 1108x1108 system: 389.3 MB over a captured launch of 100 iterations
+# iteration on the 1108x1108 system: 349.1 MB over a captured launch of 100 iterations
 # (ncu --set full of `python -m project_xplus_b200.profile_case --grid 1108 --iters 100 --spmv 0`).
-RESIDENT1_DRAM_BYTES_PER_ITER = 389.3e6 / 100
+RESIDENT1_DRAM_BYTES_PER_ITER = 349.1e6 / 100
 
 
 def parse():

@@ -529,7 +529,7 @@ def run_b200(args):
             s3 = xp.PcgSolver.from_dataset(d, device=local, **kw3)
             t0 = time.perf_counter()
             if name.startswith("learned_gtg"):
-                s3.set_gnn(params)  # inference, one refinement sweep, rows normalized: on the GPU
+                s3.set_gnn(params)  # inference, four refinement sweeps, rows normalized: on the GPU
             else:
                 s3.set_gtg(fsai_lower(d.row_ptr, d.col_idx, d.values))
             pre_ms = (time.perf_counter() - t0) * 1e3  # preconditioner set-up on this handle

@@ -256,13 +256,15 @@ int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
  * (nullable) gets the host+device time of the inference. */
 int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
                       const float* params, int fallback_iters, double* infer_ms);
-/* xplus_pcg_set_gnn (which is this with refine_sweeps = 1) with the number of refinement sweeps
+/* xplus_pcg_set_gnn (which is this with refine_sweeps = 4) with the number of refinement sweeps
  * (0..16) run on the GPU between inference and normalization: each sweep takes the lower
  * entries j of every row i in ascending order and sets Ghat_ij to the minimizer of the row's
  * quadratic form (G A G^T)_ii at fixed Ghat_ii, a Gauss-Seidel step on the row's FSAI system
  * A[P_i, P_i] g = e_i.  Every step lowers the row's Kaporin term, so a sweep never makes a row
  * worse; it fixes rows the network cannot resolve, chiefly the two ends of a very stiff
- * element (a_ij^2 close to a_ii a_jj), where the row's best ratio G_ij / G_ii is sharp. */
+ * element (a_ij^2 close to a_ii a_jj), where the row's best ratio G_ij / G_ii is sharp.
+ * Repeated sweeps approach the exact FSAI row; from the network's G four sweeps come within
+ * 1% of FSAI's iteration count on the 1108x1108 system, where from Jacobi ten are needed. */
 int xplus_pcg_set_gnn_ex(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
                          const float* params, int fallback_iters, int refine_sweeps, double* infer_ms);
 /* The handle's current G in g_low order (g_low NULL: only *n_glow). */

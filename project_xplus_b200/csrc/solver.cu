@@ -1145,7 +1145,7 @@ int xplus_pcg_set_gtg(xplus_pcg* h, const int* row_ptr, const int* col_idx, cons
 
 int xplus_pcg_set_gnn(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,
                       const float* params, int fallback_iters, double* infer_ms) {
-    return xplus_pcg_set_gnn_ex(h, row_ptr, col_idx, values, params, fallback_iters, 1, infer_ms);
+    return xplus_pcg_set_gnn_ex(h, row_ptr, col_idx, values, params, fallback_iters, 4, infer_ms);
 }
 
 int xplus_pcg_set_gnn_ex(xplus_pcg* h, const int* row_ptr, const int* col_idx, const double* values,

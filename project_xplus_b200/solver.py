@@ -280,7 +280,7 @@ class PcgSolver:
         g = None if g_low is None else np.ascontiguousarray(g_low, np.float64)
         check(lib.xplus_pcg_set_gtg(self._h, ptr(self.row_ptr), ptr(self.col_idx), ptr(g), int(fallback_iters)))
 
-    def set_gnn(self, params=None, fallback_iters: int = 0, refine_sweeps: int = 1) -> float:
+    def set_gnn(self, params=None, fallback_iters: int = 0, refine_sweeps: int = 4) -> float:
         """M^-1 = G^T G with G predicted on the GPU by the learned network (default: the
         shipped weights), refined by `refine_sweeps` Gauss-Seidel sweeps on each row's quadratic
         form and normalized to (G A G^T)_ii = 1.  Returns the inference time in ms."""

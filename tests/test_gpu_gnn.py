@@ -292,8 +292,8 @@ def test_solver_inference_matches_trainer(trainer):
         raw = _gmat(d, t.predict(k))  # the trainer's output has the same row directions
         ratio = np.asarray(G.multiply(raw).sum(axis=1)).ravel() / np.asarray(raw.multiply(raw).sum(axis=1)).ravel()
         np.testing.assert_allclose(G.toarray(), (sp.diags(ratio) @ raw).toarray(), rtol=1e-5, atol=1e-6 * abs(got).max())
-        # the default: one sweep, then normalization
-        s.set_gnn(theta)
+        # one sweep, then normalization
+        s.set_gnn(theta, refine_sweeps=1)
         got1 = s.get_gtg()
         ref1 = _glow_from_oracle(d, *O.normalize_rows(g, O.refine_rows(g, go, gd, 1), gd))
         assert_close_bf16(got1, ref1, rtol=1e-3)
@@ -328,10 +328,12 @@ def test_learned_beats_same_layout_jacobi_in_time(gpu):
     and 1000x1000 systems, and on the 300x300 one in no more kernel time.  Whether the fewer
     iterations pay in time depends on the system: a G^T G iteration costs three Jacobi
     iterations at 300x300 and four to five at 1000x1000 (three grid barriers, A, G and G^T
-    streamed, more than L2 holds as the grid grows).  Measured learned / Jacobi kernel time:
-    0.90-0.93 on 300x300 (475 against 1526 iterations) and 0.90-0.96 on 600x600 (817 against
-    2814) over several machines, 1.05 on 1000x1000 (794 against 3428), and 0.47 on the
-    1108x1108 benchmark system, where one very stiff element holds Jacobi to 5721 iterations.
+    streamed, more than L2 holds as the grid grows).  Measured learned / Jacobi kernel time
+    with one refinement sweep: 0.90-0.93 on 300x300 (475 against 1526 iterations) and
+    0.90-0.96 on 600x600 (817 against 2814) over several machines, 1.05-1.11 on 1000x1000 (794
+    against 3428); with the default four sweeps 0.91 on 600x600, 1.04 on 1000x1000 (746
+    iterations) and 0.44 on the 1108x1108 benchmark system, where one very stiff element holds
+    Jacobi to 5721 iterations.
     Both timed on their second solve."""
     from project_xplus_b200 import PcgSolver, XPLUS_TAU_REL_TRUE
     from project_xplus_b200 import generators as gen
